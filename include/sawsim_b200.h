@@ -1,0 +1,153 @@
+/*
+ * sawsim_b200 — B200 frequency-sweep backend for SawSim's piezoelectric FEM.
+ *
+ * C ABI: opaque handle, plain pointers and sizes, int status returns, no
+ * exceptions across the boundary.  Complex arrays are interleaved (re, im)
+ * float64.  The caller keeps ownership of host memory; the handle owns all
+ * device memory.  A handle is single-threaded and uses one CUDA stream; do not
+ * fork a process after ss_create.
+ *
+ * The reference (Duane245/sawsim 2.1.0) has no C interface: its de-facto plugin
+ * boundary is the frequency-solver engine object built by
+ *   src/sawsim/solver.py:108   sweep.FrequencySolver(K, M, *bc)
+ *   src/sawsim/hex_solver.py:92 FrequencySolver3D(K, M, boundary, t_fb, t_lr)
+ * and driven per frequency by src/sawsim/frequency_tasks.py:33-55.  Each entry
+ * point below names the reference function whose work it replaces.
+ */
+#ifndef SAWSIM_B200_H
+#define SAWSIM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ss_handle ss_handle;
+
+/* status codes */
+#define SS_OK          0
+#define SS_EINVAL     -1   /* bad argument or size                              */
+#define SS_ECUDA      -2   /* CUDA runtime / driver error                       */
+#define SS_ESINGULAR  -3   /* zero pivot after static perturbation              */
+#define SS_ENOCONV    -4   /* iterative refinement did not converge             */
+#define SS_ETIMEOUT   -5   /* a bounded device wait ran out                     */
+#define SS_ENOMEM     -6   /* device allocation failed                          */
+#define SS_ESTATE     -7   /* call out of order (e.g. sweep before analyze)      */
+
+/* element families (src/sawsim/saw2d/piezo_fem.py:283, :373; saw3d/assembly.py:230) */
+#define SS_Q9_ME0   0      /* plane strain [ux | uy | phi], 3 DOF/node           */
+#define SS_Q9_ME1   1      /* [ux | uy | uz | phi], 4 DOF/node                   */
+#define SS_HEX27    2      /* u interleaved 3n+c, phi at 3N+n                    */
+
+/* precision modes for ss_sweep */
+#define SS_PREC_FP64   0   /* complex128 fronts, FP64 throughout (the drop-in)   */
+#define SS_PREC_MIXED  1   /* complex64 fronts, 3xTF32 tensor-core Schur updates,
+                              FP64 residual and refinement                       */
+
+/* matrix selectors for ss_set_csr / ss_export_csr */
+#define SS_MAT_K    0      /* global stiffness                                   */
+#define SS_MAT_M    1      /* global mass                                        */
+#define SS_MAT_D    2      /* global damping (Rayleigh beta*D part)              */
+#define SS_MAT_KC   3      /* condensed active stiffness, active-DOF order       */
+#define SS_MAT_MC   4      /* condensed active mass, active-DOF order            */
+
+/* Create / destroy.  `device` is the CUDA ordinal. */
+int ss_create(ss_handle **out, int device);
+void ss_destroy(ss_handle *h);
+/* Last error message of this handle (never NULL). */
+const char *ss_last_error(const ss_handle *h);
+
+/*
+ * Mesh input of the GPU assembly (replaces the inputs of piezo_fem.assemble,
+ * src/sawsim/saw2d/piezo_fem.py:283, and form_stiffness_mass_3d,
+ * src/sawsim/saw2d/saw3d/assembly.py:230).
+ *   pos_m   : n_nodes x 2 (Q9) or x 3 (Hex27) coordinates in metres
+ *   conn    : n_elem x 9 (Q9) or x 27 (Hex27) 0-based node ids
+ *   elem_mat: n_elem material indices
+ */
+int ss_set_mesh(ss_handle *h, int element_kind, int64_t n_nodes, const double *pos_m,
+                int64_t n_elem, const int64_t *conn, const int32_t *elem_mat);
+
+/*
+ * Materials in device axes (already rotated).  Complex interleaved:
+ * C: n_mat x 6 x 6 x 2, e: n_mat x 3 x 6 x 2, eps: n_mat x 3 x 3 x 2; rho real.
+ * For SS_Q9_ME0 pass the zero-lifted full tensors, as piezo_fem.py:389-401 does.
+ * `which` = SS_MAT_K for the stiffness/mass materials, SS_MAT_D for the Rayleigh
+ * damping materials (solver.py:109-115).
+ */
+int ss_set_materials(ss_handle *h, int which, int n_mat, const double *rho,
+                     const double *C, const double *e, const double *eps);
+
+/*
+ * PML regions (piezo_fem.py:192-242 for Q9, saw3d/assembly.py:127-143 for Hex27).
+ * Region r stretches axis a (bit a of axis_mask[r]) by
+ *   alpha = 1 + dmax*(1 - ((c - outer)/(inner - outer))^2)^npow / (i omega_top)
+ * with c the element's centre-node coordinate; `clip` clamps the ratio to [0,1]
+ * (the Q9 form clamps, the Hex27 form does not).  elem_region[e] = -1 for none.
+ * inner/outer: n_regions x 3.
+ */
+int ss_set_pml(ss_handle *h, int n_regions, const int32_t *axis_mask, const double *dmax,
+               const int32_t *npow, const double *inner, const double *outer, int clip,
+               const int32_t *elem_region, double omega_top);
+
+/*
+ * Boundary sets (sweep.py:41-72 / saw3d/boundary.py:84-148).
+ * merge groups as CSR: group g = group_dofs[group_ptr[g] .. group_ptr[g+1]),
+ * first entry the master (sweep.py:97-144).  For the Hex27 two-stage fold pass
+ * the front/back groups first and then the left/right groups with
+ * `two_stage` = number of groups in the first stage (bc_solve.py:25-44); 0 for
+ * the single union-find fold.
+ */
+int ss_set_bc(ss_handle *h, int64_t gdof, int64_t n_fix, const int64_t *fix,
+              int64_t n_zheng, const int64_t *zheng, int64_t n_fu, const int64_t *fu,
+              int64_t n_groups, const int64_t *group_ptr, const int64_t *group_dofs,
+              int64_t two_stage);
+
+/* Drop-in input: an already assembled global matrix (what FrequencySolver
+ * receives, sweep.py:283).  Complex interleaved values. */
+int ss_set_csr(ss_handle *h, int which, int64_t n, const int64_t *indptr,
+               const int64_t *indices, const double *vals);
+
+/* GPU assembly of K and M (and D when damping materials were set). */
+int ss_assemble(ss_handle *h);
+
+/*
+ * Copy a matrix to host.  Call with vals == NULL to get sizes in *nnz.
+ * indptr: n+1, indices: nnz, vals: 2*nnz.  For SS_MAT_KC/MC the order is the
+ * reference's active-DOF order (sweep.py:308-309) on the structural pattern.
+ */
+int ss_export_csr(ss_handle *h, int which, int64_t *n, int64_t *nnz, int64_t *indptr,
+                  int64_t *indices, double *vals);
+
+/* Condensation maps, fill-reducing ordering and symbolic factorisation (host). */
+int ss_analyze(ss_handle *h);
+
+/* Rayleigh stiffness damping A = K + i w beta D - w^2 M (sweep.py:316-323). */
+int ss_set_damping(ss_handle *h, double beta);
+
+/*
+ * Sweep n_f angular frequencies at drive voltage V (FrequencySolver.solve,
+ * sweep.py:335-364, for every point; charge_stream, frequency_tasks.py:33).
+ * Q: n_f x 2 reaction charges (the reference's Q = kts . disp).
+ * status: n_f per-point status (0 ok); iters: n_f refinement steps (may be NULL).
+ */
+int ss_sweep(ss_handle *h, int n_f, const double *omega, double V, int precision,
+             double *Q, int *status, int *iters);
+
+/* Full DOF vector at one frequency (fields.npz, solver.py:131-140): gdof x 2. */
+int ss_solve_fields(ss_handle *h, double omega, double V, double *disp);
+
+/*
+ * Counters of the last calls: out[0..n) filled with
+ *  0 n_active, 1 n_fronts, 2 max_front, 3 factor_flops_per_point (complex fronts,
+ *  8 real flops per complex multiply-add), 4 nnz(L+U), 5 analyze_s, 6 assemble_ms,
+ *  7 sweep_ms, 8 factor_ms, 9 solve_ms, 10 chunk, 11 schur_gemm_ms,
+ *  12 schur_gemm_flops, 13 levels, 14 perturbed pivots, 15 kernel launches.
+ */
+int ss_stats(const ss_handle *h, double *out, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

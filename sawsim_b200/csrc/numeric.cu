@@ -1,0 +1,1041 @@
+// Numeric phase of the sweep: Bloch condensation on the device, equilibration,
+// batched multifrontal LU of A(w) = Kc - w^2 Mc (+ i w beta Dc) over a chunk of
+// frequencies that share one symbolic analysis, triangular solves, FP64
+// iterative refinement and the electrode charge Q.
+//
+// Reference semantics (src/sawsim/saw2d/sweep.py:335-364): per frequency
+//   rhs = -(Km_s - w^2 Mm_s (+ i w beta Dm_s))[active] V,  A = Km_aa - w^2 Mm_aa,
+//   disp[active] = A^-1 rhs, slaves <- masters, zheng <- V, fu <- 0, Q = kts . disp.
+// Here Q = kq . x + V * Qz with kq the charge row folded onto the active DOFs.
+#include "ss_internal.h"
+#include "dev_complex.cuh"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+
+namespace ss {
+
+// ------------------------------------------------------------------ gathers
+// out[t] = sum of src[list[ptr[t] .. ptr[t+1])] in list order (fixed order)
+__global__ void gather_sum_kernel(int64_t n, const int64_t *__restrict__ ptr, const int64_t *__restrict__ list,
+                                  const cd *__restrict__ src, cd *__restrict__ out) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  cd acc{0.0, 0.0};
+  for (int64_t q = ptr[t]; q < ptr[t + 1]; ++q) acc = acc + src[list[q]];
+  out[t] = acc;
+}
+
+// ------------------------------------------------------------------ equilibration
+// Ruiz scaling of |Kc| + w2 |Mc| (+ wb |Dc|): rows then columns to unit max norm.
+__global__ void row_absmax_kernel(int64_t n, const int64_t *__restrict__ rp, const int64_t *__restrict__ ci,
+                                  const cd *__restrict__ K, const cd *__restrict__ M, const cd *__restrict__ D,
+                                  double w2, double wb, const double *__restrict__ rs,
+                                  const double *__restrict__ cs, double *__restrict__ rmax,
+                                  unsigned long long *__restrict__ cmax) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  double m = 0.0;
+  for (int64_t t = rp[r]; t < rp[r + 1]; ++t) {
+    const int64_t c = ci[t];
+    double a = sqrt(cabs2(K[t])) + w2 * sqrt(cabs2(M[t]));
+    if (D) a += wb * sqrt(cabs2(D[t]));
+    a *= rs[r] * cs[c];
+    m = fmax(m, a);
+    if (cmax) atomicMax(&cmax[c], (unsigned long long)__double_as_longlong(a));
+  }
+  rmax[r] = m;
+}
+
+__global__ void scale_update_kernel(int64_t n, double *__restrict__ s, const double *__restrict__ mx,
+                                    const unsigned long long *__restrict__ cmx) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const double m = cmx ? __longlong_as_double((long long)cmx[r]) : mx[r];
+  if (m > 0.0) s[r] /= sqrt(m);
+}
+
+// scaled copy: A'[t] = rs[r] * A[t] * cs[c]
+__global__ void scale_csr_kernel(int64_t n, const int64_t *__restrict__ rp, const int64_t *__restrict__ ci,
+                                 const double *__restrict__ rs, const double *__restrict__ cs,
+                                 const cd *__restrict__ in, cd *__restrict__ out) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  for (int64_t t = rp[r]; t < rp[r + 1]; ++t) out[t] = in[t] * (rs[r] * cs[ci[t]]);
+}
+
+// ------------------------------------------------------------------ vectors
+// scaled right-hand sides for a chunk: b[f][R] = -V rs[R] (ks - w^2 ms + i w beta ds)[R]
+__global__ void rhs_kernel(int64_t n, int nb, const double *__restrict__ omega, double V, double beta,
+                           const cd *__restrict__ ks, const cd *__restrict__ ms, const cd *__restrict__ ds,
+                           const double *__restrict__ rs, cd *__restrict__ b) {
+  const int64_t R = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int f = blockIdx.y;
+  if (R >= n || f >= nb) return;
+  const double w = omega[f];
+  cd v = ks[R] - ms[R] * (w * w);
+  if (ds) v = v + cmul(cd{0.0, w * beta}, ds[R]);
+  b[(int64_t)f * n + R] = v * (-V * rs[R]);
+}
+
+// Q[f] = sum_R kq[R] cs[R] x[f][R] + V Qz, one block per frequency, fixed-order tree
+__global__ void charge_kernel(int64_t n, const cd *__restrict__ kq, const double *__restrict__ cs,
+                              const cd *__restrict__ x, const cd *__restrict__ Qz, double V, cd *__restrict__ Q) {
+  __shared__ cd red[256];
+  const int f = blockIdx.x;
+  cd acc{0.0, 0.0};
+  for (int64_t R = threadIdx.x; R < n; R += blockDim.x)
+    acc = acc + cmul(kq[R] * cs[R], x[(int64_t)f * n + R]);
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) Q[f] = red[0] + Qz[0] * V;
+}
+
+// r[f] = b[f] - A'(w_f) x[f]   (scaled system, FP64), and per-row |r|, |x| maxima
+__global__ void residual_kernel(int64_t n, int nb, const int64_t *__restrict__ rp, const int64_t *__restrict__ ci,
+                                const cd *__restrict__ K, const cd *__restrict__ M, const cd *__restrict__ D,
+                                const double *__restrict__ omega, double beta, const cd *__restrict__ b,
+                                const cd *__restrict__ x, cd *__restrict__ r) {
+  const int64_t R = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int f = blockIdx.y;
+  if (R >= n || f >= nb) return;
+  const double w = omega[f], w2 = w * w;
+  const cd *xf = x + (int64_t)f * n;
+  cd acc = b[(int64_t)f * n + R];
+  for (int64_t t = rp[R]; t < rp[R + 1]; ++t) {
+    cd a = K[t] - M[t] * w2;
+    if (D) a = a + cmul(cd{0.0, w * beta}, D[t]);
+    acc = acc - cmul(a, xf[ci[t]]);
+  }
+  r[(int64_t)f * n + R] = acc;
+}
+
+}  // namespace ss
+
+namespace ss {
+
+// Everything a front kernel needs; device pointers.
+template <class T>
+struct FrontArgs {
+  const int *fronts;                 // front ids of this launch
+  const int *k, *m, *ld;
+  const int64_t *off, *p0;
+  const int64_t *rows_ptr, *rows;    // front row lists (new indices)
+  const int64_t *child_ptr;
+  const int *child;
+  const int64_t *relpos_ptr;
+  const int *relpos;
+  const int64_t *arrow_ptr;
+  const int32_t *arrow_pos;
+  const int64_t *arrow_slot;
+  const cd *Kc, *Mc, *Dc;            // scaled condensed values (new order)
+  double beta;
+  const double *omega;               // chunk frequencies
+  cplx<T> *arena;                    // fronts of frequency f at arena + f * stride
+  int64_t stride;
+  int *piv;                          // piv[f * n + p0 + j] = local pivot row
+  int64_t n;
+  T tiny;                            // static pivot perturbation threshold
+  int *nperturb;
+};
+
+template <class T>
+__device__ inline cplx<T> to_t(cd v) { return cplx<T>{(T)v.x, (T)v.y}; }
+
+// entry of A'(w) at a condensed slot
+__device__ inline cd a_entry(const cd *K, const cd *M, const cd *D, int64_t s, double w, double beta) {
+  cd v = K[s] - M[s] * (w * w);
+  if (D) v = v + cmul(cd{0.0, w * beta}, D[s]);
+  return v;
+}
+
+// block-wide argmax of |col| over rows [lo, hi) of a column (stride ldc); ties -> lowest row
+template <class T, class Get>
+__device__ int block_argmax(int lo, int hi, Get get, T *sv, int *si) {
+  T best = (T)-1;
+  int bi = lo;
+  for (int r = lo + threadIdx.x; r < hi; r += blockDim.x) {
+    const T v = cabs1(get(r));
+    if (v > best) best = v, bi = r;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const T ov = __shfl_down_sync(0xffffffffu, best, o);
+    const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+    if (ov > best || (ov == best && oi < bi)) best = ov, bi = oi;
+  }
+  const int wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if ((threadIdx.x & 31) == 0) sv[wid] = best, si[wid] = bi;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 1; q < nw; ++q)
+      if (sv[q] > sv[0] || (sv[q] == sv[0] && si[q] < si[0])) sv[0] = sv[q], si[0] = si[q];
+  }
+  __syncthreads();
+  const int r = si[0];
+  __syncthreads();
+  return r;
+}
+
+// Fronts small enough for shared memory: one CTA per (front, frequency) assembles
+// the front (arrowhead entries of A'(w) + extend-add of the children's update
+// blocks), eliminates its k pivots with row pivoting restricted to the k
+// fully-summed rows, and writes factors and update block to the arena.
+template <class T>
+__global__ void __launch_bounds__(256) front_small_kernel(FrontArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T> *F = reinterpret_cast<cplx<T> *>(smem_raw);
+  __shared__ T s_v[8];
+  __shared__ int s_i[8];
+  __shared__ cplx<T> s_pivot;
+  const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
+  const int k = a.k[f], m = a.m[f], ld = a.ld[f];
+  const double w = a.omega[fq];
+  cplx<T> *arena = a.arena + (int64_t)fq * a.stride;
+  for (int t = threadIdx.x; t < m * m; t += blockDim.x) F[t] = cplx<T>{0, 0};
+  __syncthreads();
+  for (int64_t q = a.arrow_ptr[f] + threadIdx.x; q < a.arrow_ptr[f + 1]; q += blockDim.x) {
+    const int pos = a.arrow_pos[q];
+    F[(pos / ld) * m + pos % ld] = to_t<T>(a_entry(a.Kc, a.Mc, a.Dc, a.arrow_slot[q], w, a.beta));
+  }
+  __syncthreads();
+  for (int64_t cc = a.child_ptr[f]; cc < a.child_ptr[f + 1]; ++cc) {
+    const int ch = a.child[cc];
+    const int kc = a.k[ch], nn = a.m[ch] - kc, ldc = a.ld[ch];
+    const cplx<T> *CB = arena + a.off[ch] + (int64_t)kc * ldc + kc;
+    const int *rel = a.relpos + a.relpos_ptr[ch];
+    for (int t = threadIdx.x; t < nn * nn; t += blockDim.x) {
+      const int i = t / nn, j = t - i * nn;
+      cplx<T> &d = F[rel[i] * m + rel[j]];
+      d = d + CB[(int64_t)i * ldc + j];
+    }
+    __syncthreads();
+  }
+  int *piv = a.piv + (int64_t)fq * a.n + a.p0[f];
+  for (int j = 0; j < k; ++j) {
+    const int p = block_argmax<T>(j, k, [&](int r) { return F[r * m + j]; }, s_v, s_i);
+    if (p != j)
+      for (int c = threadIdx.x; c < m; c += blockDim.x) {
+        const cplx<T> t = F[j * m + c];
+        F[j * m + c] = F[p * m + c];
+        F[p * m + c] = t;
+      }
+    if (threadIdx.x == 0) {
+      piv[j] = p;
+      cplx<T> pv = F[j * m + j];
+      if (cabs1(pv) < a.tiny) {
+        pv = cplx<T>{a.tiny, (T)0};
+        F[j * m + j] = pv;
+        atomicAdd(a.nperturb + fq, 1);
+      }
+      s_pivot = pv;
+    }
+    __syncthreads();
+    const cplx<T> inv = cdiv(cplx<T>{1, 0}, s_pivot);
+    for (int r = j + 1 + threadIdx.x; r < m; r += blockDim.x) F[r * m + j] = cmul(F[r * m + j], inv);
+    __syncthreads();
+    const int nr = m - j - 1;
+    for (int t = threadIdx.x; t < nr * nr; t += blockDim.x) {
+      const int r = j + 1 + t / nr, c = j + 1 + t % nr;
+      F[r * m + c] = cfms(F[r * m + c], F[r * m + j], F[j * m + c]);
+    }
+    __syncthreads();
+  }
+  cplx<T> *G = arena + a.off[f];
+  for (int t = threadIdx.x; t < m * m; t += blockDim.x) G[(int64_t)(t / m) * ld + t % m] = F[t];
+}
+
+}  // namespace ss
+
+namespace ss {
+
+constexpr int kRowChunk = 32;   // rows per CTA in the large-front assembly
+constexpr int kPanel = 16;      // panel width of the blocked partial LU
+
+// Large fronts, assembly in global memory: CTA (front, frequency, row chunk)
+// zeroes its rows, drops in the arrowhead entries of those rows, then adds the
+// children's update rows that map into them (children in order: deterministic).
+template <class T>
+__global__ void __launch_bounds__(256) front_assemble_large_kernel(FrontArgs<T> a) {
+  const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
+  const int k = a.k[f], m = a.m[f], ld = a.ld[f];
+  const int r0 = blockIdx.z * kRowChunk;
+  if (r0 >= m) return;
+  const int r1 = min(m, r0 + kRowChunk);
+  const double w = a.omega[fq];
+  cplx<T> *arena = a.arena + (int64_t)fq * a.stride;
+  cplx<T> *F = arena + a.off[f];
+  for (int t = threadIdx.x; t < (r1 - r0) * m; t += blockDim.x) {
+    const int r = r0 + t / m, c = t % m;
+    F[(int64_t)r * ld + c] = cplx<T>{0, 0};
+  }
+  __syncthreads();
+  {
+    // arrow entries are sorted by row position
+    int64_t lo = a.arrow_ptr[f], hi = a.arrow_ptr[f + 1];
+    int64_t b = lo, e = hi;
+    while (b < e) {
+      int64_t mid = (b + e) / 2;
+      if (a.arrow_pos[mid] / ld < r0) b = mid + 1; else e = mid;
+    }
+    const int64_t q0 = b;
+    e = hi;
+    while (b < e) {
+      int64_t mid = (b + e) / 2;
+      if (a.arrow_pos[mid] / ld < r1) b = mid + 1; else e = mid;
+    }
+    for (int64_t q = q0 + threadIdx.x; q < b; q += blockDim.x)
+      F[a.arrow_pos[q]] = to_t<T>(a_entry(a.Kc, a.Mc, a.Dc, a.arrow_slot[q], w, a.beta));
+  }
+  __syncthreads();
+  for (int64_t cc = a.child_ptr[f]; cc < a.child_ptr[f + 1]; ++cc) {
+    const int ch = a.child[cc];
+    const int kc = a.k[ch], nn = a.m[ch] - kc, ldc = a.ld[ch];
+    const int *rel = a.relpos + a.relpos_ptr[ch];
+    int b = 0, e = nn;
+    while (b < e) { int mid = (b + e) / 2; if (rel[mid] < r0) b = mid + 1; else e = mid; }
+    const int i0 = b;
+    e = nn;
+    while (b < e) { int mid = (b + e) / 2; if (rel[mid] < r1) b = mid + 1; else e = mid; }
+    const int i1 = b;
+    const cplx<T> *CB = arena + a.off[ch] + (int64_t)kc * ldc + kc;
+    for (int t = threadIdx.x; t < (i1 - i0) * nn; t += blockDim.x) {
+      const int i = i0 + t / nn, j = t % nn;
+      cplx<T> &d = F[(int64_t)rel[i] * ld + rel[j]];
+      d = d + CB[(int64_t)i * ldc + j];
+    }
+    __syncthreads();
+  }
+}
+
+// Unblocked LU of panel columns [j0, j1) over rows [j0, m), pivot rows from [j0, k).
+template <class T>
+__global__ void __launch_bounds__(256) front_panel_kernel(FrontArgs<T> a, int j0) {
+  __shared__ T s_v[8];
+  __shared__ int s_i[8];
+  __shared__ cplx<T> s_pivot;
+  const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
+  const int k = a.k[f], m = a.m[f], ld = a.ld[f];
+  if (j0 >= k) return;
+  const int j1 = min(k, j0 + kPanel);
+  cplx<T> *F = a.arena + (int64_t)fq * a.stride + a.off[f];
+  int *piv = a.piv + (int64_t)fq * a.n + a.p0[f];
+  for (int j = j0; j < j1; ++j) {
+    const int p = block_argmax<T>(j, k, [&](int r) { return F[(int64_t)r * ld + j]; }, s_v, s_i);
+    if (p != j)
+      for (int c = j0 + threadIdx.x; c < j1; c += blockDim.x) {
+        const cplx<T> t = F[(int64_t)j * ld + c];
+        F[(int64_t)j * ld + c] = F[(int64_t)p * ld + c];
+        F[(int64_t)p * ld + c] = t;
+      }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      piv[j] = p;
+      cplx<T> pv = F[(int64_t)j * ld + j];
+      if (cabs1(pv) < a.tiny) {
+        pv = cplx<T>{a.tiny, (T)0};
+        F[(int64_t)j * ld + j] = pv;
+        atomicAdd(a.nperturb + fq, 1);
+      }
+      s_pivot = pv;
+    }
+    __syncthreads();
+    const cplx<T> inv = cdiv(cplx<T>{1, 0}, s_pivot);
+    for (int r = j + 1 + threadIdx.x; r < m; r += blockDim.x)
+      F[(int64_t)r * ld + j] = cmul(F[(int64_t)r * ld + j], inv);
+    __syncthreads();
+    const int nc = j1 - j - 1;
+    if (nc > 0) {
+      const int nr = m - j - 1;
+      for (int t = threadIdx.x; t < nr * nc; t += blockDim.x) {
+        const int r = j + 1 + t / nc, c = j + 1 + t % nc;
+        F[(int64_t)r * ld + c] = cfms(F[(int64_t)r * ld + c], F[(int64_t)r * ld + j], F[(int64_t)j * ld + c]);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Apply the panel's row swaps to the columns outside it and solve the unit-lower
+// diagonal block into the row block U[j0:j1, j1:m).  One thread per column.
+template <class T>
+__global__ void __launch_bounds__(256) front_swap_trsm_kernel(FrontArgs<T> a, int j0) {
+  const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
+  const int k = a.k[f], m = a.m[f], ld = a.ld[f];
+  if (j0 >= k) return;
+  const int j1 = min(k, j0 + kPanel);
+  const int idx = blockIdx.z * blockDim.x + threadIdx.x;
+  if (idx >= m - (j1 - j0)) return;
+  const int c = idx < j0 ? idx : idx + (j1 - j0);
+  cplx<T> *F = a.arena + (int64_t)fq * a.stride + a.off[f];
+  const int *piv = a.piv + (int64_t)fq * a.n + a.p0[f];
+  for (int j = j0; j < j1; ++j) {
+    const int p = piv[j];
+    if (p != j) {
+      const cplx<T> t = F[(int64_t)j * ld + c];
+      F[(int64_t)j * ld + c] = F[(int64_t)p * ld + c];
+      F[(int64_t)p * ld + c] = t;
+    }
+  }
+  if (c < j1) return;
+  for (int j = j0 + 1; j < j1; ++j) {
+    cplx<T> v = F[(int64_t)j * ld + c];
+    for (int t = j0; t < j; ++t) v = cfms(v, F[(int64_t)j * ld + t], F[(int64_t)t * ld + c]);
+    F[(int64_t)j * ld + c] = v;
+  }
+}
+
+// One 64x64 output tile of C -= A B inside front f: rows [r0, rhi), cols [c0, chi),
+// contraction [kk0, kk1); A = F[:, kk], B = F[kk, :].
+struct GemmTask {
+  int f, r0, c0, rhi, chi, kk0, kk1;
+};
+
+template <class T>
+__global__ void __launch_bounds__(256) front_gemm_kernel(FrontArgs<T> a, const GemmTask *__restrict__ tasks) {
+  __shared__ cplx<T> As[16][64];
+  __shared__ cplx<T> Bs[16][64];
+  const GemmTask tk = tasks[blockIdx.x];
+  const int fq = blockIdx.y;
+  const int ld = a.ld[tk.f];
+  cplx<T> *F = a.arena + (int64_t)fq * a.stride + a.off[tk.f];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  cplx<T> acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = cplx<T>{0, 0};
+  for (int kb = tk.kk0; kb < tk.kk1; kb += 16) {
+    for (int t = threadIdx.x; t < 16 * 64; t += 256) {
+      const int kk = t & 15, rr = t >> 4;           // A tile: 64 rows x 16
+      const int r = tk.r0 + rr, q = kb + kk;
+      As[kk][rr] = (r < tk.rhi && q < tk.kk1) ? F[(int64_t)r * ld + q] : cplx<T>{0, 0};
+      const int cc = t & 63, kk2 = t >> 6;          // B tile: 16 x 64 cols
+      const int c = tk.c0 + cc, q2 = kb + kk2;
+      Bs[kk2][cc] = (c < tk.chi && q2 < tk.kk1) ? F[(int64_t)q2 * ld + c] : cplx<T>{0, 0};
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < 16; ++kk) {
+      cplx<T> av[4], bv[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) av[i] = As[kk][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) bv[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          acc[i][j].x += av[i].x * bv[j].x - av[i].y * bv[j].y;
+          acc[i][j].y += av[i].x * bv[j].y + av[i].y * bv[j].x;
+        }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int r = tk.r0 + ty + 16 * i, c = tk.c0 + tx + 16 * j;
+      if (r < tk.rhi && c < tk.chi) {
+        cplx<T> &d = F[(int64_t)r * ld + c];
+        d = d - acc[i][j];
+      }
+    }
+}
+
+}  // namespace ss
+
+namespace ss {
+
+// Forward substitution for one level: CTA per (front, frequency).  v = b[pivots] +
+// children's update vectors; apply the front's row swaps; solve L11; the update
+// rows receive v[k:m] - L21 y for the parent.  y overwrites x[pivots].
+template <class T>
+__global__ void __launch_bounds__(256) front_fwd_kernel(FrontArgs<T> a, const cd *__restrict__ b,
+                                                        cd *__restrict__ x, cplx<T> *__restrict__ wv,
+                                                        int64_t wstride) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T> *v = reinterpret_cast<cplx<T> *>(smem_raw);
+  const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
+  const int k = a.k[f], m = a.m[f], ld = a.ld[f];
+  const cplx<T> *F = a.arena + (int64_t)fq * a.stride + a.off[f];
+  const int64_t p0 = a.p0[f];
+  for (int i = threadIdx.x; i < m; i += blockDim.x)
+    v[i] = i < k ? to_t<T>(b[(int64_t)fq * a.n + p0 + i]) : cplx<T>{0, 0};
+  __syncthreads();
+  cplx<T> *w = wv + (int64_t)fq * wstride;
+  for (int64_t cc = a.child_ptr[f]; cc < a.child_ptr[f + 1]; ++cc) {
+    const int ch = a.child[cc];
+    const int nn = a.m[ch] - a.k[ch];
+    const int *rel = a.relpos + a.relpos_ptr[ch];
+    const cplx<T> *wc = w + a.relpos_ptr[ch];
+    for (int i = threadIdx.x; i < nn; i += blockDim.x) v[rel[i]] = v[rel[i]] + wc[i];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const int *piv = a.piv + (int64_t)fq * a.n + p0;
+    for (int j = 0; j < k; ++j) {
+      const int p = piv[j];
+      if (p != j) {
+        const cplx<T> t = v[j];
+        v[j] = v[p];
+        v[p] = t;
+      }
+    }
+  }
+  __syncthreads();
+  for (int j = 0; j < k - 1; ++j) {
+    const cplx<T> vj = v[j];
+    for (int r = j + 1 + threadIdx.x; r < k; r += blockDim.x) v[r] = cfms(v[r], F[(int64_t)r * ld + j], vj);
+    __syncthreads();
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int r = k + wid; r < m; r += nw) {
+    cplx<T> acc{0, 0};
+    for (int t = lane; t < k; t += 32) acc = acc + cmul(F[(int64_t)r * ld + t], v[t]);
+    for (int o = 16; o > 0; o >>= 1) {
+      acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
+      acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
+    }
+    if (lane == 0) w[a.relpos_ptr[f] + r - k] = v[r] - acc;
+  }
+  for (int i = threadIdx.x; i < k; i += blockDim.x) x[(int64_t)fq * a.n + p0 + i] = cd{(double)v[i].x, (double)v[i].y};
+}
+
+// Backward substitution for one level (levels run root first): z = y - U12 x_U,
+// then U11 back substitution; x[pivots] <- z.
+template <class T>
+__global__ void __launch_bounds__(256) front_bwd_kernel(FrontArgs<T> a, cd *__restrict__ x) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T> *z = reinterpret_cast<cplx<T> *>(smem_raw);
+  const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
+  const int k = a.k[f], m = a.m[f], ld = a.ld[f];
+  const cplx<T> *F = a.arena + (int64_t)fq * a.stride + a.off[f];
+  const int64_t p0 = a.p0[f];
+  cd *xf = x + (int64_t)fq * a.n;
+  const int64_t *rows = a.rows + a.rows_ptr[f];
+  for (int i = threadIdx.x; i < m; i += blockDim.x) z[i] = to_t<T>(i < k ? xf[p0 + i] : xf[rows[i]]);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (m > k) {
+    for (int r = wid; r < k; r += nw) {
+      cplx<T> acc{0, 0};
+      for (int c = k + lane; c < m; c += 32) acc = acc + cmul(F[(int64_t)r * ld + c], z[c]);
+      for (int o = 16; o > 0; o >>= 1) {
+        acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
+        acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
+      }
+      if (lane == 0) z[r] = z[r] - acc;
+    }
+    __syncthreads();
+  }
+  for (int j = k - 1; j >= 0; --j) {
+    const cplx<T> xj = cdiv(z[j], F[(int64_t)j * ld + j]);
+    for (int r = threadIdx.x; r < j; r += blockDim.x) z[r] = cfms(z[r], F[(int64_t)r * ld + j], xj);
+    __syncthreads();
+    if (threadIdx.x == 0) z[j] = xj;
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < k; i += blockDim.x) xf[p0 + i] = cd{(double)z[i].x, (double)z[i].y};
+}
+
+// x += dx and per-frequency max |dx|, max |x| (for the refinement stopping test)
+__global__ void axpy_norm_kernel(int64_t n, cd *__restrict__ x, const cd *__restrict__ dx,
+                                 double *__restrict__ nrm) {
+  __shared__ double s_dx[256], s_x[256];
+  const int f = blockIdx.x;
+  double mdx = 0.0, mx = 0.0;
+  for (int64_t R = threadIdx.x; R < n; R += blockDim.x) {
+    const int64_t t = (int64_t)f * n + R;
+    const cd v = x[t] + dx[t];
+    x[t] = v;
+    mdx = fmax(mdx, sqrt(cabs2(dx[t])));
+    mx = fmax(mx, sqrt(cabs2(v)));
+  }
+  s_dx[threadIdx.x] = mdx;
+  s_x[threadIdx.x] = mx;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      s_dx[threadIdx.x] = fmax(s_dx[threadIdx.x], s_dx[threadIdx.x + s]);
+      s_x[threadIdx.x] = fmax(s_x[threadIdx.x], s_x[threadIdx.x + s]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    nrm[2 * f] = s_dx[0];
+    nrm[2 * f + 1] = s_x[0];
+  }
+}
+
+}  // namespace ss
+
+namespace ss {
+
+#define SS_CK(x)                                                   \
+  do {                                                             \
+    cudaError_t e_ = (x);                                          \
+    if (e_ != cudaSuccess) return cuda_fail(h, e_, #x);            \
+  } while (0)
+
+// Per-level launch plan of the factorisation, built once after the analysis.
+struct Plan {
+  std::vector<int> small_ptr, large_ptr;   // per level offsets into fronts_small / fronts_large
+  std::vector<int> fronts_small, fronts_large;
+  std::vector<int> small_maxm;             // per level max m among small fronts
+  std::vector<int> nsteps;                 // per level panel steps of the large fronts
+  std::vector<int> maxm_large;             // per level
+  std::vector<int64_t> step_ptr;           // per (level, step): tasks of that step (flattened)
+  std::vector<int64_t> level_step0;        // first (level, step) index of level l
+  std::vector<int64_t> schur_ptr;          // per level: Schur tasks
+  std::vector<GemmTask> tasks;
+  DBuf d_small, d_large, d_tasks;
+  int small_m = 0;                         // threshold used
+  double schur_flops = 0;
+};
+
+static void add_tiles(std::vector<GemmTask> &v, int f, int r0, int r1, int c0, int c1, int k0, int k1) {
+  for (int r = r0; r < r1; r += 64)
+    for (int c = c0; c < c1; c += 64) v.push_back(GemmTask{f, r, c, r1, c1, k0, k1});
+}
+
+Plan *build_plan(Handle &h, int small_m) {
+  Symbolic &S = h.sym;
+  Plan *P = new Plan();
+  P->small_m = small_m;
+  P->small_ptr.assign(1, 0);
+  P->large_ptr.assign(1, 0);
+  P->schur_ptr.assign(1, 0);
+  P->step_ptr.assign(1, 0);
+  for (int l = 0; l < S.nlevel; ++l) {
+    int mm = 0, ml = 0, kmax = 0;
+    std::vector<int> large;
+    for (int64_t q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
+      const int f = S.level_fronts[q];
+      if (S.m[f] <= small_m) {
+        P->fronts_small.push_back(f);
+        mm = std::max(mm, S.m[f]);
+      } else {
+        large.push_back(f);
+        ml = std::max(ml, S.m[f]);
+        kmax = std::max(kmax, S.k[f]);
+      }
+    }
+    P->fronts_large.insert(P->fronts_large.end(), large.begin(), large.end());
+    P->small_ptr.push_back((int)P->fronts_small.size());
+    P->large_ptr.push_back((int)P->fronts_large.size());
+    P->small_maxm.push_back(mm);
+    P->maxm_large.push_back(ml);
+    const int ns = (kmax + kPanel - 1) / kPanel;
+    P->nsteps.push_back(ns);
+    P->level_step0.push_back((int64_t)P->step_ptr.size() - 1);
+    for (int s = 0; s < ns; ++s) {
+      const int j0 = s * kPanel;
+      for (int f : large) {
+        const int k = S.k[f], m = S.m[f];
+        if (j0 >= k) continue;
+        const int j1 = std::min(k, j0 + kPanel);
+        if (j1 < k) {
+          add_tiles(P->tasks, f, j1, k, j1, m, j0, j1);
+          add_tiles(P->tasks, f, k, m, j1, k, j0, j1);
+        }
+      }
+      P->step_ptr.push_back((int64_t)P->tasks.size());
+    }
+    P->schur_ptr.push_back((int64_t)P->tasks.size());
+  }
+  // Schur tasks appended after all step tasks (own index range per level)
+  std::vector<int64_t> sp(1, (int64_t)P->tasks.size());
+  for (int l = 0; l < S.nlevel; ++l) {
+    for (int q = P->large_ptr[l]; q < P->large_ptr[l + 1]; ++q) {
+      const int f = P->fronts_large[q], k = S.k[f], m = S.m[f];
+      if (m > k) add_tiles(P->tasks, f, k, m, k, m, 0, k);
+      P->schur_flops += 8.0 * k * (double)(m - k) * (m - k);
+    }
+    sp.push_back((int64_t)P->tasks.size());
+  }
+  P->schur_ptr = sp;
+  return P;
+}
+
+int launch_condense(Handle &h) {
+  Symbolic &S = h.sym;
+  const int64_t n = S.n;
+  // gathers in the new entry order
+  std::vector<int64_t> gp(h.c_nnz + 1, 0), gs;
+  gs.reserve(h.ag_src.size());
+  for (int64_t t = 0; t < h.c_nnz; ++t) {
+    const int64_t o = h.c_perm[t];
+    gs.insert(gs.end(), h.ag_src.begin() + h.ag_ptr[o], h.ag_src.begin() + h.ag_ptr[o + 1]);
+    gp[t + 1] = (int64_t)gs.size();
+  }
+  std::vector<int64_t> vp(2 * n + 1, 0), vs;
+  for (int w = 0; w < 2; ++w)
+    for (int64_t R = 0; R < n; ++R) {
+      const int64_t P = S.act_of_new[R] + w * n;
+      vs.insert(vs.end(), h.vg_src.begin() + h.vg_ptr[P], h.vg_src.begin() + h.vg_ptr[P + 1]);
+      vp[w * n + R + 1] = (int64_t)vs.size();
+    }
+  std::vector<int64_t> qp = {0, (int64_t)h.qz_src.size()};
+  DBuf dvp, dvs, dqp, dqs;
+  SS_CK(dupload(h.dc_ptr, h.c_ptr));
+  SS_CK(dupload(h.dc_idx, h.c_idx));
+  SS_CK(dupload(h.dg_ptr, gp));
+  SS_CK(dupload(h.dg_src, gs));
+  SS_CK(dupload(dvp, vp));
+  SS_CK(dupload(dvs, vs));
+  SS_CK(dupload(dqp, qp));
+  SS_CK(dupload(dqs, h.qz_src));
+  const size_t cb = (size_t)h.c_nnz * sizeof(cd);
+  SS_CK(dalloc(h.dKc, cb));
+  SS_CK(dalloc(h.dMc, cb));
+  SS_CK(dalloc(h.dks, 2 * n * sizeof(cd)));   // ks | kq
+  SS_CK(dalloc(h.dms, n * sizeof(cd)));
+  SS_CK(dalloc(h.dQz, sizeof(cd)));
+  const unsigned gb = (unsigned)((h.c_nnz + 255) / 256), vb = (unsigned)((n + 255) / 256);
+  gather_sum_kernel<<<gb, 256, 0, h.stream>>>(h.c_nnz, h.dg_ptr.as<int64_t>(), h.dg_src.as<int64_t>(), h.dK.as<cd>(), h.dKc.as<cd>());
+  gather_sum_kernel<<<gb, 256, 0, h.stream>>>(h.c_nnz, h.dg_ptr.as<int64_t>(), h.dg_src.as<int64_t>(), h.dM.as<cd>(), h.dMc.as<cd>());
+  gather_sum_kernel<<<(unsigned)((2 * n + 255) / 256), 256, 0, h.stream>>>(2 * n, dvp.as<int64_t>(), dvs.as<int64_t>(), h.dK.as<cd>(), h.dks.as<cd>());
+  gather_sum_kernel<<<vb, 256, 0, h.stream>>>(n, dvp.as<int64_t>(), dvs.as<int64_t>(), h.dM.as<cd>(), h.dms.as<cd>());
+  gather_sum_kernel<<<1, 256, 0, h.stream>>>(1, dqp.as<int64_t>(), dqs.as<int64_t>(), h.dK.as<cd>(), h.dQz.as<cd>());
+  if (h.have_D) {
+    SS_CK(dalloc(h.dDc, cb));
+    SS_CK(dalloc(h.dds, n * sizeof(cd)));
+    gather_sum_kernel<<<gb, 256, 0, h.stream>>>(h.c_nnz, h.dg_ptr.as<int64_t>(), h.dg_src.as<int64_t>(), h.dD.as<cd>(), h.dDc.as<cd>());
+    gather_sum_kernel<<<vb, 256, 0, h.stream>>>(n, dvp.as<int64_t>(), dvs.as<int64_t>(), h.dD.as<cd>(), h.dds.as<cd>());
+  }
+  SS_CK(cudaGetLastError());
+  SS_CK(cudaStreamSynchronize(h.stream));
+  // symbolic arrays
+  SS_CK(dupload(h.d_k, S.k));
+  SS_CK(dupload(h.d_m, S.m));
+  SS_CK(dupload(h.d_ld, S.ld));
+  SS_CK(dupload(h.d_off, S.off));
+  SS_CK(dupload(h.d_p0, S.p0));
+  SS_CK(dupload(h.d_rows_ptr, S.rows_ptr));
+  SS_CK(dupload(h.d_rows, S.rows));
+  SS_CK(dupload(h.d_child_ptr, S.child_ptr));
+  SS_CK(dupload(h.d_child, S.child));
+  SS_CK(dupload(h.d_relpos_ptr, S.relpos_ptr));
+  SS_CK(dupload(h.d_relpos, S.relpos));
+  SS_CK(dupload(h.d_arrow_ptr, S.arrow_ptr));
+  SS_CK(dupload(h.d_arrow_pos, S.arrow_pos));
+  SS_CK(dupload(h.d_arrow_slot, S.arrow_slot));
+  SS_CK(dupload(h.d_level_fronts, S.level_fronts));
+  return SS_OK;
+}
+
+}  // namespace ss
+
+namespace ss {
+
+template <class T>
+static int small_limit() { return sizeof(T) == 8 ? 128 : 96; }  // cf: 128^2*8, cd: 96^2*16 bytes
+
+// equilibration at angular frequency w (Ruiz, 3 sweeps)
+static int equilibrate(Handle &h, double w) {
+  const int64_t n = h.sym.n;
+  const unsigned nb = (unsigned)((n + 255) / 256);
+  SS_CK(dalloc(h.drow_scale, n * sizeof(double)));
+  SS_CK(dalloc(h.dcol_scale, n * sizeof(double)));
+  DBuf rmax, cmax;
+  SS_CK(dalloc(rmax, n * sizeof(double)));
+  SS_CK(dalloc(cmax, n * sizeof(unsigned long long)));
+  std::vector<double> ones(n, 1.0);
+  SS_CK(cudaMemcpy(h.drow_scale.p, ones.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+  SS_CK(cudaMemcpy(h.dcol_scale.p, ones.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+  const cd *D = h.have_D && h.beta ? h.dDc.as<cd>() : nullptr;
+  for (int it = 0; it < 3; ++it) {
+    row_absmax_kernel<<<nb, 256, 0, h.stream>>>(n, h.dc_ptr.as<int64_t>(), h.dc_idx.as<int64_t>(), h.dKc.as<cd>(),
+                                                h.dMc.as<cd>(), D, w * w, w * h.beta, h.drow_scale.as<double>(),
+                                                h.dcol_scale.as<double>(), rmax.as<double>(), nullptr);
+    scale_update_kernel<<<nb, 256, 0, h.stream>>>(n, h.drow_scale.as<double>(), rmax.as<double>(), nullptr);
+    SS_CK(cudaMemsetAsync(cmax.p, 0, n * sizeof(unsigned long long), h.stream));
+    row_absmax_kernel<<<nb, 256, 0, h.stream>>>(n, h.dc_ptr.as<int64_t>(), h.dc_idx.as<int64_t>(), h.dKc.as<cd>(),
+                                                h.dMc.as<cd>(), D, w * w, w * h.beta, h.drow_scale.as<double>(),
+                                                h.dcol_scale.as<double>(), rmax.as<double>(),
+                                                cmax.as<unsigned long long>());
+    scale_update_kernel<<<nb, 256, 0, h.stream>>>(n, h.dcol_scale.as<double>(), nullptr,
+                                                  cmax.as<unsigned long long>());
+  }
+  const size_t cb = (size_t)h.c_nnz * sizeof(cd);
+  SS_CK(dalloc(h.dKs, cb));
+  SS_CK(dalloc(h.dMs, cb));
+  scale_csr_kernel<<<nb, 256, 0, h.stream>>>(n, h.dc_ptr.as<int64_t>(), h.dc_idx.as<int64_t>(),
+                                             h.drow_scale.as<double>(), h.dcol_scale.as<double>(), h.dKc.as<cd>(),
+                                             h.dKs.as<cd>());
+  scale_csr_kernel<<<nb, 256, 0, h.stream>>>(n, h.dc_ptr.as<int64_t>(), h.dc_idx.as<int64_t>(),
+                                             h.drow_scale.as<double>(), h.dcol_scale.as<double>(), h.dMc.as<cd>(),
+                                             h.dMs.as<cd>());
+  if (h.have_D) {
+    SS_CK(dalloc(h.dDs, cb));
+    scale_csr_kernel<<<nb, 256, 0, h.stream>>>(n, h.dc_ptr.as<int64_t>(), h.dc_idx.as<int64_t>(),
+                                               h.drow_scale.as<double>(), h.dcol_scale.as<double>(),
+                                               h.dDc.as<cd>(), h.dDs.as<cd>());
+  }
+  SS_CK(cudaGetLastError());
+  h.scale_w = w;
+  return SS_OK;
+}
+
+template <class T>
+struct Sweeper {
+  Handle &h;
+  Plan &P;
+  FrontArgs<T> a{};
+  int64_t wstride = 0;
+  int launches = 0;
+  explicit Sweeper(Handle &hh, Plan &pp) : h(hh), P(pp) {}
+
+  int factor(int nb) {
+    const Symbolic &S = h.sym;
+    for (int l = 0; l < S.nlevel; ++l) {
+      const int ns = P.small_ptr[l + 1] - P.small_ptr[l];
+      if (ns) {
+        FrontArgs<T> b = a;
+        b.fronts = P.d_small.as<int>() + P.small_ptr[l];
+        const int mm = P.small_maxm[l];
+        front_small_kernel<T><<<dim3(ns, nb), 256, (size_t)mm * mm * sizeof(cplx<T>), h.stream>>>(b);
+        ++launches;
+      }
+      const int nl = P.large_ptr[l + 1] - P.large_ptr[l];
+      if (!nl) continue;
+      FrontArgs<T> b = a;
+      b.fronts = P.d_large.as<int>() + P.large_ptr[l];
+      const int ml = P.maxm_large[l];
+      front_assemble_large_kernel<T><<<dim3(nl, nb, (ml + kRowChunk - 1) / kRowChunk), 256, 0, h.stream>>>(b);
+      ++launches;
+      for (int s = 0; s < P.nsteps[l]; ++s) {
+        const int j0 = s * kPanel;
+        front_panel_kernel<T><<<dim3(nl, nb), 256, 0, h.stream>>>(b, j0);
+        front_swap_trsm_kernel<T><<<dim3(nl, nb, (ml + 255) / 256), 256, 0, h.stream>>>(b, j0);
+        const int64_t q = P.level_step0[l] + s;
+        const int64_t t0 = P.step_ptr[q], t1 = P.step_ptr[q + 1];
+        if (t1 > t0)
+          front_gemm_kernel<T><<<dim3((unsigned)(t1 - t0), nb), 256, 0, h.stream>>>(b, P.d_tasks.as<GemmTask>() + t0);
+        launches += 2 + (t1 > t0);
+      }
+      const int64_t t0 = P.schur_ptr[l], t1 = P.schur_ptr[l + 1];
+      if (t1 > t0) {
+        front_gemm_kernel<T><<<dim3((unsigned)(t1 - t0), nb), 256, 0, h.stream>>>(b, P.d_tasks.as<GemmTask>() + t0);
+        ++launches;
+      }
+    }
+    SS_CK(cudaGetLastError());
+    return SS_OK;
+  }
+
+  // x <- A'^-1 b for nb frequencies (x may alias nothing; wv workspace)
+  int solve(int nb, const cd *b, cd *x, cplx<T> *wv) {
+    const Symbolic &S = h.sym;
+    const size_t sm = (size_t)S.max_m * sizeof(cplx<T>);
+    for (int l = 0; l < S.nlevel; ++l) {
+      FrontArgs<T> c = a;
+      c.fronts = h.d_level_fronts.as<int>() + S.level_ptr[l];
+      const int nf = (int)(S.level_ptr[l + 1] - S.level_ptr[l]);
+      front_fwd_kernel<T><<<dim3(nf, nb), 256, sm, h.stream>>>(c, b, x, wv, wstride);
+      ++launches;
+    }
+    for (int l = S.nlevel - 1; l >= 0; --l) {
+      FrontArgs<T> c = a;
+      c.fronts = h.d_level_fronts.as<int>() + S.level_ptr[l];
+      const int nf = (int)(S.level_ptr[l + 1] - S.level_ptr[l]);
+      front_bwd_kernel<T><<<dim3(nf, nb), 256, sm, h.stream>>>(c, x);
+      ++launches;
+    }
+    SS_CK(cudaGetLastError());
+    return SS_OK;
+  }
+};
+
+}  // namespace ss
+
+namespace ss {
+
+template <class T>
+static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double *Qout, int *status,
+                      int *iters, double *disp) {
+  Symbolic &S = h.sym;
+  const int64_t n = S.n;
+  const int pi = sizeof(T) == 8 ? 0 : 1;
+  if (!h.plan[pi]) {
+    Plan *P = build_plan(h, small_limit<T>());
+    h.plan[pi] = P;
+    SS_CK(dupload(P->d_small, P->fronts_small));
+    SS_CK(dupload(P->d_large, P->fronts_large));
+    SS_CK(dupload(P->d_tasks, P->tasks));
+    SS_CK(cudaFuncSetAttribute(front_small_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               small_limit<T>() * small_limit<T>() * (int)sizeof(cplx<T>)));
+  }
+  Plan &P = *static_cast<Plan *>(h.plan[pi]);
+  double wmax = 0;
+  for (int i = 0; i < n_f; ++i) wmax = std::max(wmax, std::fabs(omega[i]));
+  if (h.scale_w != wmax) {
+    int rc = equilibrate(h, wmax);
+    if (rc) return rc;
+  }
+  const int64_t W = S.relpos_ptr[S.nfront];
+  const double per = (double)S.arena * sizeof(cplx<T>) + n * 4.0 + W * (double)sizeof(cplx<T>) + n * 64.0 + 256;
+  size_t fr = 0, tot = 0;
+  SS_CK(cudaMemGetInfo(&fr, &tot));
+  int B = (int)std::max(1.0, std::min((double)n_f, std::min(256.0, (0.85 * (double)fr - 512e6) / per)));
+  DBuf arena, piv, wv, b, x, r, dx, dom, npert, nrm, dQ;
+  SS_CK(dalloc(arena, (size_t)B * S.arena * sizeof(cplx<T>)));
+  SS_CK(dalloc(piv, (size_t)B * n * sizeof(int)));
+  SS_CK(dalloc(wv, (size_t)B * std::max<int64_t>(W, 1) * sizeof(cplx<T>)));
+  SS_CK(dalloc(b, (size_t)B * n * sizeof(cd)));
+  SS_CK(dalloc(x, (size_t)B * n * sizeof(cd)));
+  SS_CK(dalloc(r, (size_t)B * n * sizeof(cd)));
+  SS_CK(dalloc(dx, (size_t)B * n * sizeof(cd)));
+  SS_CK(dalloc(dom, B * sizeof(double)));
+  SS_CK(dalloc(npert, B * sizeof(int)));
+  SS_CK(dalloc(nrm, 2 * B * sizeof(double)));
+  SS_CK(dalloc(dQ, B * sizeof(cd)));
+  Sweeper<T> sw(h, P);
+  FrontArgs<T> &a = sw.a;
+  a.k = h.d_k.as<int>();
+  a.m = h.d_m.as<int>();
+  a.ld = h.d_ld.as<int>();
+  a.off = h.d_off.as<int64_t>();
+  a.p0 = h.d_p0.as<int64_t>();
+  a.rows_ptr = h.d_rows_ptr.as<int64_t>();
+  a.rows = h.d_rows.as<int64_t>();
+  a.child_ptr = h.d_child_ptr.as<int64_t>();
+  a.child = h.d_child.as<int>();
+  a.relpos_ptr = h.d_relpos_ptr.as<int64_t>();
+  a.relpos = h.d_relpos.as<int>();
+  a.arrow_ptr = h.d_arrow_ptr.as<int64_t>();
+  a.arrow_pos = h.d_arrow_pos.as<int32_t>();
+  a.arrow_slot = h.d_arrow_slot.as<int64_t>();
+  const bool damp = h.have_D && h.beta != 0.0;
+  a.Kc = h.dKs.as<cd>();
+  a.Mc = h.dMs.as<cd>();
+  a.Dc = damp ? h.dDs.as<cd>() : nullptr;
+  a.beta = h.beta;
+  a.omega = dom.as<double>();
+  a.arena = arena.as<cplx<T>>();
+  a.stride = S.arena;
+  a.piv = piv.as<int>();
+  a.n = n;
+  a.tiny = sizeof(T) == 8 ? (T)1e-13 : (T)1e-6;
+  a.nperturb = npert.as<int>();
+  sw.wstride = W;
+  const int maxit = sizeof(T) == 8 ? 2 : 40;
+  const double tol = sizeof(T) == 8 ? 1e-15 : 1e-12;
+  cudaEvent_t e0, e1, e2;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventCreate(&e2);
+  double fac_ms = 0, sol_ms = 0;
+  std::vector<double> hn(2 * B);
+  std::vector<int> hp(B), hit(B);
+  std::vector<char> conv(B);
+  const unsigned vb = (unsigned)((n + 255) / 256);
+  auto t_start = std::chrono::steady_clock::now();
+  int perturbed = 0;
+  for (int c0 = 0; c0 < n_f; c0 += B) {
+    const int nb = std::min(B, n_f - c0);
+    SS_CK(cudaMemcpyAsync(dom.p, omega + c0, nb * sizeof(double), cudaMemcpyHostToDevice, h.stream));
+    SS_CK(cudaMemsetAsync(npert.p, 0, nb * sizeof(int), h.stream));
+    rhs_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, dom.as<double>(), V, h.beta, h.dks.as<cd>(),
+                                                   h.dms.as<cd>(), damp ? h.dds.as<cd>() : nullptr,
+                                                   h.drow_scale.as<double>(), b.as<cd>());
+    cudaEventRecord(e0, h.stream);
+    int rc = sw.factor(nb);
+    if (rc) return rc;
+    cudaEventRecord(e1, h.stream);
+    rc = sw.solve(nb, b.as<cd>(), x.as<cd>(), wv.as<cplx<T>>());
+    if (rc) return rc;
+    cudaEventRecord(e2, h.stream);
+    SS_CK(cudaEventSynchronize(e2));
+    float ms1 = 0, ms2 = 0;
+    cudaEventElapsedTime(&ms1, e0, e1);
+    cudaEventElapsedTime(&ms2, e1, e2);
+    fac_ms += ms1;
+    sol_ms += ms2;
+    std::fill(conv.begin(), conv.end(), 0);
+    std::fill(hit.begin(), hit.end(), 0);
+    for (int it = 0; it < maxit; ++it) {
+      residual_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, h.dc_ptr.as<int64_t>(), h.dc_idx.as<int64_t>(),
+                                                          a.Kc, a.Mc, a.Dc, dom.as<double>(), h.beta, b.as<cd>(),
+                                                          x.as<cd>(), r.as<cd>());
+      rc = sw.solve(nb, r.as<cd>(), dx.as<cd>(), wv.as<cplx<T>>());
+      if (rc) return rc;
+      axpy_norm_kernel<<<nb, 256, 0, h.stream>>>(n, x.as<cd>(), dx.as<cd>(), nrm.as<double>());
+      SS_CK(cudaMemcpyAsync(hn.data(), nrm.p, 2 * nb * sizeof(double), cudaMemcpyDeviceToHost, h.stream));
+      SS_CK(cudaStreamSynchronize(h.stream));
+      bool all = true;
+      for (int f = 0; f < nb; ++f) {
+        if (!conv[f]) {
+          ++hit[f];
+          conv[f] = hn[2 * f] <= tol * hn[2 * f + 1];
+        }
+        all = all && conv[f];
+      }
+      if (all) break;
+    }
+    charge_kernel<<<nb, 256, 0, h.stream>>>(n, h.dks.as<cd>() + n, h.dcol_scale.as<double>(), x.as<cd>(),
+                                            h.dQz.as<cd>(), V, dQ.as<cd>());
+    SS_CK(cudaGetLastError());
+    SS_CK(cudaMemcpyAsync(Qout + 2 * (int64_t)c0, dQ.p, nb * sizeof(cd), cudaMemcpyDeviceToHost, h.stream));
+    SS_CK(cudaMemcpyAsync(hp.data(), npert.p, nb * sizeof(int), cudaMemcpyDeviceToHost, h.stream));
+    SS_CK(cudaStreamSynchronize(h.stream));
+    for (int f = 0; f < nb; ++f) {
+      perturbed += hp[f];
+      if (status) status[c0 + f] = (sizeof(T) == 4 && !conv[f]) ? SS_ENOCONV : SS_OK;
+      if (iters) iters[c0 + f] = hit[f];
+    }
+    if (disp) {
+      std::vector<cd> y(n);
+      std::vector<double> cs(n);
+      SS_CK(cudaMemcpy(y.data(), x.p, n * sizeof(cd), cudaMemcpyDeviceToHost));
+      SS_CK(cudaMemcpy(cs.data(), h.dcol_scale.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+      std::vector<cd> pre(h.gdof, cd{0, 0});
+      for (int64_t Pa = 0; Pa < n; ++Pa) {
+        const int64_t R = S.new_of_act[Pa];
+        pre[h.active[Pa]] = y[R] * cs[R];
+      }
+      for (int64_t i = 0; i < h.gdof; ++i) {
+        const cd v = pre[h.rep[i]];
+        disp[2 * i] = v.x;
+        disp[2 * i + 1] = v.y;
+      }
+      for (int64_t d : h.zheng) disp[2 * d] = V, disp[2 * d + 1] = 0;
+      for (int64_t d : h.fu) disp[2 * d] = 0, disp[2 * d + 1] = 0;
+    }
+  }
+  const double wall = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaEventDestroy(e2);
+  h.st[7] = wall;
+  h.st[8] = fac_ms;
+  h.st[9] = sol_ms;
+  h.st[10] = B;
+  h.st[12] = P.schur_flops;
+  h.st[14] = perturbed;
+  h.st[15] = sw.launches;
+  return SS_OK;
+}
+
+int run_sweep(Handle &h, int n_f, const double *omega, double V, int precision, double *Q, int *status,
+              int *iters, double *disp_out) {
+  if (precision == SS_PREC_MIXED) return sweep_impl<float>(h, n_f, omega, V, Q, status, iters, disp_out);
+  return sweep_impl<double>(h, n_f, omega, V, Q, status, iters, disp_out);
+}
+
+}  // namespace ss
+
+namespace ss {
+void free_plans(Handle &h) {
+  for (int i = 0; i < 2; ++i) {
+    delete static_cast<Plan *>(h.plan[i]);
+    h.plan[i] = nullptr;
+  }
+}
+}  // namespace ss

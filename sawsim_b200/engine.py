@@ -1,0 +1,177 @@
+"""Python host layer of the B200 sweep backend.
+
+``FrequencySolver`` mirrors the engine the reference's pipeline builds and
+drives (``src/sawsim/saw2d/sweep.py:275-393``): ``solve(omega, V)`` returns
+``(disp, Q, |Y|)``, ``sweep(freqs, V)`` the charges, ``n_active`` the size of the
+condensed system.  Construction goes from the inputs of the reference's
+assembly (``piezo_fem.assemble``, ``piezo_fem.py:283``) and boundary builder
+(``sweep.bc_periodic``, ``sweep.py:41``), because assembly, condensation and
+every frequency's factorisation run on the GPU.  All numerical work is done by
+``libsawsim_b200.so``; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import scipy.sparse as sp
+
+from . import _lib as L
+from .materials import pack
+
+PRECISION = {'fp64': L.SS_PREC_FP64, 'mixed': L.SS_PREC_MIXED}
+
+
+class Handle:
+    """Owns one ``ss_handle``; raises ``SawsimError`` on any non-zero status."""
+
+    def __init__(self, device: int = 0):
+        self.lib = L.load()
+        self.h = C.c_void_p()
+        rc = self.lib.ss_create(C.byref(self.h), int(device))
+        if rc != L.SS_OK:
+            raise L.SawsimError(rc, 'ss_create failed (no CUDA device?)')
+
+    def __call__(self, name, *args):
+        rc = getattr(self.lib, name)(self.h, *args)
+        if rc != L.SS_OK:
+            raise L.SawsimError(rc, self.lib.ss_last_error(self.h).decode())
+        return rc
+
+    def close(self):
+        if self.h:
+            self.lib.ss_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _pml_arrays(elem_tag, pml_regions, ne):
+    """Region arrays for ss_set_pml from reference-style PMLRegion objects (piezo_fem.py:192-242)."""
+    regions = list(pml_regions or [])
+    region = np.full(ne, -1, dtype=np.int32)
+    axis, dmax, npow, inner, outer = [], [], [], [], []
+    for r, reg in enumerate(regions):
+        region[np.asarray(elem_tag) == reg.tag] = r
+        mask = (1 if 'x' in reg.kind else 0) | (2 if 'y' in reg.kind else 0)
+        axis.append(mask)
+        dmax.append(reg.dmax)
+        npow.append(reg.n)
+        inner.append([reg.xa, reg.ya, 0.0])
+        outer.append([reg.xp, reg.yp, 0.0])
+    return (len(regions), L.i32(axis), L.f64(dmax), L.i32(npow), L.f64(np.reshape(inner, (-1, 3))),
+            L.f64(np.reshape(outer, (-1, 3))), region)
+
+
+def _bc_arrays(bc):
+    fix, zheng, fu, groups = bc
+    groups = [np.asarray(g, dtype=np.int64).ravel() for g in groups]
+    gptr = np.zeros(len(groups) + 1, dtype=np.int64)
+    gptr[1:] = np.cumsum([g.size for g in groups])
+    gd = np.concatenate(groups) if groups else np.zeros(0, dtype=np.int64)
+    return L.i64(fix), L.i64(zheng), L.i64(fu), L.i64(gptr), L.i64(gd)
+
+
+class FrequencySolver:
+    """Sweep engine on one B200 with the reference engine's ``solve``/``sweep`` surface."""
+
+    def __init__(self, handle: Handle, gdof: int, ndisp: int, kind: int, zheng, fu):
+        self._h = handle
+        self.gdof = int(gdof)
+        self.ndisp = ndisp
+        self.kind = kind
+        self.zheng = np.asarray(zheng, dtype=np.int64)
+        self.fu = np.asarray(fu, dtype=np.int64)
+
+    @classmethod
+    def from_q9(cls, model, materials, mat_idx, pml_regions, omega_top, bc, mode_extension=1,
+                damping_materials=None, beta=0.0, device=0):
+        """Assemble on the GPU from the inputs of ``piezo_fem.assemble`` (ME1) or
+        ``piezo_fem.assemble_ME0`` (``mode_extension=0``, projected xy tensors) and
+        the ``(fix, zheng, fu, merge_groups)`` tuple of ``sweep.bc_periodic``."""
+        h = Handle(device)
+        ndisp = 3 if mode_extension else 2
+        kind = L.SS_Q9_ME1 if mode_extension else L.SS_Q9_ME0
+        pos = L.f64(model.pos_m[:, :2])
+        quads = L.i64(model.quads)
+        emat = L.i32(mat_idx)
+        h('ss_set_mesh', kind, pos.shape[0], L.ptr(pos, C.c_double), quads.shape[0], L.ptr(quads, C.c_int64),
+          L.ptr(emat, C.c_int32))
+        rho, Cm, em, epsm = pack(materials, ndisp)
+        h('ss_set_materials', L.SS_MAT_K, len(rho), L.ptr(rho, C.c_double), L.ptr(Cm, C.c_double),
+          L.ptr(em, C.c_double), L.ptr(epsm, C.c_double))
+        if damping_materials is not None:
+            rho, Cm, em, epsm = pack(damping_materials, ndisp)
+            h('ss_set_materials', L.SS_MAT_D, len(rho), L.ptr(rho, C.c_double), L.ptr(Cm, C.c_double),
+              L.ptr(em, C.c_double), L.ptr(epsm, C.c_double))
+        nreg, axis, dmax, npow, inner, outer, region = _pml_arrays(model.elem_tag, pml_regions, quads.shape[0])
+        h('ss_set_pml', nreg, L.ptr(axis, C.c_int32), L.ptr(dmax, C.c_double), L.ptr(npow, C.c_int32),
+          L.ptr(inner, C.c_double), L.ptr(outer, C.c_double), 1, L.ptr(region, C.c_int32), float(omega_top))
+        h('ss_assemble')
+        eng = cls(h, (ndisp + 1) * pos.shape[0], ndisp, kind, bc[1], bc[2])
+        eng._set_bc(bc, two_stage=0)
+        if damping_materials is not None and beta:
+            h('ss_set_damping', float(beta))
+        return eng
+
+    def _set_bc(self, bc, two_stage=0):
+        fix, zheng, fu, gptr, gd = _bc_arrays(bc)
+        self._h('ss_set_bc', self.gdof, fix.size, L.ptr(fix, C.c_int64), zheng.size, L.ptr(zheng, C.c_int64),
+                fu.size, L.ptr(fu, C.c_int64), gptr.size - 1, L.ptr(gptr, C.c_int64), L.ptr(gd, C.c_int64),
+                int(two_stage))
+        self._h('ss_analyze')
+
+    # ------------------------------------------------------------------ queries
+    def stats(self) -> dict:
+        out = np.zeros(16)
+        self._h('ss_stats', L.ptr(out, C.c_double), 16)
+        keys = ['n_active', 'n_fronts', 'max_front', 'factor_flops_per_point', 'nnz_lu', 'analyze_s',
+                'assemble_ms', 'sweep_ms', 'factor_ms', 'solve_ms', 'chunk', 'schur_gemm_ms',
+                'schur_gemm_flops', 'levels', 'perturbed_pivots', 'launches']
+        return dict(zip(keys, out.tolist()))
+
+    @property
+    def n_active(self) -> int:
+        return int(self.stats()['n_active'])
+
+    def export(self, which: int):
+        """Device matrix as scipy CSR (global K/M/D, or condensed KC/MC in active order)."""
+        n = C.c_int64()
+        nnz = C.c_int64()
+        self._h('ss_export_csr', which, C.byref(n), C.byref(nnz), None, None, None)
+        ip = np.zeros(n.value + 1, dtype=np.int64)
+        ix = np.zeros(nnz.value, dtype=np.int64)
+        v = np.zeros(2 * nnz.value, dtype=np.float64)
+        self._h('ss_export_csr', which, C.byref(n), C.byref(nnz), L.ptr(ip, C.c_int64), L.ptr(ix, C.c_int64),
+                L.ptr(v, C.c_double))
+        return sp.csr_matrix((v.view(np.complex128), ix, ip), shape=(n.value, n.value))
+
+    # ------------------------------------------------------------------ solves
+    def charges(self, omegas, V: float = 1.0, precision: str = 'fp64'):
+        """Batched sweep: (Q complex[n_f], status int[n_f], refinement steps int[n_f])."""
+        om = L.f64(np.atleast_1d(omegas))
+        Q = np.zeros(2 * om.size)
+        st = np.zeros(om.size, dtype=np.int32)
+        it = np.zeros(om.size, dtype=np.int32)
+        self._h('ss_sweep', om.size, L.ptr(om, C.c_double), float(V), PRECISION[precision], L.ptr(Q, C.c_double),
+                L.ptr(st, C.c_int), L.ptr(it, C.c_int))
+        return Q.view(np.complex128), st, it
+
+    def sweep(self, fre, V: float = 1.0, precision: str = 'fp64'):
+        """Charges at frequencies ``fre`` (Hz), all points in batched GPU factorisations."""
+        Q, st, _ = self.charges(2 * np.pi * np.asarray(fre, dtype=float), V, precision)
+        return Q
+
+    def solve(self, omega: float, V: float = 1.0):
+        """One point: ``(disp, Q, |Y|)`` like ``FrequencySolver.solve`` (sweep.py:335-364)."""
+        disp = np.zeros(2 * self.gdof)
+        self._h('ss_solve_fields', float(omega), float(V), L.ptr(disp, C.c_double))
+        Q, _, _ = self.charges([omega], V, 'fp64')
+        return disp.view(np.complex128), Q[0], abs(1j * omega * Q[0] / V)
+
+    def close(self):
+        self._h.close()
