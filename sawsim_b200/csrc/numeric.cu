@@ -735,7 +735,7 @@ int launch_condense(Handle &h) {
 namespace ss {
 
 template <class T>
-static int small_limit() { return sizeof(T) == 8 ? 128 : 96; }  // cf: 128^2*8, cd: 96^2*16 bytes
+static int small_limit() { return sizeof(T) == 8 ? 96 : 128; }  // cd: 96^2*16, cf: 128^2*8 bytes
 
 // equilibration at angular frequency w (Ruiz, 3 sweeps)
 static int equilibrate(Handle &h, double w) {
