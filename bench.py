@@ -1,0 +1,266 @@
+#!/usr/bin/env python
+"""Benchmark: Y11 frequency points per second on one B200.
+
+Workload: the seeded ME1 two-layer Q9 cell (3m film 0.6p / SiO2 0.3p / Si 3p /
+PML 1p, 64x256 elements, 264,708 DOF, 262k active) swept over 201 frequencies
+in 1.6-2.0 GHz.  One step = one whole sweep (all 201 points: batched
+factorisation of every point, solves, refinement, charges).  K/M assembly,
+condensation, ordering and symbolic analysis are host/device setup, done once
+before timing and reported separately.
+
+``--impl reference`` times the reference's CPU algorithm (the oracle port of
+src/sawsim/saw2d/sweep.py: real-block SciPy SuperLU per point, the route the
+reference takes without PARDISO) on this host's cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+PEAKS = REPO / 'MEASURED_PEAKS.json'
+CPU_SAMPLE = (32, 128)   # bounded CPU sample: the same cell family at half resolution per axis
+METRIC = 'Y11 points/s, 1 B200: batched FP32-TC+refine vs FP64 sweep, fr/fa within 1 kHz'
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument('--gpus', type=int, default=1)
+    p.add_argument('--steps', type=int, default=3)
+    p.add_argument('--warmup', type=int, default=3)
+    p.add_argument('--impl', default='b200', choices=['b200', 'reference'])
+    p.add_argument('--precision', default='mixed', choices=['mixed', 'fp64'])
+    p.add_argument('--case', default='me1_64x256')
+    p.add_argument('--points', type=int, default=None)
+    p.add_argument('--no-cpu-baseline', action='store_true')
+    return p.parse_args()
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def __enter__(self):
+        q = ('clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,'
+             'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,'
+             'clocks_event_reasons.sw_power_cap')
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.index), f'--query-gpu={q}',
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except FileNotFoundError:
+            self.proc = None
+            return self
+
+        def reader():
+            for line in self.proc.stdout:
+                self.samples.append([x.strip() for x in line.split(',')])
+        self._t = threading.Thread(target=reader, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        if not self.samples:
+            return dict(sm_mhz=None, sm_max_mhz=None, reasons=['unsampled'])
+        sm = [float(s[0]) for s in self.samples if s[0].replace('.', '').isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace('.', '').isdigit()]
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 3 + i and s[3 + i] == 'Active'})
+        return dict(sm_mhz=statistics.median(sm) if sm else None, sm_max_mhz=max(mx) if mx else None,
+                    reasons=reasons, samples=len(self.samples))
+
+
+def peaks():
+    try:
+        d = json.loads(PEAKS.read_text())
+        return d, 'measured'
+    except Exception:
+        return dict(hbm_gbs=6650.0, bf16_tflops=1590.0, bf16_tflops_sustained=1400.0), 'fallback'
+
+
+# ----------------------------------------------------------------------------- CPU side
+def _cpu_point(args):
+    """One frequency point of the reference algorithm (oracle port), in a worker process."""
+    case_name, cols, rows, f = args
+    os.environ.setdefault('OMP_NUM_THREADS', '1')
+    from helpers_cpu import oracle_solver_for
+    eng = oracle_solver_for(case_name, cols, rows)
+    t = time.perf_counter()
+    eng.solve(2 * np.pi * f, 1.0, route='realblock')
+    return time.perf_counter() - t
+
+
+def cpu_sweep_sample(case_name, cols, rows, npoints, workers):
+    """Points/s of the reference route on a bounded sample, `workers` spawn processes."""
+    import multiprocessing as mp
+    from sawsim_b200 import cases
+    c = cases.make_case(case_name, cols=cols, rows=rows)
+    fs = np.linspace(c.freqs[0], c.freqs[-1], npoints)
+    ctx = mp.get_context('spawn')
+    with ctx.Pool(workers, initializer=_cpu_init) as pool:
+        pool.map(_cpu_point, [(case_name, cols, rows, fs[0])] * workers)      # build per-worker engines
+        t = time.perf_counter()
+        pool.map(_cpu_point, [(case_name, cols, rows, f) for f in fs], chunksize=1)
+        dt = time.perf_counter() - t
+    ndof = c.mesh.N * (4 if c.mode_extension else 3)
+    return npoints / dt, ndof
+
+
+def _cpu_init():
+    sys.path.insert(0, str(REPO))
+    sys.path.insert(0, str(REPO / 'oracle'))
+
+
+def reference_arm(a, rank, world):
+    """Reference CPU implementation (oracle port) on this host, rank 0 only."""
+    if rank != 0:
+        return
+    workers = min(8, os.cpu_count() or 1)
+    cols, rows = CPU_SAMPLE
+    res = []
+    for i in range(a.warmup + a.steps):
+        v, ndof = cpu_sweep_sample(a.case, cols, rows, 2 * workers, workers)
+        if i >= a.warmup:
+            res.append(v)
+    value = float(np.mean(res))
+    sample = (f'{2 * workers} frequency points per step of the {a.case} cell family at reduced resolution '
+              f'{cols}x{rows} ({ndof} DOF; one full-size point takes minutes on one core), real-block SciPy '
+              f'SuperLU per point as the reference without PARDISO, {workers} spawn workers x 1 BLAS thread')
+    print(json.dumps(dict(impl='reference', metric=METRIC, value=value, unit='points/s', n_gpus=a.gpus,
+                          steps=a.steps, warmup=a.warmup, higher_is_better=True, scaling='weak', vs_baseline=None,
+                          dtype='f64', data='synthetic',
+                          config=dict(workload=f'{a.case} (reference CPU route, bounded sample)', points_per_step=2 * workers),
+                          cpu_baseline=dict(value=value, unit='points/s', cores=workers, kind='port', sample=sample),
+                          e2e=dict(value=value, unit='points/s', h2d_bytes_per_step=0, d2h_bytes_per_step=0))),
+          flush=True)
+
+
+# ----------------------------------------------------------------------------- GPU side
+def b200_arm(a, rank, world, local):
+    import torch
+    import torch.distributed as dist
+    from sawsim_b200 import cases
+    torch.cuda.set_device(local)
+    c = cases.make_case(a.case, points=a.points)
+    t0 = time.perf_counter()
+    eng = cases.engine_for(c, device=local)
+    setup_s = time.perf_counter() - t0
+    st0 = eng.stats()
+    w = 2 * np.pi * c.freqs
+    nf = w.size
+    for _ in range(a.warmup):
+        Q, status, iters = eng.charges(w, 1.0, a.precision)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    dev_ms, wall_s, schur_ms, launches = [], [], [], 0
+    barrier()
+    with Clocks(local) as clk:
+        for _ in range(a.steps):
+            t = time.perf_counter()
+            Q, status, iters = eng.charges(w, 1.0, a.precision)      # host buffers in, host Q out
+            wall_s.append(time.perf_counter() - t)
+            s = eng.stats()
+            dev_ms.append(s['sweep_device_ms'])
+            schur_ms.append(s['schur_gemm_ms'])
+            launches += int(s['launches'])
+        barrier()
+    dev = float(np.sum(dev_ms)) / 1e3
+    wall = float(np.sum(wall_s))
+    if world > 1:
+        t = torch.tensor([dev, wall], device='cuda', dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev, wall = t.tolist()
+    s = eng.stats()
+    pk, pk_kind = peaks()
+    schur_flops_launch = s['schur_gemm_flops'] / max(1.0, s['schur_launches'])
+    schur_ms_launch = float(np.mean(schur_ms)) / max(1.0, s['schur_launches'])
+    if a.precision == 'mixed':
+        peak = pk.get('bf16_tflops', 1590.0) / 2
+        peak_note = f'TF32 dense = half the {pk_kind} cuBLAS bf16 burst'
+    else:
+        peak = 37.0
+        peak_note = 'FP64 nominal 37 TFLOP/s (no FP64 figure in MEASURED_PEAKS.json)'
+    achieved = schur_flops_launch / (schur_ms_launch * 1e-3) / 1e12 if schur_ms_launch > 0 else None
+    line = None
+    if rank == 0:
+        cpu = None
+        if not a.no_cpu_baseline:
+            workers = min(8, os.cpu_count() or 1)
+            v, ndof = cpu_sweep_sample(a.case, *CPU_SAMPLE, 2 * workers, workers)
+            cpu = dict(value=v, unit='points/s', cores=workers, kind='port',
+                       sample=f'{2 * workers} points of the {a.case} family at {CPU_SAMPLE[0]}x{CPU_SAMPLE[1]} '
+                              f'({ndof} DOF, a quarter of the cell), real-block SciPy SuperLU as the reference '
+                              f'without PARDISO, {workers} spawn workers x 1 BLAS thread')
+        bad = int(np.sum(status != 0))
+        line = dict(metric=METRIC, value=world * nf * a.steps / dev, unit='points/s', n_gpus=world,
+                    steps=a.steps, warmup=a.warmup, ms_per_step=dev * 1e3 / a.steps, higher_is_better=True,
+                    scaling='weak', vs_baseline=None, dtype='c64+f64' if a.precision == 'mixed' else 'c128',
+                    data='synthetic',
+                    config=dict(workload=f'{a.case}: ME1 two-layer Q9 cell {c.info["cols"]}x{c.info["rows"]}, '
+                                         f'{nf} points 1.6-2.0 GHz, seed {c.info["seed"]}',
+                                precision=a.precision, n_active=int(st0['n_active']), fronts=int(st0['n_fronts']),
+                                factor_gflop_per_point=st0['factor_flops_per_point'] / 1e9,
+                                setup_s=setup_s, analyze_s=st0['analyze_s'], assemble_ms=st0['assemble_ms'],
+                                l2='inputs larger than L2 (front arena of GBs per chunk)',
+                                chunk=int(s['chunk']), points_not_converged=bad,
+                                mean_refinement_steps=float(np.mean(iters)), parallelism=f'replicas x{world}'),
+                    e2e=dict(value=world * nf * a.steps / wall, unit='points/s', h2d_bytes_per_step=8 * nf,
+                             d2h_bytes_per_step=16 * nf + 8 * nf),
+                    gpu_launches=launches,
+                    roofline=dict(kernel='front_gemm_kernel (Schur update F22 -= F21 F12)', bound='tensor',
+                                  achieved=achieved, peak=peak, unit='TFLOP/s',
+                                  frac=(achieved / peak) if achieved else None, traffic=None, peak_note=peak_note,
+                                  flops_per_launch=schur_flops_launch),
+                    clocks=clk.summary(), cpu_baseline=cpu)
+    return line
+
+
+def main():
+    a = parse()
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    if a.impl == 'reference':
+        reference_arm(a, rank, world)
+        return
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group('nccl', timeout=timedelta(seconds=600))
+    line = b200_arm(a, rank, world, local)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

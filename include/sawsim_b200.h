@@ -143,7 +143,9 @@ int ss_solve_fields(ss_handle *h, double omega, double V, double *disp);
  *  0 n_active, 1 n_fronts, 2 max_front, 3 factor_flops_per_point (complex fronts,
  *  8 real flops per complex multiply-add), 4 nnz(L+U), 5 analyze_s, 6 assemble_ms,
  *  7 sweep_ms, 8 factor_ms, 9 solve_ms, 10 chunk, 11 schur_gemm_ms,
- *  12 schur_gemm_flops, 13 levels, 14 perturbed pivots, 15 kernel launches.
+ *  12 schur_gemm_flops, 13 levels, 14 perturbed pivots, 15 kernel launches,
+ *  16 Schur GEMM launches, 17 device time of the last ss_sweep (ms, CUDA events),
+ *  18 refinement solves of the last ss_sweep.
  */
 int ss_stats(const ss_handle *h, double *out, int n);
 

@@ -13,6 +13,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 
 namespace ss {
 
@@ -789,8 +791,26 @@ struct Sweeper {
   Plan &P;
   FrontArgs<T> a{};
   int64_t wstride = 0;
-  int launches = 0;
-  explicit Sweeper(Handle &hh, Plan &pp) : h(hh), P(pp) {}
+  int launches = 0, schur_launches = 0;
+  std::vector<cudaEvent_t> ev;               // Schur GEMM timing, one pair per level
+  int nev = 0;
+  double schur_ms = 0;
+  explicit Sweeper(Handle &hh, Plan &pp) : h(hh), P(pp) {
+    ev.resize(2 * std::max(1, h.sym.nlevel));
+    for (auto &e : ev) cudaEventCreate(&e);
+  }
+  ~Sweeper() {
+    for (auto &e : ev) cudaEventDestroy(e);
+  }
+  // after the stream reached the end of factor(): add up the Schur GEMM time
+  void collect() {
+    for (int i = 0; i < nev; ++i) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]);
+      schur_ms += ms;
+    }
+    nev = 0;
+  }
 
   int factor(int nb) {
     const Symbolic &S = h.sym;
@@ -822,8 +842,12 @@ struct Sweeper {
       }
       const int64_t t0 = P.schur_ptr[l], t1 = P.schur_ptr[l + 1];
       if (t1 > t0) {
+        cudaEventRecord(ev[2 * nev], h.stream);
         front_gemm_kernel<T><<<dim3((unsigned)(t1 - t0), nb), 256, 0, h.stream>>>(b, P.d_tasks.as<GemmTask>() + t0);
+        cudaEventRecord(ev[2 * nev + 1], h.stream);
+        ++nev;
         ++launches;
+        ++schur_launches;
       }
     }
     SS_CK(cudaGetLastError());
@@ -937,6 +961,10 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
   std::vector<char> conv(B);
   const unsigned vb = (unsigned)((n + 255) / 256);
   auto t_start = std::chrono::steady_clock::now();
+  cudaEvent_t eall0, eall1;
+  cudaEventCreate(&eall0);
+  cudaEventCreate(&eall1);
+  cudaEventRecord(eall0, h.stream);
   int perturbed = 0;
   for (int c0 = 0; c0 < n_f; c0 += B) {
     const int nb = std::min(B, n_f - c0);
@@ -958,6 +986,7 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
     cudaEventElapsedTime(&ms2, e1, e2);
     fac_ms += ms1;
     sol_ms += ms2;
+    sw.collect();
     std::fill(conv.begin(), conv.end(), 0);
     std::fill(hit.begin(), hit.end(), 0);
     for (int it = 0; it < maxit; ++it) {
@@ -970,6 +999,8 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
       SS_CK(cudaMemcpyAsync(hn.data(), nrm.p, 2 * nb * sizeof(double), cudaMemcpyDeviceToHost, h.stream));
       SS_CK(cudaStreamSynchronize(h.stream));
       bool all = true;
+      if (getenv("SS_DEBUG_IR"))
+        fprintf(stderr, "IR it %d: dx/x f0 %.3e f_last %.3e\n", it, hn[0] / hn[1], hn[2 * (nb - 1)] / hn[2 * nb - 1]);
       for (int f = 0; f < nb; ++f) {
         if (!conv[f]) {
           ++hit[f];
@@ -1009,6 +1040,13 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
       for (int64_t d : h.fu) disp[2 * d] = 0, disp[2 * d + 1] = 0;
     }
   }
+  cudaEventRecord(eall1, h.stream);
+  cudaEventSynchronize(eall1);
+  float total_f = 0;
+  cudaEventElapsedTime(&total_f, eall0, eall1);
+  const double total_ms = total_f;
+  cudaEventDestroy(eall0);
+  cudaEventDestroy(eall1);
   const double wall = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -1017,7 +1055,10 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
   h.st[8] = fac_ms;
   h.st[9] = sol_ms;
   h.st[10] = B;
-  h.st[12] = P.schur_flops;
+  h.st[11] = sw.schur_ms;
+  h.st[12] = P.schur_flops * n_f;
+  h.st[16] = sw.schur_launches;
+  h.st[17] = total_ms;
   h.st[14] = perturbed;
   h.st[15] = sw.launches;
   return SS_OK;

@@ -117,7 +117,7 @@ struct Handle {
   DBuf dKs, dMs, dDs;                    // equilibrated condensed values
   double scale_w = -1;                   // frequency the scaling was computed at
   // stats
-  double st[16] = {0};
+  double st[24] = {0};
 };
 
 // ---------------------------------------------------------------- kernels

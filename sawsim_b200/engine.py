@@ -127,11 +127,12 @@ class FrequencySolver:
 
     # ------------------------------------------------------------------ queries
     def stats(self) -> dict:
-        out = np.zeros(16)
-        self._h('ss_stats', L.ptr(out, C.c_double), 16)
+        out = np.zeros(24)
+        self._h('ss_stats', L.ptr(out, C.c_double), 24)
         keys = ['n_active', 'n_fronts', 'max_front', 'factor_flops_per_point', 'nnz_lu', 'analyze_s',
                 'assemble_ms', 'sweep_ms', 'factor_ms', 'solve_ms', 'chunk', 'schur_gemm_ms',
-                'schur_gemm_flops', 'levels', 'perturbed_pivots', 'launches']
+                'schur_gemm_flops', 'levels', 'perturbed_pivots', 'launches', 'schur_launches',
+                'sweep_device_ms', 'refine_solves']
         return dict(zip(keys, out.tolist()))
 
     @property
