@@ -9,6 +9,7 @@
 // Here Q = kq . x + V * Qz with kq the charge row folded onto the active DOFs.
 #include "ss_internal.h"
 #include "dev_complex.cuh"
+#include "krylov.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -736,6 +737,10 @@ int launch_condense(Handle &h) {
 
 namespace ss {
 
+constexpr int kKrylovM = 30;            // FGMRES restart length (mixed precision)
+constexpr int kKrylovRestarts = 4;
+constexpr double kKrylovTol = 1e-13;    // relative residual target
+
 template <class T>
 static int small_limit() { return sizeof(T) == 8 ? 96 : 128; }  // cd: 96^2*16, cf: 128^2*8 bytes
 
@@ -904,7 +909,9 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
     if (rc) return rc;
   }
   const int64_t W = S.relpos_ptr[S.nfront];
-  const double per = (double)S.arena * sizeof(cplx<T>) + n * 4.0 + W * (double)sizeof(cplx<T>) + n * 64.0 + 256;
+  const double krylov = sizeof(T) == 4 ? (2.0 * kKrylovM + 2) * n * sizeof(cd) : 0.0;
+  const double per = (double)S.arena * sizeof(cplx<T>) + n * 4.0 + W * (double)sizeof(cplx<T>) + n * 64.0 + krylov + 256;
+  KrylovWork kw;
   size_t fr = 0, tot = 0;
   SS_CK(cudaMemGetInfo(&fr, &tot));
   int B = (int)std::max(1.0, std::min((double)n_f, std::min(256.0, (0.85 * (double)fr - 512e6) / per)));
@@ -989,7 +996,31 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
     sw.collect();
     std::fill(conv.begin(), conv.end(), 0);
     std::fill(hit.begin(), hit.end(), 0);
-    for (int it = 0; it < maxit; ++it) {
+    const bool use_krylov = sizeof(T) == 4 || getenv("SS_FP64_KRYLOV") != nullptr;
+    if (use_krylov) {
+      // FGMRES-IR: FP64 Krylov, complex64 factors as right preconditioner
+      std::vector<int> kits;
+      std::vector<char> kconv;
+      auto pre = [&](const cd *src, cd *dst) { return sw.solve(nb, src, dst, wv.as<cplx<T>>()); };
+      rc = fgmres(h, kw, nb, kKrylovM, kKrylovRestarts, kKrylovTol, a.Kc, a.Mc, a.Dc, dom.as<double>(), b.as<cd>(),
+                  x.as<cd>(), pre, kits, kconv);
+      if (rc) return rc;
+      for (int f = 0; f < nb; ++f) hit[f] = kits[f], conv[f] = kconv[f];
+    }
+    if (getenv("SS_DEBUG_IR")) {
+      // backward error of the direct solve: |b - A x| / |b|, and the solution size
+      residual_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, h.dc_ptr.as<int64_t>(), h.dc_idx.as<int64_t>(),
+                                                          a.Kc, a.Mc, a.Dc, dom.as<double>(), h.beta, b.as<cd>(),
+                                                          x.as<cd>(), r.as<cd>());
+      norm2_kernel<<<nb, 256, 0, h.stream>>>(n, r.as<cd>(), nrm.as<double>());
+      norm2_kernel<<<nb, 256, 0, h.stream>>>(n, b.as<cd>(), nrm.as<double>() + nb);
+      std::vector<double> q(2 * nb);
+      cudaMemcpyAsync(q.data(), nrm.p, 2 * nb * sizeof(double), cudaMemcpyDeviceToHost, h.stream);
+      cudaStreamSynchronize(h.stream);
+      fprintf(stderr, "direct solve (%s): |r|/|b| f0 %.3e f_last %.3e\n", sizeof(T) == 8 ? "c128" : "c64",
+              q[0] / q[nb], q[nb - 1] / q[2 * nb - 1]);
+    }
+    for (int it = 0; it < (use_krylov ? 0 : maxit); ++it) {
       residual_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, h.dc_ptr.as<int64_t>(), h.dc_idx.as<int64_t>(),
                                                           a.Kc, a.Mc, a.Dc, dom.as<double>(), h.beta, b.as<cd>(),
                                                           x.as<cd>(), r.as<cd>());
