@@ -149,6 +149,38 @@ int ss_solve_fields(ss_handle *h, double omega, double V, double *disp);
  */
 int ss_stats(const ss_handle *h, double *out, int n);
 
+/*
+ * Q9 assembly that allocates nothing (no counterpart in the reference: it
+ * serves callers of this library that cannot allocate device memory, e.g.
+ * code running while a stream is captured into a CUDA graph, or a host
+ * framework that owns all device memory through its own pool).
+ *
+ * Every pointer is a device pointer the caller owns: the mesh and materials as
+ * for ss_set_mesh / ss_set_materials (materials already zero-lifted for
+ * ndisp == 2), the PML as for ss_set_pml (n_regions == 0: no PML; the Q9 form
+ * clamps the ratio), and the global pattern: indptr (ndisp+1)*n_nodes+1 row
+ * pointers of the component-major K layout and the node adjacency nadj_ptr /
+ * nadj (sorted neighbours, self included).  K and M (nnz complex values each)
+ * are zeroed and then filled.  Element matrices go through a fixed internal
+ * scratch of 512 elements (11.3 MB, allocated with the library image on every
+ * GPU that loads it); larger meshes are processed in 512-element batches.
+ * Shared slots are summed with atomic adds, so results equal ss_assemble's to
+ * rounding, not bit for bit.  The first call on a device resolves the scratch
+ * address (make it before any stream capture).  All calls share the scratch:
+ * calls that overlap on the GPU (other streams, other threads) race.  The call
+ * synchronises `stream` (a cudaStream_t, NULL for the legacy default stream)
+ * and returns SS_EINVAL when the pattern does not contain an element's node
+ * pair.
+ */
+int ss_assemble_q9_noalloc(int ndisp, int64_t n_nodes, const double *pos, int64_t n_elem,
+                           const int64_t *conn, const int32_t *elem_mat, const double *rho,
+                           const double *C, const double *e, const double *eps, int n_regions,
+                           const int32_t *elem_region, const int32_t *pml_axis,
+                           const double *pml_dmax, const int32_t *pml_npow,
+                           const double *pml_inner, const double *pml_outer, double omega_top,
+                           const int64_t *indptr, const int64_t *nadj_ptr, const int64_t *nadj,
+                           int64_t nnz, double *K, double *M, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -10,6 +10,7 @@
 // so repeated assemblies are bitwise identical and no atomics are used.
 #include "ss_internal.h"
 #include "dev_complex.cuh"
+#include "q9_element.cuh"
 
 namespace ss {
 
@@ -55,13 +56,6 @@ __device__ inline void q9_shape(double x, double y, double *N, double *dx, doubl
   dy[7] = 0.25 * (-4 * x * y * (x - 1));
   dy[8] = 0.25 * (8 * y * (x * x - 1));
 }
-
-struct PmlDev {
-  const int32_t *axis, *npow, *elem_region;
-  const double *dmax, *inner, *outer;
-  int clip;
-  double omega;
-};
 
 // alphas (a1, a2, a3) of one element from its centre coordinate
 // (piezo_fem.py:222-242; saw3d/assembly.py:127-143)
@@ -211,6 +205,14 @@ __global__ void __launch_bounds__(128) q9_element_kernel(
 namespace ss {
 
 int64_t global_slot(const Handle &h, int64_t i, int a, int64_t r, int b);
+
+cudaError_t launch_q9_elements(cudaStream_t s, int64_t ne, int nc, const double *pos, const int64_t *conn,
+                               const int32_t *emat, const double *rho, const double *C, const double *e,
+                               const double *eps, const PmlDev &pml, cd *Kel, cd *Mel) {
+  if (ne <= 0) return cudaSuccess;
+  q9_element_kernel<<<(unsigned)((ne + 3) / 4), 128, 0, s>>>(ne, nc, pos, conn, emat, rho, C, e, eps, pml, Kel, Mel);
+  return cudaGetLastError();
+}
 
 // Sum the element contributions of every (node pair, component pair) in
 // ascending element order into the global CSR values.

@@ -8,7 +8,7 @@ from conftest import REPO
 
 def declared():
     txt = (REPO / 'include' / 'sawsim_b200.h').read_text()
-    return sorted(set(re.findall(r'\b(ss_[a-z_]+)\s*\(', txt)))
+    return sorted(set(re.findall(r'\b(ss_[a-z0-9_]+)\s*\(', txt)))
 
 
 def test_header_and_binding_agree():
