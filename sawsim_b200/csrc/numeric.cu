@@ -315,7 +315,38 @@ __global__ void __launch_bounds__(256) front_assemble_large_kernel(FrontArgs<T> 
   }
 }
 
-// Unblocked LU of panel columns [j0, j1) over rows [j0, m), pivot rows from [j0, k).
+// Rows [k, m) of the panel columns: L21[:, j0:j1] = F21[:, j0:j1] U_jj^-1 (each
+// row independent, one thread per row; U_jj staged in shared memory).
+template <class T>
+__global__ void __launch_bounds__(256) front_l21_kernel(FrontArgs<T> a, int j0) {
+  __shared__ cplx<T> U[kPanel][kPanel];
+  const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
+  const int k = a.k[f], m = a.m[f], ld = a.ld[f];
+  if (j0 >= k) return;
+  const int j1 = min(k, j0 + kPanel), w = j1 - j0;
+  const cplx<T> *Fc = a.arena + (int64_t)fq * a.stride + a.off[f];
+  for (int t = threadIdx.x; t < w * w; t += blockDim.x) U[t / w][t % w] = Fc[(int64_t)(j0 + t / w) * ld + j0 + t % w];
+  __syncthreads();
+  const int r = k + blockIdx.z * blockDim.x + threadIdx.x;
+  if (r >= m) return;
+  cplx<T> *row = a.arena + (int64_t)fq * a.stride + a.off[f] + (int64_t)r * ld + j0;
+  cplx<T> x[kPanel];
+#pragma unroll
+  for (int c = 0; c < kPanel; ++c)
+    if (c < w) x[c] = row[c];
+#pragma unroll
+  for (int c = 0; c < kPanel; ++c) {
+    if (c >= w) break;
+    cplx<T> v = x[c];
+    for (int t = 0; t < c; ++t) v = cfms(v, x[t], U[t][c]);
+    x[c] = cdiv(v, U[c][c]);
+  }
+#pragma unroll
+  for (int c = 0; c < kPanel; ++c)
+    if (c < w) row[c] = x[c];
+}
+
+// Unblocked LU of panel columns [j0, j1) over the fully-summed rows [j0, k).
 template <class T>
 __global__ void __launch_bounds__(256) front_panel_kernel(FrontArgs<T> a, int j0) {
   __shared__ T s_v[8];
@@ -348,12 +379,12 @@ __global__ void __launch_bounds__(256) front_panel_kernel(FrontArgs<T> a, int j0
     }
     __syncthreads();
     const cplx<T> inv = cdiv(cplx<T>{1, 0}, s_pivot);
-    for (int r = j + 1 + threadIdx.x; r < m; r += blockDim.x)
+    for (int r = j + 1 + threadIdx.x; r < k; r += blockDim.x)
       F[(int64_t)r * ld + j] = cmul(F[(int64_t)r * ld + j], inv);
     __syncthreads();
     const int nc = j1 - j - 1;
     if (nc > 0) {
-      const int nr = m - j - 1;
+      const int nr = k - j - 1;
       for (int t = threadIdx.x; t < nr * nc; t += blockDim.x) {
         const int r = j + 1 + t / nc, c = j + 1 + t % nc;
         F[(int64_t)r * ld + c] = cfms(F[(int64_t)r * ld + c], F[(int64_t)r * ld + j], F[(int64_t)j * ld + c]);
@@ -398,49 +429,73 @@ struct GemmTask {
   int f, r0, c0, rhi, chi, kk0, kk1;
 };
 
+constexpr int kGemmBM = 128, kGemmBN = 64, kGemmBK = 8;
+
+// 128x64 complex tile per CTA, 8x4 outputs per thread; K in chunks of 8 with
+// the next chunk prefetched into registers while the current one is consumed.
 template <class T>
 __global__ void __launch_bounds__(256) front_gemm_kernel(FrontArgs<T> a, const GemmTask *__restrict__ tasks) {
-  __shared__ cplx<T> As[16][64];
-  __shared__ cplx<T> Bs[16][64];
+  constexpr int BM = kGemmBM, BN = kGemmBN, BK = kGemmBK;
+  __shared__ cplx<T> As[BK][BM];
+  __shared__ cplx<T> Bs[BK][BN];
   const GemmTask tk = tasks[blockIdx.x];
   const int fq = blockIdx.y;
   const int ld = a.ld[tk.f];
   cplx<T> *F = a.arena + (int64_t)fq * a.stride + a.off[tk.f];
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  cplx<T> acc[4][4];
+  cplx<T> acc[8][4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 8; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = cplx<T>{0, 0};
-  for (int kb = tk.kk0; kb < tk.kk1; kb += 16) {
-    for (int t = threadIdx.x; t < 16 * 64; t += 256) {
-      const int kk = t & 15, rr = t >> 4;           // A tile: 64 rows x 16
-      const int r = tk.r0 + rr, q = kb + kk;
-      As[kk][rr] = (r < tk.rhi && q < tk.kk1) ? F[(int64_t)r * ld + q] : cplx<T>{0, 0};
-      const int cc = t & 63, kk2 = t >> 6;          // B tile: 16 x 64 cols
-      const int c = tk.c0 + cc, q2 = kb + kk2;
-      Bs[kk2][cc] = (c < tk.chi && q2 < tk.kk1) ? F[(int64_t)q2 * ld + c] : cplx<T>{0, 0};
+  cplx<T> pa[4], pb[2];
+  auto fetch = [&](int kb) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int idx = threadIdx.x + 256 * q, rr = idx >> 3, kk = idx & 7;
+      const int r = tk.r0 + rr, c = kb + kk;
+      pa[q] = (r < tk.rhi && c < tk.kk1) ? F[(int64_t)r * ld + c] : cplx<T>{0, 0};
+    }
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int idx = threadIdx.x + 256 * q, kk = idx >> 6, cc = idx & 63;
+      const int r = kb + kk, c = tk.c0 + cc;
+      pb[q] = (c < tk.chi && r < tk.kk1) ? F[(int64_t)r * ld + c] : cplx<T>{0, 0};
+    }
+  };
+  fetch(tk.kk0);
+  for (int kb = tk.kk0; kb < tk.kk1; kb += BK) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int idx = threadIdx.x + 256 * q;
+      As[idx & 7][idx >> 3] = pa[q];
+    }
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int idx = threadIdx.x + 256 * q;
+      Bs[idx >> 6][idx & 63] = pb[q];
     }
     __syncthreads();
-#pragma unroll 4
-    for (int kk = 0; kk < 16; ++kk) {
-      cplx<T> av[4], bv[4];
+    if (kb + BK < tk.kk1) fetch(kb + BK);
 #pragma unroll
-      for (int i = 0; i < 4; ++i) av[i] = As[kk][ty + 16 * i];
+    for (int kk = 0; kk < BK; ++kk) {
+      cplx<T> av[8], bv[4];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) av[i] = As[kk][ty + 16 * i];
 #pragma unroll
       for (int j = 0; j < 4; ++j) bv[j] = Bs[kk][tx + 16 * j];
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < 8; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-          acc[i][j].x += av[i].x * bv[j].x - av[i].y * bv[j].y;
-          acc[i][j].y += av[i].x * bv[j].y + av[i].y * bv[j].x;
+          acc[i][j].x = fma(av[i].x, bv[j].x, fma(-av[i].y, bv[j].y, acc[i][j].x));
+          acc[i][j].y = fma(av[i].x, bv[j].y, fma(av[i].y, bv[j].x, acc[i][j].y));
         }
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 8; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const int r = tk.r0 + ty + 16 * i, c = tk.c0 + tx + 16 * j;
@@ -603,8 +658,8 @@ struct Plan {
 };
 
 static void add_tiles(std::vector<GemmTask> &v, int f, int r0, int r1, int c0, int c1, int k0, int k1) {
-  for (int r = r0; r < r1; r += 64)
-    for (int c = c0; c < c1; c += 64) v.push_back(GemmTask{f, r, c, r1, c1, k0, k1});
+  for (int r = r0; r < r1; r += kGemmBM)
+    for (int c = c0; c < c1; c += kGemmBN) v.push_back(GemmTask{f, r, c, r1, c1, k0, k1});
 }
 
 Plan *build_plan(Handle &h, int small_m) {
@@ -838,6 +893,8 @@ struct Sweeper {
       for (int s = 0; s < P.nsteps[l]; ++s) {
         const int j0 = s * kPanel;
         front_panel_kernel<T><<<dim3(nl, nb), 256, 0, h.stream>>>(b, j0);
+        front_l21_kernel<T><<<dim3(nl, nb, (ml + 255) / 256), 256, 0, h.stream>>>(b, j0);
+        ++launches;
         front_swap_trsm_kernel<T><<<dim3(nl, nb, (ml + 255) / 256), 256, 0, h.stream>>>(b, j0);
         const int64_t q = P.level_step0[l] + s;
         const int64_t t0 = P.step_ptr[q], t1 = P.step_ptr[q + 1];
