@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(256) front_small_kernel(FrontArgs<T> a) {
 namespace ss {
 
 constexpr int kRowChunk = 32;   // rows per CTA in the large-front assembly
-constexpr int kPanel = 16;      // panel width of the blocked partial LU
+constexpr int kPanel = 32;      // panel width of the blocked partial LU
 
 // Large fronts, assembly in global memory: CTA (front, frequency, row chunk)
 // zeroes its rows, drops in the arrowhead entries of those rows, then adds the
@@ -338,6 +338,7 @@ __global__ void __launch_bounds__(256) front_l21_kernel(FrontArgs<T> a, int j0) 
   for (int c = 0; c < kPanel; ++c) {
     if (c >= w) break;
     cplx<T> v = x[c];
+#pragma unroll
     for (int t = 0; t < c; ++t) v = cfms(v, x[t], U[t][c]);
     x[c] = cdiv(v, U[c][c]);
   }
@@ -394,33 +395,51 @@ __global__ void __launch_bounds__(256) front_panel_kernel(FrontArgs<T> a, int j0
   }
 }
 
-// Apply the panel's row swaps to the columns outside it and solve the unit-lower
-// diagonal block into the row block U[j0:j1, j1:m).  One thread per column.
+// mode 0: apply the panel's row swaps to every column outside it (one thread per
+// column).  mode 1: solve the unit-lower diagonal block into the row block
+// U[j0:j1, j1:m) (one thread per column, L_jj staged in shared memory).
 template <class T>
-__global__ void __launch_bounds__(256) front_swap_trsm_kernel(FrontArgs<T> a, int j0) {
+__global__ void __launch_bounds__(256) front_swap_trsm_kernel(FrontArgs<T> a, int j0, int mode) {
+  __shared__ cplx<T> L[kPanel][kPanel];
   const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
   const int k = a.k[f], m = a.m[f], ld = a.ld[f];
   if (j0 >= k) return;
-  const int j1 = min(k, j0 + kPanel);
-  const int idx = blockIdx.z * blockDim.x + threadIdx.x;
-  if (idx >= m - (j1 - j0)) return;
-  const int c = idx < j0 ? idx : idx + (j1 - j0);
+  const int j1 = min(k, j0 + kPanel), w = j1 - j0;
   cplx<T> *F = a.arena + (int64_t)fq * a.stride + a.off[f];
-  const int *piv = a.piv + (int64_t)fq * a.n + a.p0[f];
-  for (int j = j0; j < j1; ++j) {
-    const int p = piv[j];
-    if (p != j) {
-      const cplx<T> t = F[(int64_t)j * ld + c];
-      F[(int64_t)j * ld + c] = F[(int64_t)p * ld + c];
-      F[(int64_t)p * ld + c] = t;
+  const int idx = blockIdx.z * blockDim.x + threadIdx.x;
+  if (mode == 0) {
+    if (idx >= m - w) return;
+    const int c = idx < j0 ? idx : idx + w;
+    const int *piv = a.piv + (int64_t)fq * a.n + a.p0[f];
+    for (int j = j0; j < j1; ++j) {
+      const int p = piv[j];
+      if (p != j) {
+        const cplx<T> t = F[(int64_t)j * ld + c];
+        F[(int64_t)j * ld + c] = F[(int64_t)p * ld + c];
+        F[(int64_t)p * ld + c] = t;
+      }
     }
+    return;
   }
-  if (c < j1) return;
-  for (int j = j0 + 1; j < j1; ++j) {
-    cplx<T> v = F[(int64_t)j * ld + c];
-    for (int t = j0; t < j; ++t) v = cfms(v, F[(int64_t)j * ld + t], F[(int64_t)t * ld + c]);
-    F[(int64_t)j * ld + c] = v;
+  for (int t = threadIdx.x; t < w * w; t += blockDim.x) L[t / w][t % w] = F[(int64_t)(j0 + t / w) * ld + j0 + t % w];
+  __syncthreads();
+  const int c = j1 + idx;
+  if (c >= m) return;
+  cplx<T> v[kPanel];
+#pragma unroll
+  for (int i = 0; i < kPanel; ++i)
+    if (i < w) v[i] = F[(int64_t)(j0 + i) * ld + c];
+#pragma unroll
+  for (int i = 1; i < kPanel; ++i) {
+    if (i >= w) break;
+    cplx<T> x = v[i];
+#pragma unroll
+    for (int t = 0; t < i; ++t) x = cfms(x, L[i][t], v[t]);
+    v[i] = x;
   }
+#pragma unroll
+  for (int i = 0; i < kPanel; ++i)
+    if (i < w) F[(int64_t)(j0 + i) * ld + c] = v[i];
 }
 
 // One 64x64 output tile of C -= A B inside front f: rows [r0, rhi), cols [c0, chi),
@@ -429,36 +448,47 @@ struct GemmTask {
   int f, r0, c0, rhi, chi, kk0, kk1;
 };
 
-constexpr int kGemmBM = 128, kGemmBN = 64, kGemmBK = 8;
+constexpr int kGemmBK = 8;
+// tile shapes: square (Schur update), skinny (panel column update), short (U row update)
+enum GemmShape { kSquare = 0, kSkinny = 1, kShort = 2 };
+template <int S> struct Tile;
+template <> struct Tile<kSquare> { static constexpr int BM = 128, BN = 64, TM = 8, TN = 4; };
+template <> struct Tile<kSkinny> { static constexpr int BM = 256, BN = 32, TM = 8, TN = 4; };
+template <> struct Tile<kShort> { static constexpr int BM = 32, BN = 256, TM = 4, TN = 8; };
+static inline int tile_bm(int s) { return s == kSquare ? 128 : s == kSkinny ? 256 : 32; }
+static inline int tile_bn(int s) { return s == kSquare ? 64 : s == kSkinny ? 32 : 256; }
 
-// 128x64 complex tile per CTA, 8x4 outputs per thread; K in chunks of 8 with
-// the next chunk prefetched into registers while the current one is consumed.
-template <class T>
+// One BMxBN complex tile of C -= A B per CTA, TMxTN outputs per thread; K in
+// chunks of 8 with the next chunk prefetched into registers.
+template <class T, int S>
 __global__ void __launch_bounds__(256) front_gemm_kernel(FrontArgs<T> a, const GemmTask *__restrict__ tasks) {
-  constexpr int BM = kGemmBM, BN = kGemmBN, BK = kGemmBK;
+  constexpr int BM = Tile<S>::BM, BN = Tile<S>::BN, TM = Tile<S>::TM, TN = Tile<S>::TN, BK = kGemmBK;
+  constexpr int TX = BN / TN, TY = BM / TM;
+  static_assert(TX * TY == 256, "256 threads");
+  constexpr int NA = BM * BK / 256, NBt = BN * BK / 256;
   __shared__ cplx<T> As[BK][BM];
   __shared__ cplx<T> Bs[BK][BN];
   const GemmTask tk = tasks[blockIdx.x];
   const int fq = blockIdx.y;
   const int ld = a.ld[tk.f];
   cplx<T> *F = a.arena + (int64_t)fq * a.stride + a.off[tk.f];
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  cplx<T> acc[8][4];
+  const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
+  cplx<T> acc[TM][TN];
 #pragma unroll
-  for (int i = 0; i < 8; ++i)
+  for (int i = 0; i < TM; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = cplx<T>{0, 0};
-  cplx<T> pa[4], pb[2];
+    for (int j = 0; j < TN; ++j) acc[i][j] = cplx<T>{0, 0};
+  cplx<T> pa[NA], pb[NBt];
   auto fetch = [&](int kb) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int idx = threadIdx.x + 256 * q, rr = idx >> 3, kk = idx & 7;
+    for (int q = 0; q < NA; ++q) {
+      const int idx = threadIdx.x + 256 * q, rr = idx / BK, kk = idx % BK;
       const int r = tk.r0 + rr, c = kb + kk;
       pa[q] = (r < tk.rhi && c < tk.kk1) ? F[(int64_t)r * ld + c] : cplx<T>{0, 0};
     }
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const int idx = threadIdx.x + 256 * q, kk = idx >> 6, cc = idx & 63;
+    for (int q = 0; q < NBt; ++q) {
+      const int idx = threadIdx.x + 256 * q, kk = idx / BN, cc = idx % BN;
       const int r = kb + kk, c = tk.c0 + cc;
       pb[q] = (c < tk.chi && r < tk.kk1) ? F[(int64_t)r * ld + c] : cplx<T>{0, 0};
     }
@@ -466,28 +496,28 @@ __global__ void __launch_bounds__(256) front_gemm_kernel(FrontArgs<T> a, const G
   fetch(tk.kk0);
   for (int kb = tk.kk0; kb < tk.kk1; kb += BK) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 0; q < NA; ++q) {
       const int idx = threadIdx.x + 256 * q;
-      As[idx & 7][idx >> 3] = pa[q];
+      As[idx % BK][idx / BK] = pa[q];
     }
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
+    for (int q = 0; q < NBt; ++q) {
       const int idx = threadIdx.x + 256 * q;
-      Bs[idx >> 6][idx & 63] = pb[q];
+      Bs[idx / BN][idx % BN] = pb[q];
     }
     __syncthreads();
     if (kb + BK < tk.kk1) fetch(kb + BK);
 #pragma unroll
     for (int kk = 0; kk < BK; ++kk) {
-      cplx<T> av[8], bv[4];
+      cplx<T> av[TM], bv[TN];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) av[i] = As[kk][ty + 16 * i];
+      for (int i = 0; i < TM; ++i) av[i] = As[kk][ty + TY * i];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) bv[j] = Bs[kk][tx + 16 * j];
+      for (int j = 0; j < TN; ++j) bv[j] = Bs[kk][tx + TX * j];
 #pragma unroll
-      for (int i = 0; i < 8; ++i)
+      for (int i = 0; i < TM; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
+        for (int j = 0; j < TN; ++j) {
           acc[i][j].x = fma(av[i].x, bv[j].x, fma(-av[i].y, bv[j].y, acc[i][j].x));
           acc[i][j].y = fma(av[i].x, bv[j].y, fma(av[i].y, bv[j].x, acc[i][j].y));
         }
@@ -495,10 +525,10 @@ __global__ void __launch_bounds__(256) front_gemm_kernel(FrontArgs<T> a, const G
     __syncthreads();
   }
 #pragma unroll
-  for (int i = 0; i < 8; ++i)
+  for (int i = 0; i < TM; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int r = tk.r0 + ty + 16 * i, c = tk.c0 + tx + 16 * j;
+    for (int j = 0; j < TN; ++j) {
+      const int r = tk.r0 + ty + TY * i, c = tk.c0 + tx + TX * j;
       if (r < tk.rhi && c < tk.chi) {
         cplx<T> &d = F[(int64_t)r * ld + c];
         d = d - acc[i][j];
@@ -657,9 +687,9 @@ struct Plan {
   double schur_flops = 0;
 };
 
-static void add_tiles(std::vector<GemmTask> &v, int f, int r0, int r1, int c0, int c1, int k0, int k1) {
-  for (int r = r0; r < r1; r += kGemmBM)
-    for (int c = c0; c < c1; c += kGemmBN) v.push_back(GemmTask{f, r, c, r1, c1, k0, k1});
+static void add_tiles(std::vector<GemmTask> &v, int shape, int f, int r0, int r1, int c0, int c1, int k0, int k1) {
+  for (int r = r0; r < r1; r += tile_bm(shape))
+    for (int c = c0; c < c1; c += tile_bn(shape)) v.push_back(GemmTask{f, r, c, r1, c1, k0, k1});
 }
 
 Plan *build_plan(Handle &h, int small_m) {
@@ -692,16 +722,22 @@ Plan *build_plan(Handle &h, int small_m) {
     const int ns = (kmax + kPanel - 1) / kPanel;
     P->nsteps.push_back(ns);
     P->level_step0.push_back((int64_t)P->step_ptr.size() - 1);
+    // left-looking (Crout) steps: before panel j0 its columns get all earlier
+    // pivots (skinny GEMM, K = j0), after it the U row block does (short GEMM)
     for (int s = 0; s < ns; ++s) {
       const int j0 = s * kPanel;
       for (int f : large) {
         const int k = S.k[f], m = S.m[f];
-        if (j0 >= k) continue;
+        if (j0 >= k || j0 == 0) continue;
         const int j1 = std::min(k, j0 + kPanel);
-        if (j1 < k) {
-          add_tiles(P->tasks, f, j1, k, j1, m, j0, j1);
-          add_tiles(P->tasks, f, k, m, j1, k, j0, j1);
-        }
+        add_tiles(P->tasks, kSkinny, f, j0, m, j0, j1, 0, j0);
+      }
+      P->step_ptr.push_back((int64_t)P->tasks.size());
+      for (int f : large) {
+        const int k = S.k[f], m = S.m[f];
+        if (j0 >= k || j0 == 0) continue;
+        const int j1 = std::min(k, j0 + kPanel);
+        if (j1 < m) add_tiles(P->tasks, kShort, f, j0, j1, j1, m, 0, j0);
       }
       P->step_ptr.push_back((int64_t)P->tasks.size());
     }
@@ -712,7 +748,7 @@ Plan *build_plan(Handle &h, int small_m) {
   for (int l = 0; l < S.nlevel; ++l) {
     for (int q = P->large_ptr[l]; q < P->large_ptr[l + 1]; ++q) {
       const int f = P->fronts_large[q], k = S.k[f], m = S.m[f];
-      if (m > k) add_tiles(P->tasks, f, k, m, k, m, 0, k);
+      if (m > k) add_tiles(P->tasks, kSquare, f, k, m, k, m, 0, k);
       P->schur_flops += 8.0 * k * (double)(m - k) * (m - k);
     }
     sp.push_back((int64_t)P->tasks.size());
@@ -890,22 +926,30 @@ struct Sweeper {
       const int ml = P.maxm_large[l];
       front_assemble_large_kernel<T><<<dim3(nl, nb, (ml + kRowChunk - 1) / kRowChunk), 256, 0, h.stream>>>(b);
       ++launches;
+      const GemmTask *tasks = P.d_tasks.as<GemmTask>();
+      const unsigned zc = (unsigned)((ml + 255) / 256);
       for (int s = 0; s < P.nsteps[l]; ++s) {
         const int j0 = s * kPanel;
+        const int64_t q = P.level_step0[l] + 2 * s;
+        const int64_t g0 = P.step_ptr[q], g1 = P.step_ptr[q + 1], g2 = P.step_ptr[q + 2];
+        if (g1 > g0) {   // panel columns <- earlier pivots
+          front_gemm_kernel<T, kSkinny><<<dim3((unsigned)(g1 - g0), nb), 256, 0, h.stream>>>(b, tasks + g0);
+          ++launches;
+        }
         front_panel_kernel<T><<<dim3(nl, nb), 256, 0, h.stream>>>(b, j0);
-        front_l21_kernel<T><<<dim3(nl, nb, (ml + 255) / 256), 256, 0, h.stream>>>(b, j0);
-        ++launches;
-        front_swap_trsm_kernel<T><<<dim3(nl, nb, (ml + 255) / 256), 256, 0, h.stream>>>(b, j0);
-        const int64_t q = P.level_step0[l] + s;
-        const int64_t t0 = P.step_ptr[q], t1 = P.step_ptr[q + 1];
-        if (t1 > t0)
-          front_gemm_kernel<T><<<dim3((unsigned)(t1 - t0), nb), 256, 0, h.stream>>>(b, P.d_tasks.as<GemmTask>() + t0);
-        launches += 2 + (t1 > t0);
+        front_l21_kernel<T><<<dim3(nl, nb, zc), 256, 0, h.stream>>>(b, j0);
+        front_swap_trsm_kernel<T><<<dim3(nl, nb, zc), 256, 0, h.stream>>>(b, j0, 0);
+        if (g2 > g1) {   // U row block <- earlier pivots
+          front_gemm_kernel<T, kShort><<<dim3((unsigned)(g2 - g1), nb), 256, 0, h.stream>>>(b, tasks + g1);
+          ++launches;
+        }
+        front_swap_trsm_kernel<T><<<dim3(nl, nb, zc), 256, 0, h.stream>>>(b, j0, 1);
+        launches += 4;
       }
       const int64_t t0 = P.schur_ptr[l], t1 = P.schur_ptr[l + 1];
       if (t1 > t0) {
         cudaEventRecord(ev[2 * nev], h.stream);
-        front_gemm_kernel<T><<<dim3((unsigned)(t1 - t0), nb), 256, 0, h.stream>>>(b, P.d_tasks.as<GemmTask>() + t0);
+        front_gemm_kernel<T, kSquare><<<dim3((unsigned)(t1 - t0), nb), 256, 0, h.stream>>>(b, tasks + t0);
         cudaEventRecord(ev[2 * nev + 1], h.stream);
         ++nev;
         ++launches;
@@ -971,8 +1015,14 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
   KrylovWork kw;
   size_t fr = 0, tot = 0;
   SS_CK(cudaMemGetInfo(&fr, &tot));
+  // device work buffers persist in the handle: repeated sweeps reuse them
+  DBuf &arena = h.wk[0], &piv = h.wk[1], &wv = h.wk[2], &b = h.wk[3], &x = h.wk[4], &r = h.wk[5], &dx = h.wk[6],
+       &dom = h.wk[7], &npert = h.wk[8], &nrm = h.wk[9], &dQ = h.wk[10];
+  // the chunk size counts only memory not already held by these buffers
+  for (int i = 0; i < 11; ++i) fr += h.wk[i].bytes;
   int B = (int)std::max(1.0, std::min((double)n_f, std::min(256.0, (0.85 * (double)fr - 512e6) / per)));
-  DBuf arena, piv, wv, b, x, r, dx, dom, npert, nrm, dQ;
+  // a buffer that must grow is released first so that old and new never coexist
+  if ((size_t)B * S.arena * sizeof(cplx<T>) > arena.bytes) arena.release();
   SS_CK(dalloc(arena, (size_t)B * S.arena * sizeof(cplx<T>)));
   SS_CK(dalloc(piv, (size_t)B * n * sizeof(int)));
   SS_CK(dalloc(wv, (size_t)B * std::max<int64_t>(W, 1) * sizeof(cplx<T>)));

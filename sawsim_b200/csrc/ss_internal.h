@@ -112,6 +112,7 @@ struct Handle {
       d_relpos, d_arrow_ptr, d_arrow_pos, d_arrow_slot, d_level_fronts, d_p0;
   // numeric work
   DBuf arena, piv, dperm_new, work;
+  DBuf wk[12];                           // sweep work buffers, kept across calls
   size_t arena_chunk = 0;
   void *plan[2] = {nullptr, nullptr};   // factorisation plans per precision
   DBuf dKs, dMs, dDs;                    // equilibrated condensed values
