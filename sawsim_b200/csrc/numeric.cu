@@ -577,22 +577,99 @@ __global__ void __launch_bounds__(256) front_fwd_kernel(FrontArgs<T> a, const cd
     }
   }
   __syncthreads();
-  for (int j = 0; j < k - 1; ++j) {
-    const cplx<T> vj = v[j];
-    for (int r = j + 1 + threadIdx.x; r < k; r += blockDim.x) v[r] = cfms(v[r], F[(int64_t)r * ld + j], vj);
+  // blocked unit-lower solve: warp 0 solves each 32x32 diagonal block with
+  // shuffles, then every warp updates the rows below (coalesced row dots)
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int jb = 0; jb < k; jb += 32) {
+    const int je = min(k, jb + 32), bw = je - jb;
+    if (wid == 0) {
+      cplx<T> x = lane < bw ? v[jb + lane] : cplx<T>{0, 0};
+      for (int t = 0; t < bw - 1; ++t) {
+        cplx<T> xt;
+        xt.x = __shfl_sync(0xffffffffu, x.x, t);
+        xt.y = __shfl_sync(0xffffffffu, x.y, t);
+        if (lane > t && lane < bw) x = cfms(x, F[(int64_t)(jb + lane) * ld + jb + t], xt);
+      }
+      if (lane < bw) v[jb + lane] = x;
+    }
+    __syncthreads();
+    const cplx<T> vt = lane < bw ? v[jb + lane] : cplx<T>{0, 0};
+    for (int r = je + wid; r < k; r += nw) {
+      cplx<T> acc = lane < bw ? cmul(F[(int64_t)r * ld + jb + lane], vt) : cplx<T>{0, 0};
+      for (int o = 16; o > 0; o >>= 1) {
+        acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
+        acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
+      }
+      if (lane == 0) v[r] = v[r] - acc;
+    }
     __syncthreads();
   }
+  // update rows keep the children's sums; front_fwd_l21_kernel subtracts L21 y
+  for (int r = k + threadIdx.x; r < m; r += blockDim.x) w[a.relpos_ptr[f] + r - k] = v[r];
+  for (int i = threadIdx.x; i < k; i += blockDim.x) x[(int64_t)fq * a.n + p0 + i] = cd{(double)v[i].x, (double)v[i].y};
+}
+
+constexpr int kSolveRows = 64;   // rows per CTA of the solve GEMV kernels
+
+// Update rows of the forward solve: w[r - k] -= L21[r, :] y, CTA per
+// (front, frequency, 64-row chunk), one warp per row with coalesced dots.
+template <class T>
+__global__ void __launch_bounds__(256) front_fwd_l21_kernel(FrontArgs<T> a, const cd *__restrict__ x,
+                                                            cplx<T> *__restrict__ wv, int64_t wstride) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T> *y = reinterpret_cast<cplx<T> *>(smem_raw);
+  const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
+  const int k = a.k[f], m = a.m[f], ld = a.ld[f];
+  const int r0 = k + blockIdx.z * kSolveRows;
+  if (r0 >= m) return;
+  const int r1 = min(m, r0 + kSolveRows);
+  const cplx<T> *F = a.arena + (int64_t)fq * a.stride + a.off[f];
+  const int64_t p0 = a.p0[f];
+  for (int i = threadIdx.x; i < k; i += blockDim.x) y[i] = to_t<T>(x[(int64_t)fq * a.n + p0 + i]);
+  __syncthreads();
+  cplx<T> *w = wv + (int64_t)fq * wstride + a.relpos_ptr[f] - k;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int r = k + wid; r < m; r += nw) {
+  for (int r = r0 + wid; r < r1; r += nw) {
     cplx<T> acc{0, 0};
-    for (int t = lane; t < k; t += 32) acc = acc + cmul(F[(int64_t)r * ld + t], v[t]);
+    for (int t = lane; t < k; t += 32) acc = acc + cmul(F[(int64_t)r * ld + t], y[t]);
     for (int o = 16; o > 0; o >>= 1) {
       acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
       acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
     }
-    if (lane == 0) w[a.relpos_ptr[f] + r - k] = v[r] - acc;
+    if (lane == 0) w[r] = w[r] - acc;
   }
-  for (int i = threadIdx.x; i < k; i += blockDim.x) x[(int64_t)fq * a.n + p0 + i] = cd{(double)v[i].x, (double)v[i].y};
+}
+
+// First phase of the backward solve: x[pivots] -= U12 x_U, CTA per (front,
+// frequency, 64 pivot rows); x_U gathered from the ancestors' solution.
+template <class T>
+__global__ void __launch_bounds__(256) front_bwd_u12_kernel(FrontArgs<T> a, cd *__restrict__ x) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T> *xu = reinterpret_cast<cplx<T> *>(smem_raw);
+  const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
+  const int k = a.k[f], m = a.m[f], ld = a.ld[f];
+  const int q0 = blockIdx.z * kSolveRows;
+  if (q0 >= k || m == k) return;
+  const int q1 = min(k, q0 + kSolveRows);
+  const cplx<T> *F = a.arena + (int64_t)fq * a.stride + a.off[f];
+  cd *xf = x + (int64_t)fq * a.n;
+  const int64_t *rows = a.rows + a.rows_ptr[f];
+  for (int i = threadIdx.x; i < m - k; i += blockDim.x) xu[i] = to_t<T>(xf[rows[k + i]]);
+  __syncthreads();
+  const int64_t p0 = a.p0[f];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int r = q0 + wid; r < q1; r += nw) {
+    cplx<T> acc{0, 0};
+    for (int c = lane; c < m - k; c += 32) acc = acc + cmul(F[(int64_t)r * ld + k + c], xu[c]);
+    for (int o = 16; o > 0; o >>= 1) {
+      acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
+      acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
+    }
+    if (lane == 0) {
+      const cd cur = xf[p0 + r];
+      xf[p0 + r] = cd{cur.x - (double)acc.x, cur.y - (double)acc.y};
+    }
+  }
 }
 
 // Backward substitution for one level (levels run root first): z = y - U12 x_U,
@@ -607,26 +684,35 @@ __global__ void __launch_bounds__(256) front_bwd_kernel(FrontArgs<T> a, cd *__re
   const int64_t p0 = a.p0[f];
   cd *xf = x + (int64_t)fq * a.n;
   const int64_t *rows = a.rows + a.rows_ptr[f];
-  for (int i = threadIdx.x; i < m; i += blockDim.x) z[i] = to_t<T>(i < k ? xf[p0 + i] : xf[rows[i]]);
+  (void)rows;
+  for (int i = threadIdx.x; i < k; i += blockDim.x) z[i] = to_t<T>(xf[p0 + i]);   // y - U12 x_U
   __syncthreads();
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  if (m > k) {
-    for (int r = wid; r < k; r += nw) {
-      cplx<T> acc{0, 0};
-      for (int c = k + lane; c < m; c += 32) acc = acc + cmul(F[(int64_t)r * ld + c], z[c]);
+  // blocked upper solve from the bottom: warp 0 solves each diagonal block,
+  // then every warp updates the rows above it
+  for (int je = k; je > 0; je -= 32) {
+    const int jb = max(0, je - 32), bw = je - jb;
+    if (wid == 0) {
+      cplx<T> x = lane < bw ? z[jb + lane] : cplx<T>{0, 0};
+      for (int t = bw - 1; t >= 0; --t) {
+        if (lane == t) x = cdiv(x, F[(int64_t)(jb + t) * ld + jb + t]);
+        cplx<T> xt;
+        xt.x = __shfl_sync(0xffffffffu, x.x, t);
+        xt.y = __shfl_sync(0xffffffffu, x.y, t);
+        if (lane < t) x = cfms(x, F[(int64_t)(jb + lane) * ld + jb + t], xt);
+      }
+      if (lane < bw) z[jb + lane] = x;
+    }
+    __syncthreads();
+    const cplx<T> xt = lane < bw ? z[jb + lane] : cplx<T>{0, 0};
+    for (int r = wid; r < jb; r += nw) {
+      cplx<T> acc = lane < bw ? cmul(F[(int64_t)r * ld + jb + lane], xt) : cplx<T>{0, 0};
       for (int o = 16; o > 0; o >>= 1) {
         acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
         acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
       }
       if (lane == 0) z[r] = z[r] - acc;
     }
-    __syncthreads();
-  }
-  for (int j = k - 1; j >= 0; --j) {
-    const cplx<T> xj = cdiv(z[j], F[(int64_t)j * ld + j]);
-    for (int r = threadIdx.x; r < j; r += blockDim.x) z[r] = cfms(z[r], F[(int64_t)r * ld + j], xj);
-    __syncthreads();
-    if (threadIdx.x == 0) z[j] = xj;
     __syncthreads();
   }
   for (int i = threadIdx.x; i < k; i += blockDim.x) xf[p0 + i] = cd{(double)z[i].x, (double)z[i].y};
@@ -685,6 +771,7 @@ struct Plan {
   DBuf d_small, d_large, d_tasks;
   int small_m = 0;                         // threshold used
   double schur_flops = 0;
+  std::vector<int> lvl_maxk, lvl_maxu;     // per level max k and max m-k (solve grids)
 };
 
 static void add_tiles(std::vector<GemmTask> &v, int shape, int f, int r0, int r1, int c0, int c1, int k0, int k1) {
@@ -701,6 +788,14 @@ Plan *build_plan(Handle &h, int small_m) {
   P->schur_ptr.assign(1, 0);
   P->step_ptr.assign(1, 0);
   for (int l = 0; l < S.nlevel; ++l) {
+    int lk = 0, lu = 0;
+    for (int64_t q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
+      const int f = S.level_fronts[q];
+      lk = std::max(lk, S.k[f]);
+      lu = std::max(lu, S.m[f] - S.k[f]);
+    }
+    P->lvl_maxk.push_back(lk);
+    P->lvl_maxu.push_back(lu);
     int mm = 0, ml = 0, kmax = 0;
     std::vector<int> large;
     for (int64_t q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
@@ -964,18 +1059,29 @@ struct Sweeper {
   int solve(int nb, const cd *b, cd *x, cplx<T> *wv) {
     const Symbolic &S = h.sym;
     const size_t sm = (size_t)S.max_m * sizeof(cplx<T>);
+    const size_t smk = (size_t)std::max(1, S.max_k) * sizeof(cplx<T>);
     for (int l = 0; l < S.nlevel; ++l) {
       FrontArgs<T> c = a;
       c.fronts = h.d_level_fronts.as<int>() + S.level_ptr[l];
       const int nf = (int)(S.level_ptr[l + 1] - S.level_ptr[l]);
       front_fwd_kernel<T><<<dim3(nf, nb), 256, sm, h.stream>>>(c, b, x, wv, wstride);
       ++launches;
+      if (P.lvl_maxu[l] > 0) {
+        const unsigned z = (unsigned)((P.lvl_maxu[l] + kSolveRows - 1) / kSolveRows);
+        front_fwd_l21_kernel<T><<<dim3(nf, nb, z), 256, smk, h.stream>>>(c, x, wv, wstride);
+        ++launches;
+      }
     }
     for (int l = S.nlevel - 1; l >= 0; --l) {
       FrontArgs<T> c = a;
       c.fronts = h.d_level_fronts.as<int>() + S.level_ptr[l];
       const int nf = (int)(S.level_ptr[l + 1] - S.level_ptr[l]);
-      front_bwd_kernel<T><<<dim3(nf, nb), 256, sm, h.stream>>>(c, x);
+      if (P.lvl_maxu[l] > 0) {
+        const unsigned z = (unsigned)((P.lvl_maxk[l] + kSolveRows - 1) / kSolveRows);
+        front_bwd_u12_kernel<T><<<dim3(nf, nb, z), 256, (size_t)P.lvl_maxu[l] * sizeof(cplx<T>), h.stream>>>(c, x);
+        ++launches;
+      }
+      front_bwd_kernel<T><<<dim3(nf, nb), 256, smk, h.stream>>>(c, x);
       ++launches;
     }
     SS_CK(cudaGetLastError());
@@ -1063,7 +1169,7 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
   a.tiny = sizeof(T) == 8 ? (T)1e-13 : (T)1e-6;
   a.nperturb = npert.as<int>();
   sw.wstride = W;
-  const int maxit = sizeof(T) == 8 ? 2 : 40;
+  const int maxit = sizeof(T) == 8 ? 1 : 40;   // FP64: one refinement step
   const double tol = sizeof(T) == 8 ? 1e-15 : 1e-12;
   cudaEvent_t e0, e1, e2;
   cudaEventCreate(&e0);
