@@ -1,0 +1,121 @@
+"""Resonance / antiresonance extraction from a swept admittance curve (host side).
+
+Restates the fr/fa part of the reference's figure-of-merit module
+(``src/sawsim/metrics.py``), which judges the sweep's fr/fa criterion:
+
+* ``resonances`` :98-171 -- |Y|/f removes the static-capacitance slope; every
+  local maximum of |Y|/f (``_local_extrema`` :33-35) is paired with the lowest
+  |Y|/f sample before the next maximum; pairs whose minimum lies more than 15 %
+  above the peak frequency are bulk-wave humps and are dropped; the main pair is
+  the one with the largest relative dip (capped at 0.5), ties broken by the
+  highest peak;
+* ``_vfit`` :18-27 -- sub-sample refinement: vertex of a V through the extreme
+  sample and its neighbours, clipped to half a step (fr is fitted on 1/(|Y|/f),
+  fa on |Y|/f);
+* ``compare`` :188-199 -- fr/fa deviation in MHz and ppm, k2eff in %-points;
+* ``_rounded`` :174-185 -- GHz and MHz rounded to 0.1 kHz, other floats to 6
+  significant digits.
+
+Q extraction and the mode list of the reference are not restated: the sweep
+backend needs only fr, fa and k2eff to state its accuracy against FP64.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+K2_FORMULA = 'k2eff = pi^2/4 * (fa - fr) / fa'
+
+
+def _vertex(f, g, i):
+    """Frequency of the vertex of the V through samples i-1, i, i+1 of g (minimum at i)."""
+    if i <= 0 or i >= len(g) - 1:
+        return float(f[i])
+    half = 0.5 * (f[i + 1] - f[i - 1])
+    slope = max(g[i - 1] - g[i], g[i + 1] - g[i]) / half
+    if not slope > 0:
+        return float(f[i])
+    shift = (g[i - 1] - g[i + 1]) / (2.0 * slope)
+    return float(f[i] + min(max(shift, -half / 2), half / 2))
+
+
+def _maxima(y):
+    """Interior indices i with y[i] > y[i-1] and y[i] >= y[i+1]."""
+    mid = y[1:-1]
+    return np.flatnonzero((mid > y[:-2]) & (mid >= y[2:])) + 1
+
+
+def _minima(y):
+    return _maxima(-y)
+
+
+def _round(key, v):
+    if isinstance(v, float):
+        if key.endswith('_ghz'):
+            return round(v, 7)
+        if key.endswith('_mhz'):
+            return round(v, 4)
+        return float('%.6g' % v)
+    return v
+
+
+def resonances(frequency_hz, admittance) -> dict:
+    """fr / fa (GHz), k2eff and warnings of a sampled admittance (complex Y or |Y|)."""
+    f = np.asarray(frequency_hz, dtype=float)
+    mag = np.abs(np.asarray(admittance))
+    n = f.size
+    out = dict(fr_ghz=None, fa_ghz=None, k2eff=None, k2_formula=K2_FORMULA, frequency_step_mhz=None,
+               uncertainty_mhz=None, points_between_fr_fa=None, warnings=[])
+    if n < 5 or not np.all(np.isfinite(mag)):
+        out['warnings'].append('curve too short or contains non-finite values')
+        return out
+    step = float(np.max(np.diff(f)))
+    out['frequency_step_mhz'] = step * 1e-6
+    out['uncertainty_mhz'] = step * 0.5e-6
+    g = mag / f
+    inv = 1.0 / np.maximum(g, np.finfo(float).tiny)
+    peaks = _maxima(g)
+    pairs = []
+    for j, p in enumerate(peaks):
+        stop = int(peaks[j + 1]) if j + 1 < len(peaks) else n - 1
+        a = int(p) + int(np.argmin(g[p:stop + 1]))
+        if a == p:
+            continue
+        if a != n - 1 and f[a] - f[p] > 0.15 * f[p]:
+            continue
+        pairs.append(((g[p] - g[a]) / g[p], int(p), a))
+    if not pairs:
+        if int(np.argmax(g)) in (0, n - 1):
+            out['warnings'].append('peak_at_band_edge')
+        else:
+            out['warnings'].append('no_resonance_found')
+        return {k: _round(k, v) for k, v in out.items()}
+    _, r, a = max(pairs, key=lambda t: (min(t[0], 0.5), g[t[1]]))
+    fr = _vertex(f, inv, r)
+    out['fr_ghz'] = fr * 1e-9
+    if a == n - 1:
+        out['warnings'].append('antiresonance_not_found')
+    else:
+        fa = _vertex(f, g, a)
+        out['fa_ghz'] = fa * 1e-9
+        out['k2eff'] = math.pi ** 2 / 4 * (fa - fr) / fa
+        out['points_between_fr_fa'] = int(a - r - 1)
+        if a - r < 6:
+            out['warnings'].append('coarse_sampling')
+    if max(g[0], g[-1]) > 3 * g[r]:
+        out['warnings'].append('stronger_response_at_band_edge')
+    return {k: _round(k, v) for k, v in out.items()}
+
+
+def compare(reference: dict, candidate: dict) -> dict:
+    """fr/fa/k2eff deviation of ``candidate`` from ``reference`` (both from ``resonances``)."""
+    d = {}
+    for key in ('fr_ghz', 'fa_ghz'):
+        a, b = reference.get(key), candidate.get(key)
+        ok = a is not None and b is not None
+        d[key.replace('_ghz', '_diff_mhz')] = _round('_mhz', (b - a) * 1e3) if ok else None
+        d[key.replace('_ghz', '_diff_ppm')] = _round('', (b - a) / a * 1e6) if ok else None
+    a, b = reference.get('k2eff'), candidate.get('k2eff')
+    d['k2eff_diff_pct_points'] = _round('', (b - a) * 100) if a is not None and b is not None else None
+    return d
