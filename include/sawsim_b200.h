@@ -139,6 +139,18 @@ int ss_sweep(ss_handle *h, int n_f, const double *omega, double V, int precision
 int ss_solve_fields(ss_handle *h, double omega, double V, double *disp);
 
 /*
+ * Adjoint of the charge at one frequency: lambda (n_active x 2, the reference's
+ * active-DOF order) solves A_aa^T lambda = kq, where A_aa = Km_aa - w^2 Mm_aa
+ * (+ i w beta Dm_aa) and kq is the charge row kts = K^T s folded onto the
+ * active DOFs (sweep.py:301-305, :356-362), so that dQ = -lambda^T dA x for a
+ * perturbation dA of the condensed system.  The reference has no adjoint; this
+ * is the transposed solve with the same factors that its PARDISO/SuperLU call
+ * (sweep.py:346-353) would need.  Returns the solve status (SS_ENOCONV when the
+ * mixed-precision refinement did not reach its tolerance).
+ */
+int ss_solve_adjoint(ss_handle *h, double omega, int precision, double *lambda);
+
+/*
  * Counters of the last calls: out[0..n) filled with
  *  0 n_active, 1 n_fronts, 2 max_front, 3 factor_flops_per_point (complex fronts,
  *  8 real flops per complex multiply-add), 4 nnz(L+U), 5 analyze_s, 6 assemble_ms,

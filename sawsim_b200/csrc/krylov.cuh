@@ -11,11 +11,18 @@
 
 namespace ss {
 
-// y_f = A'(w_f) x_f
+// Sparse operator of the scaled condensed system: the CSR pattern (rp, ci) and,
+// for the transposed operator, the value slot of each entry (vp; nullptr = the
+// entry's own slot).
+struct MatOp {
+  const int64_t *rp, *ci, *vp;
+};
+
+// y_f = A'(w_f) x_f   (or A'(w_f)^T x_f with the transposed pattern)
 __global__ void spmv_kernel(int64_t n, int nb, const int64_t *__restrict__ rp, const int64_t *__restrict__ ci,
-                            const cd *__restrict__ K, const cd *__restrict__ M, const cd *__restrict__ D,
-                            const double *__restrict__ omega, double beta, const cd *__restrict__ x,
-                            cd *__restrict__ y) {
+                            const int64_t *__restrict__ vp, const cd *__restrict__ K, const cd *__restrict__ M,
+                            const cd *__restrict__ D, const double *__restrict__ omega, double beta,
+                            const cd *__restrict__ x, cd *__restrict__ y) {
   const int64_t R = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int f = blockIdx.y;
   if (R >= n || f >= nb) return;
@@ -23,8 +30,9 @@ __global__ void spmv_kernel(int64_t n, int nb, const int64_t *__restrict__ rp, c
   const cd *xf = x + (int64_t)f * n;
   cd acc{0.0, 0.0};
   for (int64_t t = rp[R]; t < rp[R + 1]; ++t) {
-    cd a = K[t] - M[t] * w2;
-    if (D) a = a + cmul(cd{0.0, w * beta}, D[t]);
+    const int64_t s = vp ? vp[t] : t;
+    cd a = K[s] - M[s] * w2;
+    if (D) a = a + cmul(cd{0.0, w * beta}, D[s]);
     acc = acc + cmul(a, xf[ci[t]]);
   }
   y[(int64_t)f * n + R] = acc;
@@ -109,7 +117,7 @@ struct KrylovWork {
 // precond(src, dst) applies M^-1 to nb vectors.  Returns the number of
 // preconditioner applications per frequency in `its`, converged flags in `conv`.
 template <class Precond>
-int fgmres(Handle &h, KrylovWork &kw, int nb, int m, int restarts, double tol, const cd *Kc, const cd *Mc,
+int fgmres(Handle &h, KrylovWork &kw, const MatOp &op, int nb, int m, int restarts, double tol, const cd *Kc, const cd *Mc,
            const cd *Dc, const double *d_omega, const cd *b, cd *x, Precond precond, std::vector<int> &its,
            std::vector<char> &conv) {
   const int64_t n = h.sym.n;
@@ -143,7 +151,7 @@ int fgmres(Handle &h, KrylovWork &kw, int nb, int m, int restarts, double tol, c
   std::vector<char> done(nb);
   for (int cyc = 0; cyc < restarts; ++cyc) {
     // r = b - A x  -> V_0
-    spmv_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, h.dc_ptr.as<int64_t>(), h.dc_idx.as<int64_t>(), Kc, Mc,
+    spmv_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, op.rp, op.ci, op.vp, Kc, Mc,
                                                     Dc, d_omega, h.beta, x, w);
     KCK(cudaMemcpyAsync(V, b, vec, cudaMemcpyDeviceToDevice, h.stream));
     {
@@ -174,7 +182,7 @@ int fgmres(Handle &h, KrylovWork &kw, int nb, int m, int restarts, double tol, c
       cd *Vj = V + (size_t)j * nb * n, *Zj = Z + (size_t)j * nb * n;
       int rc = precond(Vj, Zj);
       if (rc) return rc;
-      spmv_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, h.dc_ptr.as<int64_t>(), h.dc_idx.as<int64_t>(), Kc,
+      spmv_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, op.rp, op.ci, op.vp, Kc,
                                                       Mc, Dc, d_omega, h.beta, Zj, w);
       // classical Gram-Schmidt, twice
       for (int pass = 0; pass < 2; ++pass) {
@@ -249,7 +257,7 @@ int fgmres(Handle &h, KrylovWork &kw, int nb, int m, int restarts, double tol, c
     KCK(cudaGetLastError());
   }
   // final true residual check
-  spmv_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, h.dc_ptr.as<int64_t>(), h.dc_idx.as<int64_t>(), Kc, Mc, Dc,
+  spmv_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, op.rp, op.ci, op.vp, Kc, Mc, Dc,
                                                   d_omega, h.beta, x, w);
   {
     std::vector<cd> one(nb, cd{1.0, 0.0});

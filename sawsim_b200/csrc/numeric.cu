@@ -10,6 +10,7 @@
 #include "ss_internal.h"
 #include "dev_complex.cuh"
 #include "krylov.cuh"
+#include "tc_gemm.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -100,10 +101,11 @@ __global__ void charge_kernel(int64_t n, const cd *__restrict__ kq, const double
 }
 
 // r[f] = b[f] - A'(w_f) x[f]   (scaled system, FP64), and per-row |r|, |x| maxima
+// (vp: value slot of each pattern entry, for the transposed operator; nullptr = own slot)
 __global__ void residual_kernel(int64_t n, int nb, const int64_t *__restrict__ rp, const int64_t *__restrict__ ci,
-                                const cd *__restrict__ K, const cd *__restrict__ M, const cd *__restrict__ D,
-                                const double *__restrict__ omega, double beta, const cd *__restrict__ b,
-                                const cd *__restrict__ x, cd *__restrict__ r) {
+                                const int64_t *__restrict__ vp, const cd *__restrict__ K, const cd *__restrict__ M,
+                                const cd *__restrict__ D, const double *__restrict__ omega, double beta,
+                                const cd *__restrict__ b, const cd *__restrict__ x, cd *__restrict__ r) {
   const int64_t R = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int f = blockIdx.y;
   if (R >= n || f >= nb) return;
@@ -111,8 +113,9 @@ __global__ void residual_kernel(int64_t n, int nb, const int64_t *__restrict__ r
   const cd *xf = x + (int64_t)f * n;
   cd acc = b[(int64_t)f * n + R];
   for (int64_t t = rp[R]; t < rp[R + 1]; ++t) {
-    cd a = K[t] - M[t] * w2;
-    if (D) a = a + cmul(cd{0.0, w * beta}, D[t]);
+    const int64_t s = vp ? vp[t] : t;
+    cd a = K[s] - M[s] * w2;
+    if (D) a = a + cmul(cd{0.0, w * beta}, D[s]);
     acc = acc - cmul(a, xf[ci[t]]);
   }
   r[(int64_t)f * n + R] = acc;
@@ -442,12 +445,6 @@ __global__ void __launch_bounds__(256) front_swap_trsm_kernel(FrontArgs<T> a, in
     if (i < w) F[(int64_t)(j0 + i) * ld + c] = v[i];
 }
 
-// One 64x64 output tile of C -= A B inside front f: rows [r0, rhi), cols [c0, chi),
-// contraction [kk0, kk1); A = F[:, kk], B = F[kk, :].
-struct GemmTask {
-  int f, r0, c0, rhi, chi, kk0, kk1;
-};
-
 constexpr int kGemmBK = 8;
 // tile shapes: square (Schur update), skinny (panel column update), short (U row update)
 enum GemmShape { kSquare = 0, kSkinny = 1, kShort = 2 };
@@ -718,6 +715,189 @@ __global__ void __launch_bounds__(256) front_bwd_kernel(FrontArgs<T> a, cd *__re
   for (int i = threadIdx.x; i < k; i += blockDim.x) xf[p0 + i] = cd{(double)z[i].x, (double)z[i].y};
 }
 
+// ------------------------------------------------------------------ transposed solves
+// A'^T mu = c with P A' = L U (P: the row swaps inside each front, in pivot
+// order):  U^T w = c (levels bottom-up), L^T z = w (levels top-down), mu = P^T z.
+// The adjoint of the charge functional and the dual-weighted charge correction
+// of the mixed-precision sweep use these.
+
+// U^T solve for one level: v = c[pivots] + the children's update vectors;
+// U11^T w = v[0:k] (lower triangular, non-unit); the update rows keep the
+// children's sums and front_tfwd_u12_kernel subtracts U12^T w.  w -> x[pivots].
+template <class T>
+__global__ void __launch_bounds__(256) front_tfwd_kernel(FrontArgs<T> a, const cd *__restrict__ c,
+                                                         cd *__restrict__ x, cplx<T> *__restrict__ wv,
+                                                         int64_t wstride) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T> *v = reinterpret_cast<cplx<T> *>(smem_raw);
+  const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
+  const int k = a.k[f], m = a.m[f], ld = a.ld[f];
+  const cplx<T> *F = a.arena + (int64_t)fq * a.stride + a.off[f];
+  const int64_t p0 = a.p0[f];
+  for (int i = threadIdx.x; i < m; i += blockDim.x)
+    v[i] = i < k ? to_t<T>(c[(int64_t)fq * a.n + p0 + i]) : cplx<T>{0, 0};
+  __syncthreads();
+  cplx<T> *w = wv + (int64_t)fq * wstride;
+  for (int64_t cc = a.child_ptr[f]; cc < a.child_ptr[f + 1]; ++cc) {
+    const int ch = a.child[cc];
+    const int nn = a.m[ch] - a.k[ch];
+    const int *rel = a.relpos + a.relpos_ptr[ch];
+    const cplx<T> *wc = w + a.relpos_ptr[ch];
+    for (int i = threadIdx.x; i < nn; i += blockDim.x) v[rel[i]] = v[rel[i]] + wc[i];
+    __syncthreads();
+  }
+  // entry (i, t) of U11^T is F[t * ld + i]; warp 0 solves each 32-wide diagonal
+  // block, then one thread per row below it subtracts the block (coalesced in r)
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int jb = 0; jb < k; jb += 32) {
+    const int je = min(k, jb + 32), bw = je - jb;
+    if (wid == 0) {
+      cplx<T> xv = lane < bw ? v[jb + lane] : cplx<T>{0, 0};
+      for (int t = 0; t < bw; ++t) {
+        if (lane == t) xv = cdiv(xv, F[(int64_t)(jb + t) * ld + jb + t]);
+        cplx<T> xt;
+        xt.x = __shfl_sync(0xffffffffu, xv.x, t);
+        xt.y = __shfl_sync(0xffffffffu, xv.y, t);
+        if (lane > t && lane < bw) xv = cfms(xv, F[(int64_t)(jb + t) * ld + jb + lane], xt);
+      }
+      if (lane < bw) v[jb + lane] = xv;
+    }
+    __syncthreads();
+    for (int r = je + threadIdx.x; r < k; r += blockDim.x) {
+      cplx<T> acc = v[r];
+      for (int t = 0; t < bw; ++t) acc = cfms(acc, F[(int64_t)(jb + t) * ld + r], v[jb + t]);
+      v[r] = acc;
+    }
+    __syncthreads();
+  }
+  for (int r = k + threadIdx.x; r < m; r += blockDim.x) w[a.relpos_ptr[f] + r - k] = v[r];
+  for (int i = threadIdx.x; i < k; i += blockDim.x) x[(int64_t)fq * a.n + p0 + i] = cd{(double)v[i].x, (double)v[i].y};
+}
+
+// Update rows of the U^T solve: w[r - k] -= sum_i U12[i, r] x_i; CTA per (front,
+// frequency, 256 update rows), one thread per row (coalesced column reads).
+template <class T>
+__global__ void __launch_bounds__(256) front_tfwd_u12_kernel(FrontArgs<T> a, const cd *__restrict__ x,
+                                                             cplx<T> *__restrict__ wv, int64_t wstride) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T> *y = reinterpret_cast<cplx<T> *>(smem_raw);
+  const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
+  const int k = a.k[f], m = a.m[f], ld = a.ld[f];
+  const int rb = k + blockIdx.z * blockDim.x;
+  if (rb >= m) return;
+  const cplx<T> *F = a.arena + (int64_t)fq * a.stride + a.off[f];
+  const int64_t p0 = a.p0[f];
+  for (int i = threadIdx.x; i < k; i += blockDim.x) y[i] = to_t<T>(x[(int64_t)fq * a.n + p0 + i]);
+  __syncthreads();
+  const int r = rb + threadIdx.x;
+  if (r >= m) return;
+  cplx<T> acc{0, 0};
+  for (int i = 0; i < k; ++i) acc = acc + cmul(F[(int64_t)i * ld + r], y[i]);
+  cplx<T> *w = wv + (int64_t)fq * wstride + a.relpos_ptr[f] - k;
+  w[r] = w[r] - acc;
+}
+
+// First phase of the L^T solve (levels top-down): x[pivots] -= L21^T x_U, with
+// x_U the ancestors' solution at this front's update rows; CTA per (front,
+// frequency, 256 pivots), one thread per pivot (coalesced row reads).
+template <class T>
+__global__ void __launch_bounds__(256) front_tbwd_l21_kernel(FrontArgs<T> a, cd *__restrict__ x) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T> *xu = reinterpret_cast<cplx<T> *>(smem_raw);
+  const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
+  const int k = a.k[f], m = a.m[f], ld = a.ld[f];
+  const int ib = blockIdx.z * blockDim.x;
+  if (ib >= k || m == k) return;
+  const cplx<T> *F = a.arena + (int64_t)fq * a.stride + a.off[f];
+  cd *xf = x + (int64_t)fq * a.n;
+  const int64_t *rows = a.rows + a.rows_ptr[f];
+  for (int i = threadIdx.x; i < m - k; i += blockDim.x) xu[i] = to_t<T>(xf[rows[k + i]]);
+  __syncthreads();
+  const int i = ib + threadIdx.x;
+  if (i >= k) return;
+  cplx<T> acc{0, 0};
+  for (int r = 0; r < m - k; ++r) acc = acc + cmul(F[(int64_t)(k + r) * ld + i], xu[r]);
+  const int64_t p = a.p0[f] + i;
+  xf[p] = cd{xf[p].x - (double)acc.x, xf[p].y - (double)acc.y};
+}
+
+// L11^T z = x[pivots] (upper triangular, unit diagonal; entry (i, t) is
+// F[t * ld + i]) from the last pivot up, then this front's row swaps undone in
+// reverse pivot order; the result -> x[pivots].  The forward solve applies a
+// front's swaps before its L11 solve, so the transposed sequence undoes them
+// right after the L11^T solve, before any descendant reads these entries.
+template <class T>
+__global__ void __launch_bounds__(256) front_tbwd_kernel(FrontArgs<T> a, cd *__restrict__ x) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T> *z = reinterpret_cast<cplx<T> *>(smem_raw);
+  const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
+  const int k = a.k[f], ld = a.ld[f];
+  const cplx<T> *F = a.arena + (int64_t)fq * a.stride + a.off[f];
+  const int64_t p0 = a.p0[f];
+  cd *xf = x + (int64_t)fq * a.n;
+  for (int i = threadIdx.x; i < k; i += blockDim.x) z[i] = to_t<T>(xf[p0 + i]);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int je = k; je > 0; je -= 32) {
+    const int jb = max(0, je - 32), bw = je - jb;
+    if (wid == 0) {
+      cplx<T> xv = lane < bw ? z[jb + lane] : cplx<T>{0, 0};
+      for (int t = bw - 1; t > 0; --t) {
+        cplx<T> xt;
+        xt.x = __shfl_sync(0xffffffffu, xv.x, t);
+        xt.y = __shfl_sync(0xffffffffu, xv.y, t);
+        if (lane < t) xv = cfms(xv, F[(int64_t)(jb + t) * ld + jb + lane], xt);
+      }
+      if (lane < bw) z[jb + lane] = xv;
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < jb; r += blockDim.x) {
+      cplx<T> acc = z[r];
+      for (int t = 0; t < bw; ++t) acc = cfms(acc, F[(int64_t)(jb + t) * ld + r], z[jb + t]);
+      z[r] = acc;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const int *piv = a.piv + (int64_t)fq * a.n + p0;
+    for (int j = k - 1; j >= 0; --j) {
+      const int p = piv[j];
+      if (p != j) {
+        const cplx<T> t = z[j];
+        z[j] = z[p];
+        z[p] = t;
+      }
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < k; i += blockDim.x) xf[p0 + i] = cd{(double)z[i].x, (double)z[i].y};
+}
+
+// out[f] = sum_R u[f][R] * v[f][R] (bilinear, no conjugate), fixed-order tree
+__global__ void dotu_kernel(int64_t n, const cd *__restrict__ u, const cd *__restrict__ v, cd *__restrict__ out) {
+  __shared__ cd red[256];
+  const int f = blockIdx.x;
+  cd acc{0.0, 0.0};
+  for (int64_t R = threadIdx.x; R < n; R += blockDim.x) acc = acc + cmul(u[(int64_t)f * n + R], v[(int64_t)f * n + R]);
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[f] = red[0];
+}
+
+// c[f][R] = kq[R] * cs[R] for every frequency of the chunk (the charge row in the
+// scaled variables: Q = c^T x' + V Qz)
+__global__ void charge_row_kernel(int64_t n, int nb, const cd *__restrict__ kq, const double *__restrict__ cs,
+                                  cd *__restrict__ c) {
+  const int64_t R = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int f = blockIdx.y;
+  if (R >= n || f >= nb) return;
+  c[(int64_t)f * n + R] = kq[R] * cs[R];
+}
+
 // x += dx and per-frequency max |dx|, max |x| (for the refinement stopping test)
 __global__ void axpy_norm_kernel(int64_t n, cd *__restrict__ x, const cd *__restrict__ dx,
                                  double *__restrict__ nrm) {
@@ -774,12 +954,16 @@ struct Plan {
   std::vector<int> lvl_maxk, lvl_maxu;     // per level max k and max m-k (solve grids)
 };
 
+static void add_tiles(std::vector<GemmTask> &v, int bm, int bn, int f, int r0, int r1, int c0, int c1, int k0,
+                      int k1) {
+  for (int r = r0; r < r1; r += bm)
+    for (int c = c0; c < c1; c += bn) v.push_back(GemmTask{f, r, c, r1, c1, k0, k1});
+}
 static void add_tiles(std::vector<GemmTask> &v, int shape, int f, int r0, int r1, int c0, int c1, int k0, int k1) {
-  for (int r = r0; r < r1; r += tile_bm(shape))
-    for (int c = c0; c < c1; c += tile_bn(shape)) v.push_back(GemmTask{f, r, c, r1, c1, k0, k1});
+  add_tiles(v, tile_bm(shape), tile_bn(shape), f, r0, r1, c0, c1, k0, k1);
 }
 
-Plan *build_plan(Handle &h, int small_m) {
+Plan *build_plan(Handle &h, int small_m, bool tensor_schur) {
   Symbolic &S = h.sym;
   Plan *P = new Plan();
   P->small_m = small_m;
@@ -843,7 +1027,12 @@ Plan *build_plan(Handle &h, int small_m) {
   for (int l = 0; l < S.nlevel; ++l) {
     for (int q = P->large_ptr[l]; q < P->large_ptr[l + 1]; ++q) {
       const int f = P->fronts_large[q], k = S.k[f], m = S.m[f];
-      if (m > k) add_tiles(P->tasks, kSquare, f, k, m, k, m, 0, k);
+      if (m > k) {
+        if (tensor_schur)   // complex64 Schur updates on tcgen05 tiles
+          add_tiles(P->tasks, tc::BM, tc::BN, f, k, m, k, m, 0, k);
+        else
+          add_tiles(P->tasks, kSquare, f, k, m, k, m, 0, k);
+      }
       P->schur_flops += 8.0 * k * (double)(m - k) * (m - k);
     }
     sp.push_back((int64_t)P->tasks.size());
@@ -926,6 +1115,15 @@ namespace ss {
 constexpr int kKrylovM = 30;            // FGMRES restart length (mixed precision)
 constexpr int kKrylovRestarts = 4;
 constexpr double kKrylovTol = 1e-13;    // relative residual target
+constexpr double kKrylovTolAdj = 1e-13; // same for the adjoint
+static int env_int(const char *name, int dflt) {
+  const char *v = getenv(name);
+  return v ? atoi(v) : dflt;
+}
+static double env_double(const char *name, double dflt) {
+  const char *v = getenv(name);
+  return v ? atof(v) : dflt;
+}
 
 template <class T>
 static int small_limit() { return sizeof(T) == 8 ? 96 : 128; }  // cd: 96^2*16, cf: 128^2*8 bytes
@@ -983,6 +1181,7 @@ struct Sweeper {
   FrontArgs<T> a{};
   int64_t wstride = 0;
   int launches = 0, schur_launches = 0;
+  int *tc_err = nullptr;                     // device flag: a tensor-core tile timed out
   std::vector<cudaEvent_t> ev;               // Schur GEMM timing, one pair per level
   int nev = 0;
   double schur_ms = 0;
@@ -1044,7 +1243,11 @@ struct Sweeper {
       const int64_t t0 = P.schur_ptr[l], t1 = P.schur_ptr[l + 1];
       if (t1 > t0) {
         cudaEventRecord(ev[2 * nev], h.stream);
-        front_gemm_kernel<T, kSquare><<<dim3((unsigned)(t1 - t0), nb), 256, 0, h.stream>>>(b, tasks + t0);
+        if (sizeof(T) == 4)
+          tc::front_tc_gemm_kernel<<<dim3((unsigned)(t1 - t0), nb), tc::THREADS, tc::SMEM_BYTES, h.stream>>>(
+              reinterpret_cast<cf *>(b.arena), b.stride, b.off, b.ld, tasks + t0, tc_err);
+        else
+          front_gemm_kernel<T, kSquare><<<dim3((unsigned)(t1 - t0), nb), 256, 0, h.stream>>>(b, tasks + t0);
         cudaEventRecord(ev[2 * nev + 1], h.stream);
         ++nev;
         ++launches;
@@ -1087,7 +1290,60 @@ struct Sweeper {
     SS_CK(cudaGetLastError());
     return SS_OK;
   }
+  // mu <- A'^-T c for nb frequencies (same factors; wv workspace)
+  int solve_t(int nb, const cd *cvec, cd *mu, cplx<T> *wv) {
+    const Symbolic &S = h.sym;
+    const size_t sm = (size_t)S.max_m * sizeof(cplx<T>);
+    const size_t smk = (size_t)std::max(1, S.max_k) * sizeof(cplx<T>);
+    for (int l = 0; l < S.nlevel; ++l) {
+      FrontArgs<T> c = a;
+      c.fronts = h.d_level_fronts.as<int>() + S.level_ptr[l];
+      const int nf = (int)(S.level_ptr[l + 1] - S.level_ptr[l]);
+      front_tfwd_kernel<T><<<dim3(nf, nb), 256, sm, h.stream>>>(c, cvec, mu, wv, wstride);
+      ++launches;
+      if (P.lvl_maxu[l] > 0) {
+        const unsigned z = (unsigned)((P.lvl_maxu[l] + 255) / 256);
+        front_tfwd_u12_kernel<T><<<dim3(nf, nb, z), 256, smk, h.stream>>>(c, mu, wv, wstride);
+        ++launches;
+      }
+    }
+    for (int l = S.nlevel - 1; l >= 0; --l) {
+      FrontArgs<T> c = a;
+      c.fronts = h.d_level_fronts.as<int>() + S.level_ptr[l];
+      const int nf = (int)(S.level_ptr[l + 1] - S.level_ptr[l]);
+      if (P.lvl_maxu[l] > 0) {
+        const unsigned z = (unsigned)((P.lvl_maxk[l] + 255) / 256);
+        front_tbwd_l21_kernel<T><<<dim3(nf, nb, z), 256, (size_t)P.lvl_maxu[l] * sizeof(cplx<T>), h.stream>>>(c, mu);
+        ++launches;
+      }
+      front_tbwd_kernel<T><<<dim3(nf, nb), 256, smk, h.stream>>>(c, mu);
+      ++launches;
+    }
+    SS_CK(cudaGetLastError());
+    return SS_OK;
+  }
 };
+
+// Transposed condensed pattern in the new order (built once): row C of A'^T
+// lists the rows R with an entry (R, C), ascending, and the slot of (R, C).
+static int build_transpose(Handle &h) {
+  if (h.dct_ptr.p) return SS_OK;
+  const int64_t n = h.sym.n;
+  std::vector<int64_t> tp(n + 1, 0), ti(h.c_nnz), ts(h.c_nnz);
+  for (int64_t t = 0; t < h.c_nnz; ++t) ++tp[h.c_idx[t] + 1];
+  for (int64_t c = 0; c < n; ++c) tp[c + 1] += tp[c];
+  std::vector<int64_t> fill(tp.begin(), tp.end() - 1);
+  for (int64_t R = 0; R < n; ++R)
+    for (int64_t t = h.c_ptr[R]; t < h.c_ptr[R + 1]; ++t) {
+      const int64_t q = fill[h.c_idx[t]]++;
+      ti[q] = R;
+      ts[q] = t;
+    }
+  SS_CK(dupload(h.dct_ptr, tp));
+  SS_CK(dupload(h.dct_idx, ti));
+  SS_CK(dupload(h.dct_src, ts));
+  return SS_OK;
+}
 
 }  // namespace ss
 
@@ -1095,18 +1351,32 @@ namespace ss {
 
 template <class T>
 static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double *Qout, int *status,
-                      int *iters, double *disp) {
+                      int *iters, double *disp, const SweepExtra *ex) {
   Symbolic &S = h.sym;
   const int64_t n = S.n;
   const int pi = sizeof(T) == 8 ? 0 : 1;
   if (!h.plan[pi]) {
-    Plan *P = build_plan(h, small_limit<T>());
+    Plan *P = build_plan(h, small_limit<T>(), sizeof(T) == 4);
     h.plan[pi] = P;
     SS_CK(dupload(P->d_small, P->fronts_small));
     SS_CK(dupload(P->d_large, P->fronts_large));
     SS_CK(dupload(P->d_tasks, P->tasks));
     SS_CK(cudaFuncSetAttribute(front_small_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                small_limit<T>() * small_limit<T>() * (int)sizeof(cplx<T>)));
+    SS_CK(cudaFuncSetAttribute(tc::front_tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               tc::SMEM_BYTES));
+    // solve kernels stage a whole front vector in shared memory
+    const int vec = (int)std::min<int64_t>(227 * 1024, (int64_t)S.max_m * (int64_t)sizeof(cplx<T>));
+    if (vec > 48 * 1024) {
+      SS_CK(cudaFuncSetAttribute(front_fwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vec));
+      SS_CK(cudaFuncSetAttribute(front_tfwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vec));
+      SS_CK(cudaFuncSetAttribute(front_fwd_l21_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vec));
+      SS_CK(cudaFuncSetAttribute(front_tfwd_u12_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vec));
+      SS_CK(cudaFuncSetAttribute(front_bwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vec));
+      SS_CK(cudaFuncSetAttribute(front_tbwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vec));
+      SS_CK(cudaFuncSetAttribute(front_bwd_u12_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vec));
+      SS_CK(cudaFuncSetAttribute(front_tbwd_l21_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vec));
+    }
   }
   Plan &P = *static_cast<Plan *>(h.plan[pi]);
   double wmax = 0;
@@ -1116,16 +1386,24 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
     if (rc) return rc;
   }
   const int64_t W = S.relpos_ptr[S.nfront];
-  const double krylov = sizeof(T) == 4 ? (2.0 * kKrylovM + 2) * n * sizeof(cd) : 0.0;
-  const double per = (double)S.arena * sizeof(cplx<T>) + n * 4.0 + W * (double)sizeof(cplx<T>) + n * 64.0 + krylov + 256;
+  const int krylov_m = env_int("SS_KRYLOV_M", kKrylovM);
+  const int krylov_restarts = env_int("SS_KRYLOV_RESTARTS", kKrylovRestarts);
+  const double tol_p = env_double("SS_KRYLOV_TOL", kKrylovTol);
+  const double tol_a = env_double("SS_KRYLOV_TOL_ADJ", kKrylovTolAdj);
+  const double krylov = sizeof(T) == 4 ? (2.0 * krylov_m + 2) * n * sizeof(cd) : 0.0;
+  // the mixed sweep always solves the adjoint too (dual-weighted charge correction)
+  const bool correct = sizeof(T) == 4;
+  const bool need_adjoint = correct || (ex && ex->per_chunk);
+  const double per = (double)S.arena * sizeof(cplx<T>) + n * 4.0 + W * (double)sizeof(cplx<T>) + n * 64.0 + krylov +
+                     (need_adjoint ? 32.0 * n : 0.0) + 256;
   KrylovWork kw;
   size_t fr = 0, tot = 0;
   SS_CK(cudaMemGetInfo(&fr, &tot));
   // device work buffers persist in the handle: repeated sweeps reuse them
   DBuf &arena = h.wk[0], &piv = h.wk[1], &wv = h.wk[2], &b = h.wk[3], &x = h.wk[4], &r = h.wk[5], &dx = h.wk[6],
-       &dom = h.wk[7], &npert = h.wk[8], &nrm = h.wk[9], &dQ = h.wk[10];
+       &dom = h.wk[7], &npert = h.wk[8], &nrm = h.wk[9], &dQ = h.wk[10], &mu = h.wk[11], &cvec = h.wk[12];
   // the chunk size counts only memory not already held by these buffers
-  for (int i = 0; i < 11; ++i) fr += h.wk[i].bytes;
+  for (int i = 0; i < 13; ++i) fr += h.wk[i].bytes;
   int B = (int)std::max(1.0, std::min((double)n_f, std::min(256.0, (0.85 * (double)fr - 512e6) / per)));
   // a buffer that must grow is released first so that old and new never coexist
   if ((size_t)B * S.arena * sizeof(cplx<T>) > arena.bytes) arena.release();
@@ -1139,8 +1417,18 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
   SS_CK(dalloc(dom, B * sizeof(double)));
   SS_CK(dalloc(npert, B * sizeof(int)));
   SS_CK(dalloc(nrm, 2 * B * sizeof(double)));
-  SS_CK(dalloc(dQ, B * sizeof(cd)));
+  SS_CK(dalloc(dQ, 2 * B * sizeof(cd)));
+  if (need_adjoint) {
+    SS_CK(dalloc(mu, (size_t)B * n * sizeof(cd)));
+    SS_CK(dalloc(cvec, (size_t)B * n * sizeof(cd)));
+    int rc = build_transpose(h);
+    if (rc) return rc;
+  }
+  DBuf &tcerr = h.wk[13];
+  SS_CK(dalloc(tcerr, sizeof(int)));
+  SS_CK(cudaMemsetAsync(tcerr.p, 0, sizeof(int), h.stream));
   Sweeper<T> sw(h, P);
+  sw.tc_err = tcerr.as<int>();
   FrontArgs<T> &a = sw.a;
   a.k = h.d_k.as<int>();
   a.m = h.d_m.as<int>();
@@ -1210,19 +1498,20 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
     std::fill(conv.begin(), conv.end(), 0);
     std::fill(hit.begin(), hit.end(), 0);
     const bool use_krylov = sizeof(T) == 4 || getenv("SS_FP64_KRYLOV") != nullptr;
+    const MatOp opA{h.dc_ptr.as<int64_t>(), h.dc_idx.as<int64_t>(), nullptr};
     if (use_krylov) {
       // FGMRES-IR: FP64 Krylov, complex64 factors as right preconditioner
       std::vector<int> kits;
       std::vector<char> kconv;
       auto pre = [&](const cd *src, cd *dst) { return sw.solve(nb, src, dst, wv.as<cplx<T>>()); };
-      rc = fgmres(h, kw, nb, kKrylovM, kKrylovRestarts, kKrylovTol, a.Kc, a.Mc, a.Dc, dom.as<double>(), b.as<cd>(),
+      rc = fgmres(h, kw, opA, nb, krylov_m, krylov_restarts, tol_p, a.Kc, a.Mc, a.Dc, dom.as<double>(), b.as<cd>(),
                   x.as<cd>(), pre, kits, kconv);
       if (rc) return rc;
       for (int f = 0; f < nb; ++f) hit[f] = kits[f], conv[f] = kconv[f];
     }
     if (getenv("SS_DEBUG_IR")) {
       // backward error of the direct solve: |b - A x| / |b|, and the solution size
-      residual_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, h.dc_ptr.as<int64_t>(), h.dc_idx.as<int64_t>(),
+      residual_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, h.dc_ptr.as<int64_t>(), h.dc_idx.as<int64_t>(), nullptr,
                                                           a.Kc, a.Mc, a.Dc, dom.as<double>(), h.beta, b.as<cd>(),
                                                           x.as<cd>(), r.as<cd>());
       norm2_kernel<<<nb, 256, 0, h.stream>>>(n, r.as<cd>(), nrm.as<double>());
@@ -1234,7 +1523,7 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
               q[0] / q[nb], q[nb - 1] / q[2 * nb - 1]);
     }
     for (int it = 0; it < (use_krylov ? 0 : maxit); ++it) {
-      residual_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, h.dc_ptr.as<int64_t>(), h.dc_idx.as<int64_t>(),
+      residual_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, h.dc_ptr.as<int64_t>(), h.dc_idx.as<int64_t>(), nullptr,
                                                           a.Kc, a.Mc, a.Dc, dom.as<double>(), h.beta, b.as<cd>(),
                                                           x.as<cd>(), r.as<cd>());
       rc = sw.solve(nb, r.as<cd>(), dx.as<cd>(), wv.as<cplx<T>>());
@@ -1254,6 +1543,46 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
       }
       if (all) break;
     }
+    // adjoint of the charge functional: A'^T mu = c with c = cs * kq (Q = c^T x' + V Qz)
+    std::vector<cd> corr(nb, cd{0.0, 0.0});
+    std::vector<char> aconv(nb, 1);
+    if (need_adjoint) {
+      const MatOp opT{h.dct_ptr.as<int64_t>(), h.dct_idx.as<int64_t>(), h.dct_src.as<int64_t>()};
+      charge_row_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, h.dks.as<cd>() + n, h.dcol_scale.as<double>(),
+                                                          cvec.as<cd>());
+      rc = sw.solve_t(nb, cvec.as<cd>(), mu.as<cd>(), wv.as<cplx<T>>());
+      if (rc) return rc;
+      if (use_krylov) {
+        std::vector<int> kits;
+        std::vector<char> kconv;
+        auto pre = [&](const cd *src, cd *dst) { return sw.solve_t(nb, src, dst, wv.as<cplx<T>>()); };
+        rc = fgmres(h, kw, opT, nb, krylov_m, krylov_restarts, tol_a, a.Kc, a.Mc, a.Dc, dom.as<double>(),
+                    cvec.as<cd>(), mu.as<cd>(), pre, kits, kconv);
+        if (rc) return rc;
+        for (int f = 0; f < nb; ++f) hit[f] += kits[f], aconv[f] = kconv[f];
+      } else {
+        // one FP64 refinement step, as for the primal solution
+        residual_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, opT.rp, opT.ci, opT.vp, a.Kc, a.Mc, a.Dc,
+                                                            dom.as<double>(), h.beta, cvec.as<cd>(), mu.as<cd>(),
+                                                            r.as<cd>());
+        rc = sw.solve_t(nb, r.as<cd>(), dx.as<cd>(), wv.as<cplx<T>>());
+        if (rc) return rc;
+        axpy_norm_kernel<<<nb, 256, 0, h.stream>>>(n, mu.as<cd>(), dx.as<cd>(), nrm.as<double>());
+      }
+      if (correct) {
+        // dual-weighted correction: Q = c^T x + mu^T (b - A' x) is exact up to
+        // (mu_exact - mu)^T (b - A' x), the product of the two solves' errors
+        residual_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, h.dc_ptr.as<int64_t>(), h.dc_idx.as<int64_t>(),
+                                                            nullptr, a.Kc, a.Mc, a.Dc, dom.as<double>(), h.beta,
+                                                            b.as<cd>(), x.as<cd>(), r.as<cd>());
+        dotu_kernel<<<nb, 256, 0, h.stream>>>(n, mu.as<cd>(), r.as<cd>(), dQ.as<cd>() + B);
+        SS_CK(cudaMemcpyAsync(corr.data(), dQ.as<cd>() + B, nb * sizeof(cd), cudaMemcpyDeviceToHost, h.stream));
+      }
+      if (ex && ex->per_chunk) {
+        rc = ex->per_chunk(c0, nb, x.as<cd>(), mu.as<cd>());
+        if (rc) return rc;
+      }
+    }
     charge_kernel<<<nb, 256, 0, h.stream>>>(n, h.dks.as<cd>() + n, h.dcol_scale.as<double>(), x.as<cd>(),
                                             h.dQz.as<cd>(), V, dQ.as<cd>());
     SS_CK(cudaGetLastError());
@@ -1262,7 +1591,11 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
     SS_CK(cudaStreamSynchronize(h.stream));
     for (int f = 0; f < nb; ++f) {
       perturbed += hp[f];
-      if (status) status[c0 + f] = (sizeof(T) == 4 && !conv[f]) ? SS_ENOCONV : SS_OK;
+      if (correct) {
+        Qout[2 * (int64_t)(c0 + f)] += corr[f].x;
+        Qout[2 * (int64_t)(c0 + f) + 1] += corr[f].y;
+      }
+      if (status) status[c0 + f] = (sizeof(T) == 4 && !(conv[f] && aconv[f])) ? SS_ENOCONV : SS_OK;
       if (iters) iters[c0 + f] = hit[f];
     }
     if (disp) {
@@ -1286,6 +1619,11 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
   }
   cudaEventRecord(eall1, h.stream);
   cudaEventSynchronize(eall1);
+  {
+    int e = 0;
+    SS_CK(cudaMemcpy(&e, tcerr.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) return fail(h, SS_ETIMEOUT, "sweep: a tensor-core front update timed out waiting for its MMAs");
+  }
   float total_f = 0;
   cudaEventElapsedTime(&total_f, eall0, eall1);
   const double total_ms = total_f;
@@ -1309,9 +1647,9 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
 }
 
 int run_sweep(Handle &h, int n_f, const double *omega, double V, int precision, double *Q, int *status,
-              int *iters, double *disp_out) {
-  if (precision == SS_PREC_MIXED) return sweep_impl<float>(h, n_f, omega, V, Q, status, iters, disp_out);
-  return sweep_impl<double>(h, n_f, omega, V, Q, status, iters, disp_out);
+              int *iters, double *disp_out, const SweepExtra *ex) {
+  if (precision == SS_PREC_MIXED) return sweep_impl<float>(h, n_f, omega, V, Q, status, iters, disp_out, ex);
+  return sweep_impl<double>(h, n_f, omega, V, Q, status, iters, disp_out, ex);
 }
 
 }  // namespace ss

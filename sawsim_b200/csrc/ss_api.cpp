@@ -308,3 +308,32 @@ extern "C" int ss_stats(const ss_handle *hp, double *out, int n) {
   for (int i = 0; i < n && i < 24; ++i) out[i] = hp->h.st[i];
   return SS_OK;
 }
+
+extern "C" int ss_solve_adjoint(ss_handle *hp, double omega, int precision, double *lambda) {
+  H_CHECK(hp);
+  if (!h.analyzed) return fail(h, SS_ESTATE, "adjoint: analyze first");
+  if (!lambda || !(omega > 0.0)) return fail(h, SS_EINVAL, "adjoint: bad arguments");
+  if (precision != SS_PREC_FP64 && precision != SS_PREC_MIXED) return fail(h, SS_EINVAL, "adjoint: bad precision");
+  const int64_t n = h.sym.n;
+  std::vector<cplx_d> mu(n);
+  std::vector<double> rs(n);
+  SweepExtra ex;
+  ex.per_chunk = [&](int, int, const cplx<double> *, const cplx<double> *dmu) -> int {
+    cudaError_t e = cudaMemcpyAsync(mu.data(), dmu, n * sizeof(cplx_d), cudaMemcpyDeviceToHost, h.stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(rs.data(), h.drow_scale.p, n * sizeof(double), cudaMemcpyDeviceToHost, h.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h.stream);
+    return e == cudaSuccess ? SS_OK : cuda_fail(h, e, "adjoint copy");
+  };
+  double Q[2];
+  int st = 0, it = 0;
+  int rc = run_sweep(h, 1, &omega, 1.0, precision, Q, &st, &it, nullptr, &ex);
+  if (rc) return rc;
+  // lambda = Dr mu' in the reference's active-DOF order
+  for (int64_t P = 0; P < n; ++P) {
+    const int64_t R = h.sym.new_of_act[P];
+    lambda[2 * P] = mu[R].re * rs[R];
+    lambda[2 * P + 1] = mu[R].im * rs[R];
+  }
+  return st;
+}

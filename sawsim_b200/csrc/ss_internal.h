@@ -2,12 +2,19 @@
 // and the device code (*.cu).
 #pragma once
 #include <cstdint>
+#include <functional>
 #include <string>
 #include <vector>
 #include <cuda_runtime.h>
 #include "../../include/sawsim_b200.h"
 
 namespace ss {
+
+template <class T>
+struct cplx;   // dev_complex.cuh
+struct cplx_d {   // host view of a device cplx<double>
+  double re, im;
+};
 
 // ---------------------------------------------------------------- device buffer
 struct DBuf {
@@ -112,7 +119,8 @@ struct Handle {
       d_relpos, d_arrow_ptr, d_arrow_pos, d_arrow_slot, d_level_fronts, d_p0;
   // numeric work
   DBuf arena, piv, dperm_new, work;
-  DBuf wk[12];                           // sweep work buffers, kept across calls
+  DBuf wk[16];                           // sweep work buffers, kept across calls
+  DBuf dct_ptr, dct_idx, dct_src;        // transposed condensed pattern (new order) and value slots
   size_t arena_chunk = 0;
   void *plan[2] = {nullptr, nullptr};   // factorisation plans per precision
   DBuf dKs, dMs, dDs;                    // equilibrated condensed values
@@ -126,8 +134,14 @@ struct Handle {
 int launch_assemble(Handle &h, int which);  // which 0: K+M, 1: D
 // numeric.cu
 int launch_condense(Handle &h);
+// Optional work of a sweep beyond the charges: per_chunk(c0, nb, x, mu) is called
+// for every chunk of frequencies with the scaled primal solutions x' and adjoint
+// solutions mu' (A'^T mu' = cs * kq) of that chunk on the device (nb x n each).
+struct SweepExtra {
+  std::function<int(int, int, const cplx<double> *, const cplx<double> *)> per_chunk;
+};
 int run_sweep(Handle &h, int n_f, const double *omega, double V, int precision,
-              double *Q, int *status, int *iters, double *disp_out);
+              double *Q, int *status, int *iters, double *disp_out, const SweepExtra *ex = nullptr);
 // symbolic.cpp
 int build_global_pattern(Handle &h);
 int build_condensation(Handle &h);

@@ -1,0 +1,330 @@
+// Complex64 front updates C -= A B on the 5th-generation tensor cores (sm_100a):
+// tcgen05.mma kind::tf32 with FP32 accumulators in tensor memory, operands
+// staged in 128-byte-swizzled shared memory, one elected thread issuing the MMAs,
+// completion tracked by an mbarrier (tcgen05.commit).
+//
+// Complex product as one real GEMM.  A (rows x k complex, row-major, re/im
+// interleaved) is read as a real K-major matrix A_il (rows x 2k).  B (k x n
+// complex) is expanded in shared memory into the real K-major operand B'
+// (2n rows of 2k): row 2c holds (Br, -Bi) and row 2c+1 holds (Bi, Br) at real K
+// positions (2j, 2j+1).  Then C_il = A_il B'^T is C in interleaved form:
+// column 2c = Re(AB), 2c+1 = Im(AB).  The flops equal the complex count.
+//
+// FP32 accuracy from TF32 inputs (3xTF32): every operand value v is split as
+// v = hi + lo with hi = v rounded to TF32 and lo = v - hi (exact in FP32); the
+// accumulator receives hi*hi + hi*lo + lo*hi.  The dropped lo*lo term and the
+// truncation of lo to TF32 are at the 2^-22 relative level, the FP32 rounding
+// level of the SIMT kernel this replaces.
+//
+// Tile: 128 complex rows x 64 complex columns (M = 128, N = 128 real) per CTA,
+// K in chunks of 16 complex (one 128-byte swizzle row of fp32), 2 stages of
+// 64 KB (A hi/lo, B' hi/lo).  256 threads stage the operands; thread 0 issues 12
+// MMAs of 128x128x8 per chunk.  Every mbarrier wait is bounded: on time-out the
+// CTA records the error, drains its own MMAs (bounded), frees its tensor memory
+// and returns without touching C.
+#pragma once
+#include <cstdint>
+#include "dev_complex.cuh"
+
+namespace ss {
+
+// One output tile of C -= A B inside front f: rows [r0, rhi), cols [c0, chi),
+// contraction [kk0, kk1); A = F[:, kk], B = F[kk, :] (F = the front, row-major, ld).
+struct GemmTask {
+  int f, r0, c0, rhi, chi, kk0, kk1;
+};
+
+namespace tc {
+
+constexpr int BM = 128;              // complex rows per tile (MMA M)
+constexpr int BN = 64;               // complex columns per tile (MMA N = 128 real)
+constexpr int BKC = 16;              // complex K per chunk (32 fp32 = one 128-byte row)
+constexpr int STAGES = 2;
+constexpr int THREADS = 256;
+constexpr int OPER_BYTES = 128 * 128;                 // 128 rows x 128 bytes
+constexpr int STAGE_BYTES = 4 * OPER_BYTES;           // A hi, A lo, B hi, B lo
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;   // + alignment slack
+constexpr int TMEM_COLS = 128;
+constexpr uint64_t kWaitNs = 200000000ull;           // 0.2 s bound on any mbarrier wait
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// tf32 round-to-nearest (ties away) of an fp32 value, low 13 mantissa bits zero
+__device__ __forceinline__ float tf32_hi(float v) {
+  uint32_t u = __float_as_uint(v);
+  if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x1000u) & 0xffffe000u;
+  return __uint_as_float(u);
+}
+
+// shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups 1024 B apart
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3fff);          // start address
+  d |= (uint64_t)1 << 16;                          // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;                // stride byte offset
+  d |= (uint64_t)1 << 46;                          // descriptor version (sm_100)
+  d |= (uint64_t)2 << 61;                          // 128-byte swizzle
+  return d;
+}
+
+// instruction descriptor: kind::tf32, FP32 accumulate, K-major A and B, M=128, N=128
+constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(128 >> 3) << 17) |
+                            ((uint32_t)(128 >> 4) << 24);
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n"
+      :
+      : "r"(tmem_d), "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// bounded wait for the mbarrier phase with parity `parity` to complete (at most
+// kWaitNs of wall time); false on time-out
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  const uint64_t t0 = global_ns();
+  for (;;) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (global_ns() - t0 > kWaitNs) return false;
+  }
+}
+
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// 32 consecutive fp32 columns of this warp's 32 TMEM lanes
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// byte offset of 16-byte chunk q of row r in a 128-byte-swizzled K-major operand
+__device__ __forceinline__ uint32_t sw_off(int r, int q) { return (uint32_t)(r * 128 + ((q ^ (r & 7)) << 4)); }
+
+// Per thread per chunk: A 128 rows x 8 float4 -> 4 float4 each; B 16 k-rows x 64
+// complex columns -> 4 complex each.
+struct Frag {
+  float4 a[4];
+  float2 b[4];
+};
+
+__device__ __forceinline__ void load_chunk(const cf *F, int ld, const GemmTask &tk, int kb, Frag &fr) {
+  const int t = threadIdx.x;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int idx = t + THREADS * i;        // 0..1023
+    const int row = idx >> 3, q = idx & 7;  // q: pair of complex K columns
+    const int r = tk.r0 + row, c = kb + 2 * q;
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (r < tk.rhi) {
+      const cf *p = F + (int64_t)r * ld + c;
+      if (c + 1 < tk.kk1) {
+        v = make_float4(p[0].x, p[0].y, p[1].x, p[1].y);
+      } else if (c < tk.kk1) {
+        v = make_float4(p[0].x, p[0].y, 0.f, 0.f);
+      }
+    }
+    fr.a[i] = v;
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int idx = t + THREADS * i;        // 0..1023
+    const int j = idx >> 6, cc = idx & 63;  // complex k-row, complex column
+    const int r = kb + j, c = tk.c0 + cc;
+    float2 v = make_float2(0.f, 0.f);
+    if (r < tk.kk1 && c < tk.chi) {
+      const cf e = F[(int64_t)r * ld + c];
+      v = make_float2(e.x, e.y);
+    }
+    fr.b[i] = v;
+  }
+}
+
+__device__ __forceinline__ void store_chunk(unsigned char *stage, const Frag &fr) {
+  unsigned char *ahi = stage, *alo = stage + OPER_BYTES, *bhi = stage + 2 * OPER_BYTES, *blo = stage + 3 * OPER_BYTES;
+  const int t = threadIdx.x;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int idx = t + THREADS * i;
+    const int row = idx >> 3, q = idx & 7;
+    const float4 v = fr.a[i];
+    const float4 h = make_float4(tf32_hi(v.x), tf32_hi(v.y), tf32_hi(v.z), tf32_hi(v.w));
+    const float4 l = make_float4(v.x - h.x, v.y - h.y, v.z - h.z, v.w - h.w);
+    *reinterpret_cast<float4 *>(ahi + sw_off(row, q)) = h;
+    *reinterpret_cast<float4 *>(alo + sw_off(row, q)) = l;
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int idx = t + THREADS * i;
+    const int j = idx >> 6, cc = idx & 63;
+    const float2 v = fr.b[i];
+    const float hr = tf32_hi(v.x), hi = tf32_hi(v.y), nhi = tf32_hi(-v.y);
+    const float lr = v.x - hr, li = v.y - hi, nli = -v.y - nhi;
+    // real K positions (2j, 2j+1) = byte 8j of the row: chunk j/2, half j%2
+    const uint32_t o0 = sw_off(2 * cc, j >> 1) + ((j & 1) << 3);
+    const uint32_t o1 = sw_off(2 * cc + 1, j >> 1) + ((j & 1) << 3);
+    *reinterpret_cast<float2 *>(bhi + o0) = make_float2(hr, nhi);
+    *reinterpret_cast<float2 *>(bhi + o1) = make_float2(hi, hr);
+    *reinterpret_cast<float2 *>(blo + o0) = make_float2(lr, nli);
+    *reinterpret_cast<float2 *>(blo + o1) = make_float2(li, lr);
+  }
+}
+
+// grid (tasks, frequencies); C -= A B for every task tile of every frequency
+__global__ void __launch_bounds__(THREADS, 1)
+    front_tc_gemm_kernel(cf *__restrict__ arena, int64_t stride, const int64_t *__restrict__ off,
+                         const int *__restrict__ ldv, const GemmTask *__restrict__ tasks, int *__restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
+  __shared__ __align__(8) uint64_t bars[STAGES + 1];
+  __shared__ uint32_t tmem_base_s;
+  __shared__ int abort_s;
+  unsigned char *smem = reinterpret_cast<unsigned char *>(
+      (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  const GemmTask tk = tasks[blockIdx.x];
+  const int fq = blockIdx.y;
+  const int ld = ldv[tk.f];
+  cf *F = arena + (int64_t)fq * stride + off[tk.f];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nk = (tk.kk1 - tk.kk0 + BKC - 1) / BKC;
+  if (nk <= 0) return;
+  // an earlier tile timed out: the whole CTA does nothing (one read, shared)
+  if (threadIdx.x == 0) abort_s = *reinterpret_cast<volatile int *>(err);
+  __syncthreads();
+  if (abort_s) return;
+  __syncthreads();
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s <= STAGES; ++s) mbar_init(smem_u32(&bars[s]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (wid == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)),
+                 "r"(TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_s;
+
+  Frag fr;
+  load_chunk(F, ld, tk, tk.kk0, fr);
+  bool ok = true;
+  for (int kc = 0; kc < nk; ++kc) {
+    const int s = kc % STAGES;
+    unsigned char *stage = smem + s * STAGE_BYTES;
+    // the MMAs that read this stage two chunks ago must be complete
+    if (kc >= STAGES) {
+      if (!mbar_wait(smem_u32(&bars[s]), (uint32_t)((kc / STAGES - 1) & 1))) abort_s = 1;
+    }
+    __syncthreads();
+    if (abort_s) {
+      ok = false;
+      break;
+    }
+    store_chunk(stage, fr);
+    fence_async_smem();
+    __syncthreads();
+    if (kc + 1 < nk) load_chunk(F, ld, tk, tk.kk0 + (kc + 1) * BKC, fr);   // next chunk in flight
+    if (threadIdx.x == 0) {
+      tc_fence_after();
+      const uint32_t base = smem_u32(stage);
+      const uint32_t ahi = base, alo = base + OPER_BYTES, bhi = base + 2 * OPER_BYTES, blo = base + 3 * OPER_BYTES;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {   // K = 8 fp32 = 32 bytes per MMA
+        const uint32_t ko = 32u * k;
+        mma_tf32(tmem, sw128_desc(ahi + ko), sw128_desc(bhi + ko), (kc > 0 || k > 0) ? 1u : 0u);
+        mma_tf32(tmem, sw128_desc(ahi + ko), sw128_desc(blo + ko), 1u);
+        mma_tf32(tmem, sw128_desc(alo + ko), sw128_desc(bhi + ko), 1u);
+      }
+      mma_commit(smem_u32(&bars[s]));
+    }
+  }
+  // all MMAs of this CTA complete (the last commit tracks every earlier MMA)
+  if (threadIdx.x == 0) {
+    if (ok) {
+      mma_commit(smem_u32(&bars[STAGES]));
+      if (!mbar_wait(smem_u32(&bars[STAGES]), 0u)) abort_s = 1;
+    } else {
+      // drain: the stages' last commits, bounded
+      for (int kc = nk - 1; kc >= 0 && kc >= nk - STAGES; --kc)
+        mbar_wait(smem_u32(&bars[kc % STAGES]), (uint32_t)((kc / STAGES) & 1));
+    }
+    if (abort_s) atomicExch(err, 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (!abort_s) {
+    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +32 (tile rows), real
+    // columns 64 (w / 4) .. +64 (32 complex columns)
+    const int row = 32 * (wid & 3) + lane;
+    const int r = tk.r0 + row;
+    const int cb = 32 * (wid >> 2);
+    float v[32];
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+      const uint32_t taddr = tmem + ((uint32_t)(32 * (wid & 3)) << 16) + (uint32_t)(64 * (wid >> 2) + 32 * half);
+      tmem_ld32(taddr, v);
+      if (r < tk.rhi) {
+        cf *crow = F + (int64_t)r * ld;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int c = tk.c0 + cb + 16 * half + j;
+          if (c < tk.chi) {
+            cf d = crow[c];
+            d.x -= v[2 * j];
+            d.y -= v[2 * j + 1];
+            crow[c] = d;
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (wid == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+  }
+}
+
+}  // namespace tc
+}  // namespace ss

@@ -174,5 +174,13 @@ class FrequencySolver:
         Q, _, _ = self.charges([omega], V, 'fp64')
         return disp.view(np.complex128), Q[0], abs(1j * omega * Q[0] / V)
 
+    def solve_adjoint(self, omega: float, precision: str = 'fp64'):
+        """lambda (complex, n_active, active-DOF order) with A_aa^T lambda = kq, the
+        folded charge row: dQ = -lambda^T dA x for a perturbation dA of the system."""
+        n = self.n_active
+        lam = np.zeros(2 * n)
+        self._h('ss_solve_adjoint', float(omega), PRECISION[precision], L.ptr(lam, C.c_double))
+        return lam.view(np.complex128)
+
     def close(self):
         self._h.close()

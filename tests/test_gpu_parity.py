@@ -84,6 +84,21 @@ def test_fields_match_oracle(pair):
     assert abs(Y_g - Y_o) <= 1e-7 * abs(Y_o)
 
 
+@pytest.mark.parametrize('precision,tol', [('fp64', 1e-7), ('mixed', 1e-6)])
+def test_adjoint_solves_transposed_system(pair, precision, tol):
+    """A_aa^T lambda = kq (the folded charge row) on the oracle's own matrices, and
+    lambda agrees with a SuperLU solve of the transposed system."""
+    import scipy.sparse.linalg as spla
+    case, _, _, o, g = pair
+    w = 2 * np.pi * case.freqs[len(case.freqs) // 3]
+    A, _ = o.system(w)
+    kq = (o._T.T @ o.kts)[o.active]
+    lam = g.solve_adjoint(w, precision)
+    assert np.linalg.norm(A.T @ lam - kq) <= 1e-9 * np.linalg.norm(kq)
+    ref = spla.splu(A.T.tocsc()).solve(kq)
+    assert np.max(np.abs(lam - ref)) <= tol * np.max(np.abs(ref))
+
+
 def test_double_layer_published_curve(built_lib):
     """The rebuilt sp_double_layer template reproduces the reference's published
     curve at its 5 test frequencies on the GPU FP64 path."""
