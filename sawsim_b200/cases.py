@@ -53,6 +53,8 @@ class PML:
     xp: float = 0.0
     ya: float = 0.0
     yp: float = 0.0
+    za: float = 0.0
+    zp: float = 0.0
 
 
 def bc_periodic(mesh: Mesh, lines, ndisp: int = 3, tag_bottom=21, tag_left=19, tag_right=20,
@@ -143,3 +145,106 @@ def engine_for(case: Case, device: int = 0):
     from .engine import FrequencySolver
     return FrequencySolver.from_q9(case.mesh, case.materials, case.mat_idx, case.pml, case.omega_top, case.bc,
                                    mode_extension=case.mode_extension, device=device)
+
+
+# ---------------------------------------------------------------------------- Hex27 slabs
+def bc_periodic_3d(sets, pos_m, N: int):
+    """(fix, zheng, fu, groups, two_stage) for ss_set_bc from the slab's boundary node
+    sets, following boundary_idx_vect_3ds (src/sawsim/saw2d/saw3d/boundary.py:84-148)
+    and the two-stage fold of bc_solve.py:36-44: electrode nodes leave the
+    front/back sets (their u DOFs stay front/back periodic, their phi is
+    prescribed), bottom nodes leave front/back/L/R (their phi pairs are kept
+    separately), L/R lose the back edge; pairs are matched by coordinates rounded
+    to 0.1 nm (y then z for L/R, x then z for front/back).  Groups are
+    [master, slave]: the front/back pairs first (``two_stage`` of them), then
+    the left/right pairs.  DOFs: u interleaved 3n + c, phi at 3N + n."""
+    I, D = np.intersect1d, np.setdiff1d
+    g2, L, R, front, back, zheng, fu = (np.asarray(sets[k], dtype=np.int64) for k in
+                                        ('bottom', 'L', 'R', 'front', 'back', 'zheng', 'fu'))
+    cor = np.round(np.asarray(pos_m) * 1e9, 1)
+
+    def lr(a, b):
+        return a[np.lexsort((cor[a, 2], cor[a, 1]))], b[np.lexsort((cor[b, 2], cor[b, 1]))]
+
+    def fb(a, b):
+        return a[np.lexsort((cor[a, 2], cor[a, 0]))], b[np.lexsort((cor[b, 2], cor[b, 0]))]
+
+    def mach(n):
+        return np.concatenate([3 * n, 3 * n + 1, 3 * n + 2])
+
+    fz, bz, ff, bf = I(front, zheng), I(back, zheng), I(front, fu), I(back, fu)
+    front = D(front, np.concatenate([fz, ff]))
+    back = D(back, np.concatenate([bz, bf]))
+    g2F, g2b, g2L, g2R = I(g2, front), I(g2, back), I(g2, L), I(g2, R)
+    g2Le, g2Re = D(g2L, I(g2, I(L, back))), D(g2R, I(g2, I(R, back)))
+    front, back, L, R = D(front, g2F), D(back, g2b), D(L, g2L), D(R, g2R)
+    L, R = D(L, I(L, back)), D(R, I(R, back))
+    L, R = lr(L, R)
+    front, back = fb(front, back)
+    g2F, g2b = fb(g2F, g2b)
+    g2Le, g2Re = lr(g2Le, g2Re)
+    fz, bz = fb(fz, bz)
+    ff, bf = fb(ff, bf)
+    gu = 3 * N
+    F = np.concatenate([mach(front), mach(fz), mach(ff), front + gu, g2F + gu])
+    B = np.concatenate([mach(back), mach(bz), mach(bf), back + gu, g2b + gu])
+    Lm = np.concatenate([mach(L), L + gu, g2Le + gu])
+    Rs = np.concatenate([mach(R), R + gu, g2Re + gu])
+    if F.size != B.size or Lm.size != Rs.size:
+        raise ValueError('periodic node sets do not pair up')
+    groups = [np.array([a, b]) for a, b in zip(F, B)] + [np.array([a, b]) for a, b in zip(Lm, Rs)]
+    return mach(g2), zheng + gu, fu + gu, groups, int(F.size)
+
+
+@dataclass
+class HexCase:
+    name: str
+    cell: object
+    pos_m: np.ndarray
+    hexas: np.ndarray
+    materials: list
+    mat_idx: np.ndarray
+    pml: list
+    bc: tuple
+    freqs: np.ndarray
+    info: dict = field(default_factory=dict)
+
+    @property
+    def omega_top(self) -> float:
+        return 2 * np.pi * float(self.freqs[-1])
+
+    @property
+    def N(self) -> int:
+        return int(self.pos_m.shape[0])
+
+
+HEX_CASES = {
+    # name: (nx, ny, nz, f0, f1, npoints)
+    'hex_8x4x48': (8, 4, 48, 1.6e9, 2.0e9, 101),
+}
+
+
+def make_hex_case(name: str, seed: int = 0, nx=None, ny=None, nz=None, points=None) -> HexCase:
+    """Seeded synthetic double-layer Hex27 slab (see ``cells.hex_double_layer_slab``):
+    rotated 3m film, Al electrodes, SiO2 layer and SiO2 PML (z-stretch, frozen at
+    the top frequency, dmax 1e11, n 3, as src/sawsim/hex_models.py:75-77)."""
+    x0, y0, z0, fa, fb, npt = HEX_CASES[name]
+    cell = cells.hex_double_layer_slab(nx or x0, ny or y0, nz or z0)
+    piezo, euler = _crystal(seed)
+    mats = [piezo, mt.al(), mt.sio2()]
+    idx = np.array([cell.tag_map[int(t)] for t in cell.hex_tag], dtype=np.int64)
+    pos_m = cell.POS * 1e-6
+    bottom = float(pos_m[:, 2].min())
+    pml = [PML(tag=cell.pml_tag, kind='z', za=cell.pml_top_um * 1e-6, zp=bottom)]
+    bc = bc_periodic_3d(cell.sets, pos_m, pos_m.shape[0])
+    freqs = np.linspace(fa, fb, points or npt)
+    return HexCase(name, cell, pos_m, cell.HEXAS27, mats, idx, pml, bc, freqs,
+                   dict(seed=seed, euler_deg=list(map(float, euler)), nx=cell.info['nx'], ny=cell.info['ny'],
+                        nz=cell.info['nz']))
+
+
+def hex_engine_for(case: HexCase, device: int = 0):
+    """GPU engine for a Hex27 slab (assembly, two-stage fold and analysis on the device)."""
+    from .engine import FrequencySolver
+    return FrequencySolver.from_hex27(case.pos_m, case.hexas, case.cell.hex_tag, case.materials, case.mat_idx,
+                                      case.pml, case.omega_top, case.bc, device=device)

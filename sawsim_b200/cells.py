@@ -249,3 +249,154 @@ def me1_four_layer_cell(columns: int = 128, rows: int = 512, pitch_um: float = 1
                                 Band(23, 0.5 * p, r_poly), Band(24, 3 * p, r_si),
                                 Band(25, p, r_pml)],
                    Band(TAG_ELECTRODE, 0.08 * p, 1))
+
+
+# ---------------------------------------------------------------------------- Hex27 slab
+HEX_TAG_PIEZO, HEX_TAG_ELECTRODE, HEX_TAG_LAYER = 7, 8, 9   # volume tags of sp_hex_meshes/double.py:120-123
+
+
+def _h27_factor(code, t):
+    return t * (t - 1.0) if code == 0 else t * (t + 1.0) if code == 1 else (t + 1.0) * (t - 1.0)
+
+
+# raw H27 functions (factor codes per axis: 0 t(t-1), 1 t(t+1), 2 (t+1)(t-1)) and the
+# sortSF27 permutation (src/sawsim/saw2d/saw3d/elements.py:28-44)
+_H27_RAW = [(0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0), (0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1),
+            (2, 0, 0), (1, 2, 0), (2, 1, 0), (0, 2, 0), (0, 0, 2), (1, 0, 2), (1, 1, 2), (0, 1, 2),
+            (2, 0, 1), (1, 2, 1), (2, 1, 1), (0, 2, 1), (2, 2, 0), (2, 0, 2), (1, 2, 2), (2, 1, 2),
+            (0, 2, 2), (2, 2, 1), (2, 2, 2)]
+_H27_PERM = [6, 5, 4, 7, 2, 1, 0, 3, 17, 18, 14, 16, 13, 19, 12, 15, 9, 10, 8, 11, 25, 22, 23, 21, 24, 20, 26]
+
+
+def h27_local_nodes() -> np.ndarray:
+    """(27, 3) natural coordinates in {-1, 0, 1} of the node of each H27 function:
+    per axis, t(t-1) vanishes except at -1, t(t+1) except at +1, (t+1)(t-1) except at 0."""
+    return np.array([[-1.0 if c == 0 else 1.0 if c == 1 else 0.0 for c in _H27_RAW[r]] for r in _H27_PERM])
+
+
+@dataclass
+class HexCell:
+    """A structured Hex27 slab: nodes (um), 0-based connectivity, volume tags and the
+    boundary node sets of ``find_saw_boundary_3ds`` (src/sawsim/saw2d/saw3d/boundary.py:32-51)."""
+
+    POS: np.ndarray
+    HEXAS27: np.ndarray
+    hex_tag: np.ndarray
+    sets: dict
+    tag_map: dict
+    pml_tag: int
+    pml_top_um: float
+    pml_bottom_um: float
+    period_um: float
+    aperture_um: float
+    info: dict = field(default_factory=dict)
+
+
+def hex_slab_cell(pitch_um: float, nx: int, ny: int, bands, electrode: Band, aperture_um: float,
+                  metal_ratio: float = 0.5) -> HexCell:
+    """Two-pitch-wide periodic Hex27 slab (the layout of src/sawsim/sp_hex_meshes/double.py:21-135).
+
+    x in [0, 2p] (nx uniform cells, L/R periodic), y in [0, aperture] (ny cells,
+    front/back periodic), z downward from the surface through ``bands`` (last band
+    = PML, tagged by its own tag); the + and - electrode blocks of width
+    ``metal_ratio * p`` centred at p/2 and 3p/2 stand ``electrode.thickness_um``
+    above the surface with ``electrode.rows`` element layers.  Node sets: L (x=0),
+    R (x=2p), front (y=0), back (y=aperture), bottom (z=min), zheng / fu = the outer
+    surface nodes of the + / - electrode blocks, base included.
+    """
+    p = float(pitch_um)
+    w = 2 * p
+    xs = np.array([w * i / nx for i in range(nx + 1)])
+    edges = [p * (1 - metal_ratio) / 2, p * (1 + metal_ratio) / 2, p * (3 - metal_ratio) / 2,
+             p * (3 + metal_ratio) / 2]
+    cols = []
+    for a, b in ((edges[0], edges[1]), (edges[2], edges[3])):
+        ia, ib = int(np.argmin(np.abs(xs - a))), int(np.argmin(np.abs(xs - b)))
+        if abs(xs[ia] - a) > 1e-9 * w or abs(xs[ib] - b) > 1e-9 * w or ib <= ia:
+            raise ValueError('electrode edges must fall on cell edges')
+        cols.append((ia, ib))
+    levels, owner = _band_levels(0.0, bands)                  # bottom -> top, z
+    nz = len(owner)
+    tl = [electrode.thickness_um * r / electrode.rows for r in range(1, electrode.rows + 1)]
+    zlev = np.array(list(levels) + tl)
+    xn = np.empty(2 * nx + 1)
+    xn[0::2] = xs
+    xn[1::2] = 0.5 * (xs[:-1] + xs[1:])
+    ys = np.array([aperture_um * j / ny for j in range(ny + 1)])
+    yn = np.empty(2 * ny + 1)
+    yn[0::2] = ys
+    yn[1::2] = 0.5 * (ys[:-1] + ys[1:])
+    zn = np.empty(2 * len(zlev) - 1)
+    zn[0::2] = zlev
+    zn[1::2] = 0.5 * (zlev[:-1] + zlev[1:])
+
+    ids = {}
+    pos = []
+
+    def node(i, j, k):
+        key = (i, j, k)
+        if key not in ids:
+            ids[key] = len(pos)
+            pos.append((xn[i], yn[j], zn[k]))
+        return ids[key]
+
+    loc = h27_local_nodes().astype(int)
+    hexas, tags = [], []
+
+    def add(ex, ey, ez, tag):
+        hexas.append([node(2 * ex + 1 + lx, 2 * ey + 1 + ly, 2 * ez + 1 + lz) for lx, ly, lz in loc])
+        tags.append(tag)
+
+    for ez in range(nz):
+        for ey in range(ny):
+            for ex in range(nx):
+                add(ex, ey, ez, bands[owner[ez]].tag)
+    elec = []
+    for ia, ib in cols:
+        members = set()
+        for ez in range(nz, nz + electrode.rows):
+            for ey in range(ny):
+                for ex in range(ia, ib):
+                    add(ex, ey, ez, electrode.tag)
+        # outer surface of the block (lattice box [2ia, 2ib] x [0, 2ny] x [2nz, 2nz + 2 rows])
+        k0, k1 = 2 * nz, 2 * (nz + electrode.rows)
+        for (i, j, k), n in ids.items():
+            if 2 * ia <= i <= 2 * ib and k0 <= k <= k1 and (i in (2 * ia, 2 * ib) or j in (0, 2 * ny) or
+                                                           k in (k0, k1)):
+                members.add(n)
+        elec.append(np.array(sorted(members), dtype=np.int64))
+    P = _clean13(np.array(pos))
+    H = np.array(hexas, dtype=np.int64)
+    T = np.array(tags, dtype=np.int64)
+    lat = np.array(list(ids.keys()))
+    nid = np.array(list(ids.values()))
+    order = np.argsort(nid)
+    lat = lat[order]
+
+    def where(mask):
+        return np.sort(nid[order][mask]).astype(np.int64)
+
+    kmin = 0
+    sets = dict(L=where(lat[:, 0] == 0), R=where(lat[:, 0] == 2 * nx), front=where(lat[:, 1] == 0),
+                back=where(lat[:, 1] == 2 * ny), bottom=where(lat[:, 2] == kmin), zheng=elec[0], fu=elec[1])
+    pml = bands[-1]
+    layer_tags = [b.tag for b in bands[1:-1]]
+    tag_map = {HEX_TAG_PIEZO: 0, HEX_TAG_ELECTRODE: 1}
+    tag_map.update({t: i + 2 for i, t in enumerate(layer_tags)})
+    tag_map[pml.tag] = len(layer_tags) + 1 if layer_tags else 0
+    bottom = float(P[:, 2].min())
+    return HexCell(POS=P, HEXAS27=H, hex_tag=T, sets=sets, tag_map=tag_map, pml_tag=pml.tag,
+                   pml_top_um=bottom + pml.thickness_um, pml_bottom_um=bottom, period_um=w,
+                   aperture_um=float(aperture_um), info=dict(nx=nx, ny=ny, nz=nz, electrode_cols=cols))
+
+
+def hex_double_layer_slab(nx: int = 8, ny: int = 4, nz: int = 48, pitch_um: float = 1.085) -> HexCell:
+    """Double-layer Hex27 slab: 3m film 0.6p / SiO2 1.4p / SiO2 PML 2p (z), aperture
+    0.5p, Al electrodes 0.08p (one layer) on top.  ``nz`` element layers split
+    1/6 film, 1/3 SiO2, 1/2 PML (8/16/24 at 48).  Material order: 0 piezo, 1 Al, 2 SiO2."""
+    p = pitch_um
+    r_film = nz // 6
+    r_ox = nz // 3
+    r_pml = nz - r_film - r_ox
+    return hex_slab_cell(p, nx, ny, [Band(HEX_TAG_PIEZO, 0.6 * p, r_film), Band(HEX_TAG_LAYER, 1.4 * p, r_ox),
+                                     Band(10, 2 * p, r_pml)], Band(HEX_TAG_ELECTRODE, 0.08 * p, 1), 0.5 * p)

@@ -51,18 +51,20 @@ class Handle:
 
 
 def _pml_arrays(elem_tag, pml_regions, ne):
-    """Region arrays for ss_set_pml from reference-style PMLRegion objects (piezo_fem.py:192-242)."""
+    """Region arrays for ss_set_pml from reference-style PML regions: Q9
+    ``PMLRegion`` (piezo_fem.py:192-242, axes x/y) or the Hex27 bottom region
+    (saw3d/assembly.py:127-143, axis z with za the interface, zp the outer face)."""
     regions = list(pml_regions or [])
     region = np.full(ne, -1, dtype=np.int32)
     axis, dmax, npow, inner, outer = [], [], [], [], []
     for r, reg in enumerate(regions):
         region[np.asarray(elem_tag) == reg.tag] = r
-        mask = (1 if 'x' in reg.kind else 0) | (2 if 'y' in reg.kind else 0)
+        mask = (1 if 'x' in reg.kind else 0) | (2 if 'y' in reg.kind else 0) | (4 if 'z' in reg.kind else 0)
         axis.append(mask)
         dmax.append(reg.dmax)
         npow.append(reg.n)
-        inner.append([reg.xa, reg.ya, 0.0])
-        outer.append([reg.xp, reg.yp, 0.0])
+        inner.append([reg.xa, reg.ya, getattr(reg, 'za', 0.0)])
+        outer.append([reg.xp, reg.yp, getattr(reg, 'zp', 0.0)])
     return (len(regions), L.i32(axis), L.f64(dmax), L.i32(npow), L.f64(np.reshape(inner, (-1, 3))),
             L.f64(np.reshape(outer, (-1, 3))), region)
 
@@ -116,6 +118,32 @@ class FrequencySolver:
         eng._set_bc(bc, two_stage=0)
         if damping_materials is not None and beta:
             h('ss_set_damping', float(beta))
+        return eng
+
+    @classmethod
+    def from_hex27(cls, pos_m, hexas, elem_tag, materials, mat_idx, pml_regions, omega_top, bc, device=0):
+        """Assemble a Hex27 slab on the GPU from the inputs of
+        ``form_stiffness_mass_3d`` (saw3d/assembly.py:230: 0-based H27 connectivity,
+        coordinates in metres, full 3D tensors; the PML elements carry the PML
+        material; PML regions select elements by ``elem_tag``, no clamp) and
+        ``bc = (fix, zheng, fu, groups, two_stage)`` from ``cases.bc_periodic_3d``
+        (the two-stage fold of saw3d/bc_solve.py:36-44)."""
+        h = Handle(device)
+        pos = L.f64(pos_m)
+        conn = L.i64(hexas)
+        emat = L.i32(mat_idx)
+        h('ss_set_mesh', L.SS_HEX27, pos.shape[0], L.ptr(pos, C.c_double), conn.shape[0], L.ptr(conn, C.c_int64),
+          L.ptr(emat, C.c_int32))
+        rho, Cm, em, epsm = pack(materials, 3)
+        h('ss_set_materials', L.SS_MAT_K, len(rho), L.ptr(rho, C.c_double), L.ptr(Cm, C.c_double),
+          L.ptr(em, C.c_double), L.ptr(epsm, C.c_double))
+        nreg, axis, dmax, npow, inner, outer, region = _pml_arrays(elem_tag, pml_regions, conn.shape[0])
+        h('ss_set_pml', nreg, L.ptr(axis, C.c_int32), L.ptr(dmax, C.c_double), L.ptr(npow, C.c_int32),
+          L.ptr(inner, C.c_double), L.ptr(outer, C.c_double), 0, L.ptr(region, C.c_int32), float(omega_top))
+        h('ss_assemble')
+        fix, zheng, fu, groups, two_stage = bc
+        eng = cls(h, 4 * pos.shape[0], 3, L.SS_HEX27, zheng, fu)
+        eng._set_bc((fix, zheng, fu, groups), two_stage=two_stage)
         return eng
 
     def _set_bc(self, bc, two_stage=0):

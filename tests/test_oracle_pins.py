@@ -3,7 +3,7 @@
 * against the reference's published sp_double_layer curve (tests/data of the
   reference, copied into tests/golden/sp_double_layer.npz with its materials);
 * against the reference's own matrices and charges on small seeded cells
-  (tests/golden/ref_*.npz, produced by tests/golden/make_golden.py).
+  (tests/golden/ref_me*.npz, produced by tests/golden/make_golden.py).
 """
 import hashlib
 
@@ -59,7 +59,7 @@ def test_double_layer_realblock_route():
     assert np.max(np.abs(Qc - Qr) / np.abs(Qr)) < 5e-8
 
 
-@pytest.mark.parametrize('path', sorted(p.name for p in GOLDEN.glob('ref_*.npz')))
+@pytest.mark.parametrize('path', sorted(p.name for p in GOLDEN.glob('ref_me*.npz')))
 def test_oracle_matches_reference_run(path):
     g = np.load(GOLDEN / path)
     name = path[4:].rsplit('_', 1)[0]
