@@ -30,7 +30,13 @@ REPO = Path(__file__).resolve().parent
 sys.path.insert(0, str(REPO))
 
 PEAKS = REPO / 'MEASURED_PEAKS.json'
-CPU_SAMPLE = (32, 128)   # bounded CPU sample: the same cell family at half resolution per axis
+# bounded CPU samples: the same cell family at two reduced sizes (one full-size point
+# takes minutes to hours of SuperLU on one core); the full-size points/s is
+# extrapolated with the DOF exponent fitted between the two
+CPU_SAMPLE = {'me0_16x64': [dict(cols=8, rows=32), dict(cols=16, rows=64)],
+              'me1_64x256': [dict(cols=16, rows=64), dict(cols=32, rows=128)],
+              'me1_128x512': [dict(cols=16, rows=64), dict(cols=32, rows=128)],
+              'hex_8x4x48': [dict(nx=8, ny=1, nz=12), dict(nx=8, ny=2, nz=24)]}
 METRIC = 'Y11 points/s, 1 B200: batched FP32-TC+refine vs FP64 sweep, fr/fa within 1 kHz'
 
 
@@ -40,7 +46,7 @@ def parse():
     p.add_argument('--steps', type=int, default=3)
     p.add_argument('--warmup', type=int, default=3)
     p.add_argument('--impl', default='b200', choices=['b200', 'reference'])
-    p.add_argument('--precision', default='mixed', choices=['mixed', 'fp64'])
+    p.add_argument('--precision', default='auto', choices=['auto', 'mixed', 'fp64'])
     p.add_argument('--case', default='me1_64x256')
     p.add_argument('--points', type=int, default=None)
     p.add_argument('--no-cpu-baseline', action='store_true')
@@ -102,29 +108,50 @@ def peaks():
 # ----------------------------------------------------------------------------- CPU side
 def _cpu_point(args):
     """One frequency point of the reference algorithm (oracle port), in a worker process."""
-    case_name, cols, rows, f = args
+    case_name, size, f = args
     os.environ.setdefault('OMP_NUM_THREADS', '1')
     from helpers_cpu import oracle_solver_for
-    eng = oracle_solver_for(case_name, cols, rows)
+    eng = oracle_solver_for(case_name, **size)
     t = time.perf_counter()
-    eng.solve(2 * np.pi * f, 1.0, route='realblock')
+    if case_name.startswith('hex'):
+        eng.solve(2 * np.pi * f, 1.0)
+    else:
+        eng.solve(2 * np.pi * f, 1.0, route='realblock')
     return time.perf_counter() - t
 
 
-def cpu_sweep_sample(case_name, cols, rows, npoints, workers):
-    """Points/s of the reference route on a bounded sample, `workers` spawn processes."""
+def _dofs(c):
+    return 4 * c.N if c.name.startswith('hex') else c.mesh.N * (4 if c.mode_extension else 3)
+
+
+def cpu_sweep_sample(case_name, npoints, workers):
+    """Full-size points/s of the reference route, extrapolated from two bounded samples.
+
+    At each of two reduced sizes of the same cell family, ``npoints`` points run on
+    ``workers`` spawn processes (one BLAS thread each); the per-point cost is fitted
+    as a power of the DOF count and evaluated at the full size."""
     import multiprocessing as mp
-    from sawsim_b200 import cases
-    c = cases.make_case(case_name, cols=cols, rows=rows)
-    fs = np.linspace(c.freqs[0], c.freqs[-1], npoints)
+    full = make(case_name)
+    meas = []
     ctx = mp.get_context('spawn')
     with ctx.Pool(workers, initializer=_cpu_init) as pool:
-        pool.map(_cpu_point, [(case_name, cols, rows, fs[0])] * workers)      # build per-worker engines
-        t = time.perf_counter()
-        pool.map(_cpu_point, [(case_name, cols, rows, f) for f in fs], chunksize=1)
-        dt = time.perf_counter() - t
-    ndof = c.mesh.N * (4 if c.mode_extension else 3)
-    return npoints / dt, ndof
+        for size in CPU_SAMPLE[case_name]:
+            c = make(case_name, **size)
+            fs = np.linspace(c.freqs[0], c.freqs[-1], npoints)
+            pool.map(_cpu_point, [(case_name, size, fs[0])] * workers)      # build per-worker engines
+            t = time.perf_counter()
+            pool.map(_cpu_point, [(case_name, size, f) for f in fs], chunksize=1)
+            meas.append((_dofs(c), npoints / (time.perf_counter() - t)))
+    (n0, v0), (n1, v1) = meas
+    alpha = float(np.log(v0 / v1) / np.log(n1 / n0))
+    nf = _dofs(full)
+    value = v1 * (n1 / nf) ** alpha
+    route = ('complex SciPy SuperLU per point (the Hex27 fallback of saw3d/bc_solve.py:166-167)'
+             if case_name.startswith('hex') else 'real-block SciPy SuperLU per point as the reference without PARDISO')
+    sample = (f'{npoints} points each at {n0} and {n1} DOF of the {case_name} family ({v0:.4g} and {v1:.4g} points/s), '
+              f'{route}, {workers} spawn workers x 1 BLAS thread; per-point cost ~ DOF^{alpha:.2f} extrapolated '
+              f'to the full {nf} DOF')
+    return value, sample
 
 
 def _cpu_init():
@@ -137,37 +164,58 @@ def reference_arm(a, rank, world):
     if rank != 0:
         return
     workers = min(8, os.cpu_count() or 1)
-    cols, rows = CPU_SAMPLE
     res = []
     for i in range(a.warmup + a.steps):
-        v, ndof = cpu_sweep_sample(a.case, cols, rows, 2 * workers, workers)
+        v, sample = cpu_sweep_sample(a.case, 2 * workers, workers)
         if i >= a.warmup:
             res.append(v)
     value = float(np.mean(res))
-    sample = (f'{2 * workers} frequency points per step of the {a.case} cell family at reduced resolution '
-              f'{cols}x{rows} ({ndof} DOF; one full-size point takes minutes on one core), real-block SciPy '
-              f'SuperLU per point as the reference without PARDISO, {workers} spawn workers x 1 BLAS thread')
     print(json.dumps(dict(impl='reference', metric=METRIC, value=value, unit='points/s', n_gpus=a.gpus,
                           steps=a.steps, warmup=a.warmup, higher_is_better=True, scaling='weak', vs_baseline=None,
                           dtype='f64', data='synthetic',
-                          config=dict(workload=f'{a.case} (reference CPU route, bounded sample)', points_per_step=2 * workers),
+                          config=dict(workload=workload_name(make(a.case, a.points)),
+                                      route='oracle port of the reference route, bounded sample, extrapolated'),
                           cpu_baseline=dict(value=value, unit='points/s', cores=workers, kind='port', sample=sample),
                           e2e=dict(value=value, unit='points/s', h2d_bytes_per_step=0, d2h_bytes_per_step=0))),
           flush=True)
 
 
 # ----------------------------------------------------------------------------- GPU side
+def make(case_name, points=None, **size):
+    from sawsim_b200 import cases
+    if case_name.startswith('hex'):
+        return cases.make_hex_case(case_name, points=points, **size)
+    return cases.make_case(case_name, points=points, **size)
+
+
+def workload_name(c):
+    if c.name.startswith('hex'):
+        i = c.info
+        return (f'{c.name}: double-layer Hex27 slab {i["nx"]}x{i["ny"]}x{i["nz"]} ({4 * c.N} DOF), '
+                f'{c.freqs.size} points {c.freqs[0] / 1e9:.1f}-{c.freqs[-1] / 1e9:.1f} GHz, seed {i["seed"]}')
+    i = c.info
+    kind = 'ME1 two-layer' if c.name == 'me1_64x256' else ('ME0' if c.name.startswith('me0') else 'ME1 four-layer')
+    return (f'{c.name}: {kind} Q9 cell {i["cols"]}x{i["rows"]}, {c.freqs.size} points '
+            f'{c.freqs[0] / 1e9:.1f}-{c.freqs[-1] / 1e9:.1f} GHz, seed {i["seed"]}')
+
+
 def b200_arm(a, rank, world, local):
     import torch
     import torch.distributed as dist
     from sawsim_b200 import cases
     torch.cuda.set_device(local)
-    c = cases.make_case(a.case, points=a.points)
+    c = make(a.case, a.points)
     t0 = time.perf_counter()
-    eng = cases.engine_for(c, device=local)
+    eng = cases.hex_engine_for(c, device=local) if a.case.startswith('hex') else cases.engine_for(c, device=local)
     setup_s = time.perf_counter() - t0
     st0 = eng.stats()
-    w = 2 * np.pi * c.freqs
+    from sawsim_b200.shard import gather_charges, shard
+    # N GPUs sweep an N-times denser grid of the same band, interleaved shards of
+    # c.freqs.size points per rank (weak scaling); the charges are gathered once per sweep
+    n_total = world * c.freqs.size
+    f_all = np.linspace(c.freqs[0], c.freqs[-1], n_total)
+    mine = shard(n_total, rank, world)
+    w = 2 * np.pi * f_all[mine]
     nf = w.size
     for _ in range(a.warmup):
         Q, status, iters = eng.charges(w, 1.0, a.precision)
@@ -183,6 +231,8 @@ def b200_arm(a, rank, world, local):
         for _ in range(a.steps):
             t = time.perf_counter()
             Q, status, iters = eng.charges(w, 1.0, a.precision)      # host buffers in, host Q out
+            if world > 1:
+                Q_all = gather_charges(Q, n_total, rank, world)
             wall_s.append(time.perf_counter() - t)
             s = eng.stats()
             dev_ms.append(s['sweep_device_ms'])
@@ -191,6 +241,31 @@ def b200_arm(a, rank, world, local):
         barrier()
     dev = float(np.sum(dev_ms)) / 1e3
     wall = float(np.sum(wall_s))
+    used = 'mixed' if int(eng.stats()['precision_used']) == 1 else 'fp64'
+    # accuracy of the timed sweep: fr/fa of Y11 = -i w Q / V (solver.py:128), and for a
+    # mixed sweep its Y11 error against an FP64 sweep of the same points (untimed)
+    from sawsim_b200.metrics import compare, resonances
+    if world > 1:
+        Q_all = gather_charges(Q, n_total, rank, world)
+    else:
+        Q_all = Q
+    w_all = 2 * np.pi * f_all
+    Y = -1j * w_all * Q_all
+    res = resonances(f_all, Y)
+    acc = dict(fr_ghz=res['fr_ghz'], fa_ghz=res['fa_ghz'], k2eff=res['k2eff'])
+    any_mixed = used == 'mixed'
+    if world > 1:      # every rank takes the same collective steps
+        t = torch.tensor([1.0 if any_mixed else 0.0], device='cuda')
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        any_mixed = bool(t.item() > 0)
+    if any_mixed:
+        Q64, _, _ = eng.charges(w, 1.0, 'fp64')
+        Q64 = gather_charges(Q64, n_total, rank, world) if world > 1 else Q64
+        Y64 = -1j * w_all * Q64
+        d = compare(resonances(f_all, Y64), res)
+        acc.update(y11_max_rel_err_vs_fp64=float(np.max(np.abs(Y - Y64) / np.abs(Y64))),
+                   fr_diff_khz_vs_fp64=None if d['fr_diff_mhz'] is None else d['fr_diff_mhz'] * 1e3,
+                   fa_diff_khz_vs_fp64=None if d['fa_diff_mhz'] is None else d['fa_diff_mhz'] * 1e3)
     if world > 1:
         t = torch.tensor([dev, wall], device='cuda', dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -199,40 +274,41 @@ def b200_arm(a, rank, world, local):
     pk, pk_kind = peaks()
     schur_flops_launch = s['schur_gemm_flops'] / max(1.0, s['schur_launches'])
     schur_ms_launch = float(np.mean(schur_ms)) / max(1.0, s['schur_launches'])
-    if a.precision == 'mixed':
+    if used == 'mixed':
         peak = pk.get('bf16_tflops', 1590.0) / 2
-        peak_note = f'TF32 dense = half the {pk_kind} cuBLAS bf16 burst'
+        peak_note = (f'TF32 dense = half the {pk_kind} cuBLAS bf16 burst; achieved counts the algorithmic '
+                     f'complex flops, the 3xTF32 split issues three times as many MMA flops')
     else:
         peak = 37.0
-        peak_note = 'FP64 nominal 37 TFLOP/s (no FP64 figure in MEASURED_PEAKS.json)'
+        peak_note = 'FP64 nominal 37 TFLOP/s (fallback: MEASURED_PEAKS.json has no FP64 figure)'
     achieved = schur_flops_launch / (schur_ms_launch * 1e-3) / 1e12 if schur_ms_launch > 0 else None
     line = None
     if rank == 0:
         cpu = None
         if not a.no_cpu_baseline:
             workers = min(8, os.cpu_count() or 1)
-            v, ndof = cpu_sweep_sample(a.case, *CPU_SAMPLE, 2 * workers, workers)
-            cpu = dict(value=v, unit='points/s', cores=workers, kind='port',
-                       sample=f'{2 * workers} points of the {a.case} family at {CPU_SAMPLE[0]}x{CPU_SAMPLE[1]} '
-                              f'({ndof} DOF, a quarter of the cell), real-block SciPy SuperLU as the reference '
-                              f'without PARDISO, {workers} spawn workers x 1 BLAS thread')
+            v, sample = cpu_sweep_sample(a.case, 2 * workers, workers)
+            cpu = dict(value=v, unit='points/s', cores=workers, kind='port', sample=sample)
         bad = int(np.sum(status != 0))
         line = dict(metric=METRIC, value=world * nf * a.steps / dev, unit='points/s', n_gpus=world,
                     steps=a.steps, warmup=a.warmup, ms_per_step=dev * 1e3 / a.steps, higher_is_better=True,
-                    scaling='weak', vs_baseline=None, dtype='c64+f64' if a.precision == 'mixed' else 'c128',
+                    scaling='weak', vs_baseline=None, dtype='c64+f64' if used == 'mixed' else 'c128',
                     data='synthetic',
-                    config=dict(workload=f'{a.case}: ME1 two-layer Q9 cell {c.info["cols"]}x{c.info["rows"]}, '
-                                         f'{nf} points 1.6-2.0 GHz, seed {c.info["seed"]}',
-                                precision=a.precision, n_active=int(st0['n_active']), fronts=int(st0['n_fronts']),
+                    config=dict(workload=workload_name(c),
+                                precision=a.precision, precision_used=used, accuracy=acc,
+                                n_active=int(st0['n_active']), fronts=int(st0['n_fronts']),
                                 factor_gflop_per_point=st0['factor_flops_per_point'] / 1e9,
                                 setup_s=setup_s, analyze_s=st0['analyze_s'], assemble_ms=st0['assemble_ms'],
                                 l2='inputs larger than L2 (front arena of GBs per chunk)',
                                 chunk=int(s['chunk']), points_not_converged=bad,
-                                mean_refinement_steps=float(np.mean(iters)), parallelism=f'replicas x{world}'),
+                                mean_refinement_steps=float(np.mean(iters)), parallelism=f'interleaved frequency shards x{world}' if world > 1 else 'one GPU'),
                     e2e=dict(value=world * nf * a.steps / wall, unit='points/s', h2d_bytes_per_step=8 * nf,
                              d2h_bytes_per_step=16 * nf + 8 * nf),
                     gpu_launches=launches,
-                    roofline=dict(kernel='front_gemm_kernel (Schur update F22 -= F21 F12)', bound='tensor',
+                    roofline=dict(kernel=('front_tc_gemm_kernel (tcgen05 3xTF32 Schur update F22 -= F21 F12)'
+                                          if used == 'mixed' else
+                                          'front_gemm_kernel<double> (Schur update F22 -= F21 F12)'),
+                                  bound='tensor',
                                   achieved=achieved, peak=peak, unit='TFLOP/s',
                                   frac=(achieved / peak) if achieved else None, traffic=None, peak_note=peak_note,
                                   flops_per_launch=schur_flops_launch),

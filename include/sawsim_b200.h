@@ -43,7 +43,10 @@ typedef struct ss_handle ss_handle;
 /* precision modes for ss_sweep */
 #define SS_PREC_FP64   0   /* complex128 fronts, FP64 throughout (the drop-in)   */
 #define SS_PREC_MIXED  1   /* complex64 fronts, 3xTF32 tensor-core Schur updates,
-                              FP64 residual and refinement                       */
+                              FP64 residual, FP64 flexible GMRES on the primal and
+                              the adjoint, dual-weighted charge correction       */
+#define SS_PREC_AUTO   2   /* probe MIXED on the two band ends with 12 Krylov
+                              steps; MIXED if both converge, else FP64           */
 
 /* matrix selectors for ss_set_csr / ss_export_csr */
 #define SS_MAT_K    0      /* global stiffness                                   */
@@ -151,13 +154,37 @@ int ss_solve_fields(ss_handle *h, double omega, double V, double *disp);
 int ss_solve_adjoint(ss_handle *h, double omega, int precision, double *lambda);
 
 /*
+ * Charges and their derivatives with respect to n_params parameters, by the
+ * adjoint: dQ/dp = sum_e (s - mu)_e^T dK_e/dp d_e + w^2 mu_e^T dM_e/dp d_e with d
+ * the full DOF vector, mu the folded adjoint (ss_solve_adjoint) and s the +
+ * electrode indicator; dK_e/dp, dM_e/dp are recomputed per element by
+ * forward-mode differentiation of the element routine.  The reference has no
+ * derivative; its charge is Q = kts . disp (sweep.py:303-305, :356-363) and the
+ * element routine is piezo_fem.py:248-367.  A parameter is described by its
+ * seeds (parameter-major, any pointer may be NULL = zero):
+ *   dpos   n_params x n_nodes x 2       node velocities dX/dp (metres per unit p)
+ *   dC     n_params x n_mat x 6 x 6 x 2 d(material C)/dp, complex interleaved
+ *   de     n_params x n_mat x 3 x 6 x 2
+ *   deps   n_params x n_mat x 3 x 3 x 2
+ *   drho   n_params x n_mat
+ *   dinner, douter  n_params x n_regions x 3   d(PML bounds)/dp
+ * Outputs: Q (n_f x 2) and dQ (n_f x n_params x 2).  Q9 meshes only; no
+ * Rayleigh damping.  status: n_f per-point status as ss_sweep (may be NULL).
+ */
+int ss_adjoint_gradient(ss_handle *h, int n_f, const double *omega, double V, int precision, int n_params,
+                        const double *dpos, const double *dC, const double *de, const double *deps,
+                        const double *drho, const double *dinner, const double *douter, double *Q, double *dQ,
+                        int *status);
+
+/*
  * Counters of the last calls: out[0..n) filled with
  *  0 n_active, 1 n_fronts, 2 max_front, 3 factor_flops_per_point (complex fronts,
  *  8 real flops per complex multiply-add), 4 nnz(L+U), 5 analyze_s, 6 assemble_ms,
  *  7 sweep_ms, 8 factor_ms, 9 solve_ms, 10 chunk, 11 schur_gemm_ms,
  *  12 schur_gemm_flops, 13 levels, 14 perturbed pivots, 15 kernel launches,
  *  16 Schur GEMM launches, 17 device time of the last ss_sweep (ms, CUDA events),
- *  18 refinement solves of the last ss_sweep.
+ *  18 refinement / Krylov steps of the last ss_sweep (sum over points),
+ *  19 precision the last ss_sweep ran in (SS_PREC_FP64 or SS_PREC_MIXED).
  */
 int ss_stats(const ss_handle *h, double *out, int n);
 

@@ -15,7 +15,7 @@ LIB_PATH = Path(__file__).resolve().parent / 'libsawsim_b200.so'
 
 SS_OK, SS_EINVAL, SS_ECUDA, SS_ESINGULAR, SS_ENOCONV, SS_ETIMEOUT, SS_ENOMEM, SS_ESTATE = 0, -1, -2, -3, -4, -5, -6, -7
 SS_Q9_ME0, SS_Q9_ME1, SS_HEX27 = 0, 1, 2
-SS_PREC_FP64, SS_PREC_MIXED = 0, 1
+SS_PREC_FP64, SS_PREC_MIXED, SS_PREC_AUTO = 0, 1, 2
 SS_MAT_K, SS_MAT_M, SS_MAT_D, SS_MAT_KC, SS_MAT_MC = 0, 1, 2, 3, 4
 
 STATUS_NAMES = {0: 'ok', -1: 'invalid argument', -2: 'CUDA error', -3: 'singular', -4: 'no convergence',
@@ -45,6 +45,8 @@ SIGNATURES = [
     ('ss_sweep', C.c_int, [_P, C.c_int, _DP, C.c_double, C.c_int, _DP, _IP, _IP]),
     ('ss_solve_fields', C.c_int, [_P, C.c_double, C.c_double, _DP]),
     ('ss_solve_adjoint', C.c_int, [_P, C.c_double, C.c_int, _DP]),
+    ('ss_adjoint_gradient', C.c_int, [_P, C.c_int, _DP, C.c_double, C.c_int, C.c_int, _DP, _DP, _DP, _DP, _DP, _DP,
+                                      _DP, _DP, _DP, _IP]),
     ('ss_stats', C.c_int, [_P, _DP, C.c_int]),
     ('ss_assemble_q9_noalloc', C.c_int, [C.c_int, C.c_int64, _P, C.c_int64, _P, _P, _P, _P, _P, _P, C.c_int, _P, _P,
                                          _P, _P, _P, _P, C.c_double, _P, _P, _P, C.c_int64, _P, _P, _P]),

@@ -447,13 +447,16 @@ __global__ void __launch_bounds__(256) front_swap_trsm_kernel(FrontArgs<T> a, in
 
 constexpr int kGemmBK = 8;
 // tile shapes: square (Schur update), skinny (panel column update), short (U row update)
-enum GemmShape { kSquare = 0, kSkinny = 1, kShort = 2 };
+// tile shapes: square (Schur update; two candidates the autotuner picks from per
+// level), skinny (panel column update), short (U row update)
+enum GemmShape { kSquare = 0, kSkinny = 1, kShort = 2, kSquare64 = 3 };
 template <int S> struct Tile;
 template <> struct Tile<kSquare> { static constexpr int BM = 128, BN = 64, TM = 8, TN = 4; };
 template <> struct Tile<kSkinny> { static constexpr int BM = 256, BN = 32, TM = 8, TN = 4; };
 template <> struct Tile<kShort> { static constexpr int BM = 32, BN = 256, TM = 4, TN = 8; };
-static inline int tile_bm(int s) { return s == kSquare ? 128 : s == kSkinny ? 256 : 32; }
-static inline int tile_bn(int s) { return s == kSquare ? 64 : s == kSkinny ? 32 : 256; }
+template <> struct Tile<kSquare64> { static constexpr int BM = 64, BN = 64, TM = 4, TN = 4; };
+static inline int tile_bm(int s) { return s == kSquare ? 128 : s == kSkinny ? 256 : s == kShort ? 32 : 64; }
+static inline int tile_bn(int s) { return s == kSquare ? 64 : s == kSkinny ? 32 : s == kShort ? 256 : 64; }
 
 // One BMxBN complex tile of C -= A B per CTA, TMxTN outputs per thread; K in
 // chunks of 8 with the next chunk prefetched into registers.
@@ -952,6 +955,31 @@ struct Plan {
   int small_m = 0;                         // threshold used
   double schur_flops = 0;
   std::vector<int> lvl_maxk, lvl_maxu;     // per level max k and max m-k (solve grids)
+  // CUDA graphs of the per-chunk launch sequences, replayed for every chunk with
+  // the same batch size and buffers (key: nb and the device pointers they bake in)
+  struct Graph {
+    int kind;                              // 0 factorisation, 1 solve, 2 transposed solve
+    int nb;
+    const void *key[8];
+    cudaGraphExec_t exec = nullptr;
+    int launches = 0, schur_launches = 0, nev = 0;
+  };
+  std::vector<Graph> graphs;
+  std::vector<cudaEvent_t> ev;             // Schur GEMM timing, one pair per level (owned here so
+                                           // that captured event-record nodes stay valid)
+  // Schur-tile autotuner (FP64): the second candidate's tasks, per-level pick,
+  // and the measured per-level times of the two candidates on full chunks
+  std::vector<int64_t> schur_ptr_b;
+  std::vector<char> pick;                  // per level: 0 kSquare, 1 kSquare64
+  std::vector<int> schur_level;            // level of each Schur launch, in launch order
+  std::vector<float> t_a, t_b;
+  int tune_stage = 2;                      // 0 time A, 1 time B, 2 tuned (or not tuned)
+  int tune_nb = 0;
+  ~Plan() {
+    for (auto &g : graphs)
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+    for (auto &e : ev) cudaEventDestroy(e);
+  }
 };
 
 static void add_tiles(std::vector<GemmTask> &v, int bm, int bn, int f, int r0, int r1, int c0, int c1, int k0,
@@ -1038,6 +1066,21 @@ Plan *build_plan(Handle &h, int small_m, bool tensor_schur) {
     sp.push_back((int64_t)P->tasks.size());
   }
   P->schur_ptr = sp;
+  P->pick.assign(S.nlevel, 0);
+  if (!tensor_schur) {
+    std::vector<int64_t> sb(1, (int64_t)P->tasks.size());
+    for (int l = 0; l < S.nlevel; ++l) {
+      for (int q = P->large_ptr[l]; q < P->large_ptr[l + 1]; ++q) {
+        const int f = P->fronts_large[q], k = S.k[f], m = S.m[f];
+        if (m > k) add_tiles(P->tasks, kSquare64, f, k, m, k, m, 0, k);
+      }
+      sb.push_back((int64_t)P->tasks.size());
+    }
+    P->schur_ptr_b = sb;
+    P->t_a.assign(S.nlevel, 0.f);
+    P->t_b.assign(S.nlevel, 0.f);
+    P->tune_stage = 0;
+  }
   return P;
 }
 
@@ -1114,16 +1157,15 @@ namespace ss {
 
 constexpr int kKrylovM = 30;            // FGMRES restart length (mixed precision)
 constexpr int kKrylovRestarts = 4;
-constexpr double kKrylovTol = 1e-13;    // relative residual target
-constexpr double kKrylovTolAdj = 1e-13; // same for the adjoint
-static int env_int(const char *name, int dflt) {
-  const char *v = getenv(name);
-  return v ? atoi(v) : dflt;
-}
-static double env_double(const char *name, double dflt) {
-  const char *v = getenv(name);
-  return v ? atof(v) : dflt;
-}
+// relative residual target of the primal and adjoint Krylov solves: with the
+// dual-weighted correction the charge error is the product of the two
+// residuals' effects, ~1e-12 relative at this target
+constexpr double kKrylovTol = 1e-10;
+struct SweepOpts {
+  int krylov_m = kKrylovM;
+  int restarts = kKrylovRestarts;
+  double tol = kKrylovTol;
+};
 
 template <class T>
 static int small_limit() { return sizeof(T) == 8 ? 96 : 128; }  // cd: 96^2*16, cf: 128^2*8 bytes
@@ -1182,22 +1224,91 @@ struct Sweeper {
   int64_t wstride = 0;
   int launches = 0, schur_launches = 0;
   int *tc_err = nullptr;                     // device flag: a tensor-core tile timed out
-  std::vector<cudaEvent_t> ev;               // Schur GEMM timing, one pair per level
+  std::vector<cudaEvent_t> &ev;              // Schur GEMM timing (the plan's events)
   int nev = 0;
   double schur_ms = 0;
-  explicit Sweeper(Handle &hh, Plan &pp) : h(hh), P(pp) {
-    ev.resize(2 * std::max(1, h.sym.nlevel));
-    for (auto &e : ev) cudaEventCreate(&e);
+  cplx<T> *stage_wv = nullptr;               // solve workspace baked into the solve graphs
+  cd *stage_b = nullptr, *stage_x = nullptr; // solve input / output staging for the graphs
+  explicit Sweeper(Handle &hh, Plan &pp) : h(hh), P(pp), ev(pp.ev) {
+    if (ev.empty()) {
+      ev.resize(2 * std::max(1, h.sym.nlevel));
+      for (auto &e : ev) cudaEventCreate(&e);
+    }
   }
-  ~Sweeper() {
-    for (auto &e : ev) cudaEventDestroy(e);
+
+  // Run `body` (a launch sequence on h.stream) through a cached CUDA graph keyed by
+  // (kind, nb, key pointers): captured on first use, replayed afterwards.
+  template <class Body>
+  int graphed(int kind, int nb, std::initializer_list<const void *> key, Body body) {
+    const void *k[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    int i = 0;
+    for (const void *p : key) k[i++] = p;
+    for (auto &g : P.graphs) {
+      if (g.kind != kind || g.nb != nb) continue;
+      bool same = true;
+      for (int j = 0; j < 8; ++j) same = same && g.key[j] == k[j];
+      if (!same) continue;
+      SS_CK(cudaGraphLaunch(g.exec, h.stream));
+      launches += g.launches;
+      schur_launches += g.schur_launches;
+      nev = g.nev;
+      return SS_OK;
+    }
+    const int l0 = launches, s0 = schur_launches;
+    nev = 0;
+    cudaGraph_t graph = nullptr;
+    SS_CK(cudaStreamBeginCapture(h.stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = body();
+    const cudaError_t ce = cudaStreamEndCapture(h.stream, &graph);
+    if (rc) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    SS_CK(ce);
+    Plan::Graph g;
+    g.kind = kind;
+    g.nb = nb;
+    for (int j = 0; j < 8; ++j) g.key[j] = k[j];
+    const cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    SS_CK(ie);
+    g.launches = launches - l0;
+    g.schur_launches = schur_launches - s0;
+    g.nev = nev;
+    P.graphs.push_back(g);
+    SS_CK(cudaGraphLaunch(g.exec, h.stream));
+    return SS_OK;
+  }
+  // factorisation of a chunk as one graph replay
+  int factor_graphed(int nb) {
+    // the tuner stage selects the Schur tiles baked into the graph
+    return graphed(10 * P.tune_stage, nb, {a.arena, a.piv, a.omega, a.Kc, a.Mc, a.Dc, a.nperturb, tc_err},
+                   [&] { return factor(nb); });
+  }
+  // x <- A'^-1 b (kind 1) or A'^-T b (kind 2) through a graph over fixed staging buffers
+  int solve_graphed(int kind, int nb, const cd *b, cd *x) {
+    const int64_t n = h.sym.n;
+    SS_CK(cudaMemcpyAsync(stage_b, b, (size_t)nb * n * sizeof(cd), cudaMemcpyDeviceToDevice, h.stream));
+    int rc = graphed(kind, nb, {a.arena, a.piv, stage_b, stage_x, stage_wv, a.Kc},
+                     [&] { return kind == 1 ? solve(nb, stage_b, stage_x, stage_wv) : solve_t(nb, stage_b, stage_x, stage_wv); });
+    if (rc) return rc;
+    SS_CK(cudaMemcpyAsync(x, stage_x, (size_t)nb * n * sizeof(cd), cudaMemcpyDeviceToDevice, h.stream));
+    return SS_OK;
   }
   // after the stream reached the end of factor(): add up the Schur GEMM time
-  void collect() {
+  void collect(int nb) {
+    // the autotuner times candidate A on the first full chunk, B on the second
+    const bool tuning = P.tune_stage < 2 && (P.tune_nb == 0 || P.tune_nb == nb);
     for (int i = 0; i < nev; ++i) {
       float ms = 0;
       cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]);
       schur_ms += ms;
+      if (tuning) (P.tune_stage == 0 ? P.t_a : P.t_b)[P.schur_level[i]] = ms;
+    }
+    if (tuning) {
+      P.tune_nb = nb;
+      if (++P.tune_stage == 2)
+        for (size_t l = 0; l < P.pick.size(); ++l) P.pick[l] = P.t_b[l] < P.t_a[l];
     }
     nev = 0;
   }
@@ -1242,13 +1353,18 @@ struct Sweeper {
       }
       const int64_t t0 = P.schur_ptr[l], t1 = P.schur_ptr[l + 1];
       if (t1 > t0) {
-        cudaEventRecord(ev[2 * nev], h.stream);
+        cudaEventRecordWithFlags(ev[2 * nev], h.stream, cudaEventRecordExternal);
+        const bool use_b = sizeof(T) == 8 && (P.tune_stage == 1 || (P.tune_stage == 2 && P.pick[l]));
         if (sizeof(T) == 4)
           tc::front_tc_gemm_kernel<<<dim3((unsigned)(t1 - t0), nb), tc::THREADS, tc::SMEM_BYTES, h.stream>>>(
               reinterpret_cast<cf *>(b.arena), b.stride, b.off, b.ld, tasks + t0, tc_err);
+        else if (use_b)
+          front_gemm_kernel<T, kSquare64><<<dim3((unsigned)(P.schur_ptr_b[l + 1] - P.schur_ptr_b[l]), nb), 256, 0,
+                                            h.stream>>>(b, tasks + P.schur_ptr_b[l]);
         else
           front_gemm_kernel<T, kSquare><<<dim3((unsigned)(t1 - t0), nb), 256, 0, h.stream>>>(b, tasks + t0);
-        cudaEventRecord(ev[2 * nev + 1], h.stream);
+        if ((int)P.schur_level.size() <= nev) P.schur_level.push_back(l);
+        cudaEventRecordWithFlags(ev[2 * nev + 1], h.stream, cudaEventRecordExternal);
         ++nev;
         ++launches;
         ++schur_launches;
@@ -1351,7 +1467,7 @@ namespace ss {
 
 template <class T>
 static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double *Qout, int *status,
-                      int *iters, double *disp, const SweepExtra *ex) {
+                      int *iters, double *disp, const SweepExtra *ex, const SweepOpts &opt) {
   Symbolic &S = h.sym;
   const int64_t n = S.n;
   const int pi = sizeof(T) == 8 ? 0 : 1;
@@ -1386,16 +1502,15 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
     if (rc) return rc;
   }
   const int64_t W = S.relpos_ptr[S.nfront];
-  const int krylov_m = env_int("SS_KRYLOV_M", kKrylovM);
-  const int krylov_restarts = env_int("SS_KRYLOV_RESTARTS", kKrylovRestarts);
-  const double tol_p = env_double("SS_KRYLOV_TOL", kKrylovTol);
-  const double tol_a = env_double("SS_KRYLOV_TOL_ADJ", kKrylovTolAdj);
+  const int krylov_m = opt.krylov_m;
+  const int krylov_restarts = opt.restarts;
+  const double tol_p = opt.tol, tol_a = opt.tol;
   const double krylov = sizeof(T) == 4 ? (2.0 * krylov_m + 2) * n * sizeof(cd) : 0.0;
   // the mixed sweep always solves the adjoint too (dual-weighted charge correction)
   const bool correct = sizeof(T) == 4;
   const bool need_adjoint = correct || (ex && ex->per_chunk);
   const double per = (double)S.arena * sizeof(cplx<T>) + n * 4.0 + W * (double)sizeof(cplx<T>) + n * 64.0 + krylov +
-                     (need_adjoint ? 32.0 * n : 0.0) + 256;
+                     (need_adjoint ? 32.0 * n : 0.0) + 32.0 * n + 256;
   KrylovWork kw;
   size_t fr = 0, tot = 0;
   SS_CK(cudaMemGetInfo(&fr, &tot));
@@ -1403,7 +1518,7 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
   DBuf &arena = h.wk[0], &piv = h.wk[1], &wv = h.wk[2], &b = h.wk[3], &x = h.wk[4], &r = h.wk[5], &dx = h.wk[6],
        &dom = h.wk[7], &npert = h.wk[8], &nrm = h.wk[9], &dQ = h.wk[10], &mu = h.wk[11], &cvec = h.wk[12];
   // the chunk size counts only memory not already held by these buffers
-  for (int i = 0; i < 13; ++i) fr += h.wk[i].bytes;
+  for (int i = 0; i < 16; ++i) fr += h.wk[i].bytes;
   int B = (int)std::max(1.0, std::min((double)n_f, std::min(256.0, (0.85 * (double)fr - 512e6) / per)));
   // a buffer that must grow is released first so that old and new never coexist
   if ((size_t)B * S.arena * sizeof(cplx<T>) > arena.bytes) arena.release();
@@ -1424,11 +1539,17 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
     int rc = build_transpose(h);
     if (rc) return rc;
   }
+  DBuf &stb = h.wk[14], &stx = h.wk[15];
+  SS_CK(dalloc(stb, (size_t)B * n * sizeof(cd)));
+  SS_CK(dalloc(stx, (size_t)B * n * sizeof(cd)));
   DBuf &tcerr = h.wk[13];
   SS_CK(dalloc(tcerr, sizeof(int)));
   SS_CK(cudaMemsetAsync(tcerr.p, 0, sizeof(int), h.stream));
   Sweeper<T> sw(h, P);
   sw.tc_err = tcerr.as<int>();
+  sw.stage_b = stb.as<cd>();
+  sw.stage_x = stx.as<cd>();
+  sw.stage_wv = wv.as<cplx<T>>();
   FrontArgs<T> &a = sw.a;
   a.k = h.d_k.as<int>();
   a.m = h.d_m.as<int>();
@@ -1482,10 +1603,10 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
                                                    h.dms.as<cd>(), damp ? h.dds.as<cd>() : nullptr,
                                                    h.drow_scale.as<double>(), b.as<cd>());
     cudaEventRecord(e0, h.stream);
-    int rc = sw.factor(nb);
+    int rc = sw.factor_graphed(nb);
     if (rc) return rc;
     cudaEventRecord(e1, h.stream);
-    rc = sw.solve(nb, b.as<cd>(), x.as<cd>(), wv.as<cplx<T>>());
+    rc = sw.solve_graphed(1, nb, b.as<cd>(), x.as<cd>());
     if (rc) return rc;
     cudaEventRecord(e2, h.stream);
     SS_CK(cudaEventSynchronize(e2));
@@ -1494,7 +1615,7 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
     cudaEventElapsedTime(&ms2, e1, e2);
     fac_ms += ms1;
     sol_ms += ms2;
-    sw.collect();
+    sw.collect(nb);
     std::fill(conv.begin(), conv.end(), 0);
     std::fill(hit.begin(), hit.end(), 0);
     const bool use_krylov = sizeof(T) == 4 || getenv("SS_FP64_KRYLOV") != nullptr;
@@ -1503,7 +1624,7 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
       // FGMRES-IR: FP64 Krylov, complex64 factors as right preconditioner
       std::vector<int> kits;
       std::vector<char> kconv;
-      auto pre = [&](const cd *src, cd *dst) { return sw.solve(nb, src, dst, wv.as<cplx<T>>()); };
+      auto pre = [&](const cd *src, cd *dst) { return sw.solve_graphed(1, nb, src, dst); };
       rc = fgmres(h, kw, opA, nb, krylov_m, krylov_restarts, tol_p, a.Kc, a.Mc, a.Dc, dom.as<double>(), b.as<cd>(),
                   x.as<cd>(), pre, kits, kconv);
       if (rc) return rc;
@@ -1526,7 +1647,7 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
       residual_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, h.dc_ptr.as<int64_t>(), h.dc_idx.as<int64_t>(), nullptr,
                                                           a.Kc, a.Mc, a.Dc, dom.as<double>(), h.beta, b.as<cd>(),
                                                           x.as<cd>(), r.as<cd>());
-      rc = sw.solve(nb, r.as<cd>(), dx.as<cd>(), wv.as<cplx<T>>());
+      rc = sw.solve_graphed(1, nb, r.as<cd>(), dx.as<cd>());
       if (rc) return rc;
       axpy_norm_kernel<<<nb, 256, 0, h.stream>>>(n, x.as<cd>(), dx.as<cd>(), nrm.as<double>());
       SS_CK(cudaMemcpyAsync(hn.data(), nrm.p, 2 * nb * sizeof(double), cudaMemcpyDeviceToHost, h.stream));
@@ -1550,12 +1671,12 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
       const MatOp opT{h.dct_ptr.as<int64_t>(), h.dct_idx.as<int64_t>(), h.dct_src.as<int64_t>()};
       charge_row_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, h.dks.as<cd>() + n, h.dcol_scale.as<double>(),
                                                           cvec.as<cd>());
-      rc = sw.solve_t(nb, cvec.as<cd>(), mu.as<cd>(), wv.as<cplx<T>>());
+      rc = sw.solve_graphed(2, nb, cvec.as<cd>(), mu.as<cd>());
       if (rc) return rc;
       if (use_krylov) {
         std::vector<int> kits;
         std::vector<char> kconv;
-        auto pre = [&](const cd *src, cd *dst) { return sw.solve_t(nb, src, dst, wv.as<cplx<T>>()); };
+        auto pre = [&](const cd *src, cd *dst) { return sw.solve_graphed(2, nb, src, dst); };
         rc = fgmres(h, kw, opT, nb, krylov_m, krylov_restarts, tol_a, a.Kc, a.Mc, a.Dc, dom.as<double>(),
                     cvec.as<cd>(), mu.as<cd>(), pre, kits, kconv);
         if (rc) return rc;
@@ -1565,7 +1686,7 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
         residual_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, opT.rp, opT.ci, opT.vp, a.Kc, a.Mc, a.Dc,
                                                             dom.as<double>(), h.beta, cvec.as<cd>(), mu.as<cd>(),
                                                             r.as<cd>());
-        rc = sw.solve_t(nb, r.as<cd>(), dx.as<cd>(), wv.as<cplx<T>>());
+        rc = sw.solve_graphed(2, nb, r.as<cd>(), dx.as<cd>());
         if (rc) return rc;
         axpy_norm_kernel<<<nb, 256, 0, h.stream>>>(n, mu.as<cd>(), dx.as<cd>(), nrm.as<double>());
       }
@@ -1643,13 +1764,46 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
   h.st[17] = total_ms;
   h.st[14] = perturbed;
   h.st[15] = sw.launches;
+  {
+    double tot = 0;
+    if (iters)
+      for (int i = 0; i < n_f; ++i) tot += iters[i];
+    h.st[18] = tot;
+  }
   return SS_OK;
 }
 
+// SS_PREC_AUTO: a probe of the mixed sweep on the band's two end points with a
+// short Krylov budget (12 steps each for the primal and the adjoint); if both
+// converge the whole sweep runs
+// mixed, otherwise FP64 (the complex64 factors of a cell whose conditioning
+// defeats FP32 would need many Krylov steps per point).
 int run_sweep(Handle &h, int n_f, const double *omega, double V, int precision, double *Q, int *status,
               int *iters, double *disp_out, const SweepExtra *ex) {
-  if (precision == SS_PREC_MIXED) return sweep_impl<float>(h, n_f, omega, V, Q, status, iters, disp_out, ex);
-  return sweep_impl<double>(h, n_f, omega, V, Q, status, iters, disp_out, ex);
+  SweepOpts opt;
+  int rc;
+  double probe_ms = 0, probe_launches = 0;
+  if (precision == SS_PREC_AUTO && n_f > 0) {
+    const double ends[2] = {omega[0], omega[n_f - 1]};
+    double q[4];
+    int st[2] = {0, 0}, it[2] = {0, 0};
+    SweepOpts probe;
+    probe.restarts = 1;
+    probe.krylov_m = 12;
+    rc = sweep_impl<float>(h, n_f > 1 ? 2 : 1, ends, V, q, st, it, nullptr, nullptr, probe);
+    if (rc) return rc;
+    precision = (st[0] == SS_OK && st[1] == SS_OK) ? SS_PREC_MIXED : SS_PREC_FP64;
+    probe_ms = h.st[17];
+    probe_launches = h.st[15];
+  }
+  if (precision == SS_PREC_MIXED)
+    rc = sweep_impl<float>(h, n_f, omega, V, Q, status, iters, disp_out, ex, opt);
+  else
+    rc = sweep_impl<double>(h, n_f, omega, V, Q, status, iters, disp_out, ex, opt);
+  h.st[19] = precision;
+  h.st[17] += probe_ms;        // the probe is part of an AUTO sweep's device time
+  h.st[15] += probe_launches;
+  return rc;
 }
 
 }  // namespace ss

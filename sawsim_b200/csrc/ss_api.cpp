@@ -278,6 +278,7 @@ extern "C" int ss_set_damping(ss_handle *hp, double beta) {
   if (beta < 0.0) return fail(h, SS_EINVAL, "damping: beta must be >= 0");
   h.beta = beta;
   h.scale_w = -1;
+  free_plans(h);   // the captured launch graphs bake beta and the damping matrix in
   return SS_OK;
 }
 
@@ -286,7 +287,8 @@ extern "C" int ss_sweep(ss_handle *hp, int n_f, const double *omega, double V, i
   H_CHECK(hp);
   if (!h.analyzed) return fail(h, SS_ESTATE, "sweep: analyze first");
   if (n_f < 0 || (n_f > 0 && (!omega || !Q))) return fail(h, SS_EINVAL, "sweep: bad frequency arrays");
-  if (precision != SS_PREC_FP64 && precision != SS_PREC_MIXED) return fail(h, SS_EINVAL, "sweep: bad precision");
+  if (precision != SS_PREC_FP64 && precision != SS_PREC_MIXED && precision != SS_PREC_AUTO)
+    return fail(h, SS_EINVAL, "sweep: bad precision");
   if (V == 0.0) return fail(h, SS_EINVAL, "sweep: V must be nonzero");
   for (int i = 0; i < n_f; ++i)
     if (!(omega[i] > 0.0)) return fail(h, SS_EINVAL, "sweep: omega must be positive");
@@ -336,4 +338,20 @@ extern "C" int ss_solve_adjoint(ss_handle *hp, double omega, int precision, doub
     lambda[2 * P + 1] = mu[R].im * rs[R];
   }
   return st;
+}
+
+extern "C" int ss_adjoint_gradient(ss_handle *hp, int n_f, const double *omega, double V, int precision,
+                                   int n_params, const double *dpos, const double *dC, const double *de,
+                                   const double *deps, const double *drho, const double *dinner,
+                                   const double *douter, double *Q, double *dQ, int *status) {
+  H_CHECK(hp);
+  if (!h.analyzed) return fail(h, SS_ESTATE, "gradient: analyze first");
+  if (n_f <= 0 || !omega || !Q || !dQ || n_params <= 0) return fail(h, SS_EINVAL, "gradient: bad arguments");
+  if (precision != SS_PREC_FP64 && precision != SS_PREC_MIXED && precision != SS_PREC_AUTO)
+    return fail(h, SS_EINVAL, "gradient: bad precision");
+  if (V == 0.0) return fail(h, SS_EINVAL, "gradient: V must be nonzero");
+  for (int i = 0; i < n_f; ++i)
+    if (!(omega[i] > 0.0)) return fail(h, SS_EINVAL, "gradient: omega must be positive");
+  return run_adjoint_gradient(h, n_f, omega, V, precision, n_params, dpos, dC, de, deps, drho, dinner, douter, Q,
+                              dQ, status);
 }

@@ -142,6 +142,11 @@ struct SweepExtra {
 };
 int run_sweep(Handle &h, int n_f, const double *omega, double V, int precision,
               double *Q, int *status, int *iters, double *disp_out, const SweepExtra *ex = nullptr);
+// adjoint.cu: Q (n_f x 2) and dQ (n_f x n_params x 2) with the seeds of ss_adjoint_gradient
+int run_adjoint_gradient(Handle &h, int n_f, const double *omega, double V, int precision, int n_params,
+                         const double *dpos, const double *dC, const double *de, const double *deps,
+                         const double *drho, const double *dinner, const double *douter, double *Q, double *dQ,
+                         int *status);
 // symbolic.cpp
 int build_global_pattern(Handle &h);
 int build_condensation(Handle &h);

@@ -17,9 +17,10 @@
 // level of the SIMT kernel this replaces.
 //
 // Tile: 128 complex rows x 64 complex columns (M = 128, N = 128 real) per CTA,
-// K in chunks of 16 complex (one 128-byte swizzle row of fp32), 2 stages of
-// 64 KB (A hi/lo, B' hi/lo).  256 threads stage the operands; thread 0 issues 12
-// MMAs of 128x128x8 per chunk.  Every mbarrier wait is bounded: on time-out the
+// K in chunks of 16 complex (one 128-byte swizzle row of fp32).  Raw tiles
+// stream in with cp.async three chunks deep (24 KB each); 256 threads convert
+// each into the split, swizzled operands (2 stages of 64 KB: A hi/lo, B' hi/lo);
+// thread 0 issues 12 MMAs of 128x128x8 per chunk.  Every mbarrier wait is bounded: on time-out the
 // CTA records the error, drains its own MMAs (bounded), frees its tensor memory
 // and returns without touching C.
 #pragma once
@@ -39,11 +40,16 @@ namespace tc {
 constexpr int BM = 128;              // complex rows per tile (MMA M)
 constexpr int BN = 64;               // complex columns per tile (MMA N = 128 real)
 constexpr int BKC = 16;              // complex K per chunk (32 fp32 = one 128-byte row)
-constexpr int STAGES = 2;
+constexpr int STAGES = 2;                             // operand stages (MMA side)
+constexpr int RAW_STAGES = 3;                         // raw tile stages (cp.async side)
 constexpr int THREADS = 256;
 constexpr int OPER_BYTES = 128 * 128;                 // 128 rows x 128 bytes
 constexpr int STAGE_BYTES = 4 * OPER_BYTES;           // A hi, A lo, B hi, B lo
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;   // + alignment slack
+constexpr int RAW_A_BYTES = BM * BKC * 8;             // 128 rows x 16 complex
+constexpr int RAW_B_STRIDE = BN * 8 + 32;             // bytes per raw B row (+32: conflict-free reads)
+constexpr int RAW_B_BYTES = BKC * RAW_B_STRIDE;       // 16 rows x 64 complex
+constexpr int RAW_BYTES = RAW_A_BYTES + RAW_B_BYTES;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + RAW_STAGES * RAW_BYTES + 1024;   // + alignment slack
 constexpr int TMEM_COLS = 128;
 constexpr uint64_t kWaitNs = 200000000ull;           // 0.2 s bound on any mbarrier wait
 
@@ -57,6 +63,17 @@ __device__ __forceinline__ float tf32_hi(float v) {
   if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x1000u) & 0xffffe000u;
   return __uint_as_float(u);
 }
+
+// asynchronous global -> shared copies; src_bytes < size zero-fills the rest
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, uint32_t src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async8(uint32_t dst, const void *src, uint32_t src_bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups 1024 B apart
 __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
@@ -137,63 +154,54 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
 // byte offset of 16-byte chunk q of row r in a 128-byte-swizzled K-major operand
 __device__ __forceinline__ uint32_t sw_off(int r, int q) { return (uint32_t)(r * 128 + ((q ^ (r & 7)) << 4)); }
 
-// Per thread per chunk: A 128 rows x 8 float4 -> 4 float4 each; B 16 k-rows x 64
-// complex columns -> 4 complex each.
-struct Frag {
-  float4 a[4];
-  float2 b[4];
-};
-
-__device__ __forceinline__ void load_chunk(const cf *F, int ld, const GemmTask &tk, int kb, Frag &fr) {
+// Raw tiles of one K chunk into shared memory with cp.async: A 128 rows x 16
+// complex (16-byte pieces: two complex, aligned because ld, the front offsets
+// and the chunk start are even), B 16 rows x 64 complex (8-byte pieces: the
+// column start k + 64 t may be odd).  Out-of-range pieces are zero-filled.
+__device__ __forceinline__ void issue_chunk(unsigned char *raw, const cf *F, int ld, const GemmTask &tk, int kb) {
   const int t = threadIdx.x;
+  const uint32_t ra = smem_u32(raw), rb = ra + RAW_A_BYTES;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const int idx = t + THREADS * i;        // 0..1023
     const int row = idx >> 3, q = idx & 7;  // q: pair of complex K columns
     const int r = tk.r0 + row, c = kb + 2 * q;
-    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (r < tk.rhi) {
-      const cf *p = F + (int64_t)r * ld + c;
-      if (c + 1 < tk.kk1) {
-        v = make_float4(p[0].x, p[0].y, p[1].x, p[1].y);
-      } else if (c < tk.kk1) {
-        v = make_float4(p[0].x, p[0].y, 0.f, 0.f);
-      }
-    }
-    fr.a[i] = v;
+    const int valid = (r < tk.rhi) ? max(0, min(2, tk.kk1 - c)) : 0;
+    const cf *src = valid ? F + (int64_t)r * ld + c : F;
+    cp_async16(ra + (uint32_t)(row * 128 + q * 16), src, (uint32_t)(valid * 8));
   }
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const int idx = t + THREADS * i;        // 0..1023
     const int j = idx >> 6, cc = idx & 63;  // complex k-row, complex column
     const int r = kb + j, c = tk.c0 + cc;
-    float2 v = make_float2(0.f, 0.f);
-    if (r < tk.kk1 && c < tk.chi) {
-      const cf e = F[(int64_t)r * ld + c];
-      v = make_float2(e.x, e.y);
-    }
-    fr.b[i] = v;
+    const bool ok = r < tk.kk1 && c < tk.chi;
+    cp_async8(rb + (uint32_t)(j * RAW_B_STRIDE + cc * 8), ok ? F + (int64_t)r * ld + c : F, ok ? 8u : 0u);
   }
 }
 
-__device__ __forceinline__ void store_chunk(unsigned char *stage, const Frag &fr) {
+// Raw tiles -> the four MMA operands (A hi/lo, B' hi/lo) in 128-byte swizzle.
+__device__ __forceinline__ void convert_chunk(const unsigned char *raw, unsigned char *stage) {
   unsigned char *ahi = stage, *alo = stage + OPER_BYTES, *bhi = stage + 2 * OPER_BYTES, *blo = stage + 3 * OPER_BYTES;
   const int t = threadIdx.x;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const int idx = t + THREADS * i;
     const int row = idx >> 3, q = idx & 7;
-    const float4 v = fr.a[i];
+    const float4 v = *reinterpret_cast<const float4 *>(raw + row * 128 + q * 16);
     const float4 h = make_float4(tf32_hi(v.x), tf32_hi(v.y), tf32_hi(v.z), tf32_hi(v.w));
     const float4 l = make_float4(v.x - h.x, v.y - h.y, v.z - h.z, v.w - h.w);
     *reinterpret_cast<float4 *>(ahi + sw_off(row, q)) = h;
     *reinterpret_cast<float4 *>(alo + sw_off(row, q)) = l;
   }
+  // B: a warp takes 8 k-rows x 4 columns per step, so that its stores cover every
+  // (swizzle slot, half) pair of the rows 2cc / 2cc+1 twice (two wavefronts)
+  const int lane = t & 31, wrp = t >> 5;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const int idx = t + THREADS * i;
-    const int j = idx >> 6, cc = idx & 63;
-    const float2 v = fr.b[i];
+    const int j = 8 * (i & 1) + (lane & 7);
+    const int cc = 4 * (wrp + 8 * (i >> 1)) + (lane >> 3);
+    const float2 v = *reinterpret_cast<const float2 *>(raw + RAW_A_BYTES + j * RAW_B_STRIDE + cc * 8);
     const float hr = tf32_hi(v.x), hi = tf32_hi(v.y), nhi = tf32_hi(-v.y);
     const float lr = v.x - hr, li = v.y - hi, nli = -v.y - nhi;
     // real K positions (2j, 2j+1) = byte 8j of the row: chunk j/2, half j%2
@@ -244,13 +252,24 @@ __global__ void __launch_bounds__(THREADS, 1)
   tc_fence_after();
   const uint32_t tmem = tmem_base_s;
 
-  Frag fr;
-  load_chunk(F, ld, tk, tk.kk0, fr);
+  unsigned char *raw0 = smem + STAGES * STAGE_BYTES;
+  // prologue: the first RAW_STAGES - 1 chunks in flight
+#pragma unroll
+  for (int c = 0; c < RAW_STAGES - 1; ++c) {
+    if (c < nk) issue_chunk(raw0 + c * RAW_BYTES, F, ld, tk, tk.kk0 + c * BKC);
+    cp_async_commit();
+  }
   bool ok = true;
   for (int kc = 0; kc < nk; ++kc) {
     const int s = kc % STAGES;
     unsigned char *stage = smem + s * STAGE_BYTES;
-    // the MMAs that read this stage two chunks ago must be complete
+    // chunk kc + RAW_STAGES - 1 into the raw stage that held chunk kc - 1 (converted
+    // in the previous iteration, before its closing barrier)
+    const int cn = kc + RAW_STAGES - 1;
+    if (cn < nk) issue_chunk(raw0 + (cn % RAW_STAGES) * RAW_BYTES, F, ld, tk, tk.kk0 + cn * BKC);
+    cp_async_commit();
+    cp_async_wait<RAW_STAGES - 1>();                 // this thread's pieces of chunk kc landed
+    // the MMAs that read this operand stage two chunks ago must be complete
     if (kc >= STAGES) {
       if (!mbar_wait(smem_u32(&bars[s]), (uint32_t)((kc / STAGES - 1) & 1))) abort_s = 1;
     }
@@ -259,10 +278,9 @@ __global__ void __launch_bounds__(THREADS, 1)
       ok = false;
       break;
     }
-    store_chunk(stage, fr);
+    convert_chunk(raw0 + (kc % RAW_STAGES) * RAW_BYTES, stage);
     fence_async_smem();
     __syncthreads();
-    if (kc + 1 < nk) load_chunk(F, ld, tk, tk.kk0 + (kc + 1) * BKC, fr);   // next chunk in flight
     if (threadIdx.x == 0) {
       tc_fence_after();
       const uint32_t base = smem_u32(stage);
@@ -277,6 +295,7 @@ __global__ void __launch_bounds__(THREADS, 1)
       mma_commit(smem_u32(&bars[s]));
     }
   }
+  cp_async_wait<0>();                                // no copy outlives the CTA
   // all MMAs of this CTA complete (the last commit tracks every earlier MMA)
   if (threadIdx.x == 0) {
     if (ok) {

@@ -19,7 +19,7 @@ import scipy.sparse as sp
 from . import _lib as L
 from .materials import pack
 
-PRECISION = {'fp64': L.SS_PREC_FP64, 'mixed': L.SS_PREC_MIXED}
+PRECISION = {'fp64': L.SS_PREC_FP64, 'mixed': L.SS_PREC_MIXED, 'auto': L.SS_PREC_AUTO}
 
 
 class Handle:
@@ -160,7 +160,7 @@ class FrequencySolver:
         keys = ['n_active', 'n_fronts', 'max_front', 'factor_flops_per_point', 'nnz_lu', 'analyze_s',
                 'assemble_ms', 'sweep_ms', 'factor_ms', 'solve_ms', 'chunk', 'schur_gemm_ms',
                 'schur_gemm_flops', 'levels', 'perturbed_pivots', 'launches', 'schur_launches',
-                'sweep_device_ms', 'refine_solves']
+                'sweep_device_ms', 'refine_solves', 'precision_used']
         return dict(zip(keys, out.tolist()))
 
     @property
@@ -209,6 +209,45 @@ class FrequencySolver:
         lam = np.zeros(2 * n)
         self._h('ss_solve_adjoint', float(omega), PRECISION[precision], L.ptr(lam, C.c_double))
         return lam.view(np.complex128)
+
+    def gradient(self, omegas, seeds, V: float = 1.0, precision: str = 'fp64'):
+        """Charges and dQ/dp by the adjoint (``ss_adjoint_gradient``).
+
+        ``seeds``: one dict per parameter with optional keys dpos (n_nodes x 2,
+        metres per unit p), dC (n_mat x 6 x 6), de (n_mat x 3 x 6), deps
+        (n_mat x 3 x 3) complex, drho (n_mat,), dinner / douter (n_regions x 3).
+        Returns ``(Q[n_f], dQ[n_f, n_params], status[n_f])``."""
+        om = L.f64(np.atleast_1d(omegas))
+        npar = len(seeds)
+
+        def stack(key, shape, cplx):
+            if all(sd.get(key) is None for sd in seeds):
+                return None
+            out = []
+            for sd in seeds:
+                a = sd.get(key)
+                a = np.zeros(shape, complex if cplx else float) if a is None else np.asarray(a)
+                if cplx:
+                    a = np.stack([np.real(a), np.imag(a)], axis=-1)
+                out.append(np.asarray(a, dtype=np.float64).reshape(-1))
+            return np.ascontiguousarray(np.concatenate(out))
+
+        n_nodes = self.gdof // (self.ndisp + 1)
+        first = next((sd for sd in seeds if sd.get('dC') is not None or sd.get('drho') is not None), None)
+        n_mat = 0 if first is None else len(first['dC'] if first.get('dC') is not None else first['drho'])
+        nreg_src = next((sd for sd in seeds if sd.get('dinner') is not None or sd.get('douter') is not None), None)
+        nreg = 0 if nreg_src is None else np.asarray(
+            nreg_src['dinner'] if nreg_src.get('dinner') is not None else nreg_src['douter']).shape[0]
+        arrs = [stack('dpos', (n_nodes, 2), False), stack('dC', (n_mat, 6, 6), True), stack('de', (n_mat, 3, 6), True),
+                stack('deps', (n_mat, 3, 3), True), stack('drho', (n_mat,), False),
+                stack('dinner', (nreg, 3), False), stack('douter', (nreg, 3), False)]
+        ptrs = [None if a is None else L.ptr(a, C.c_double) for a in arrs]
+        Q = np.zeros(2 * om.size)
+        dQ = np.zeros(2 * om.size * npar)
+        st = np.zeros(om.size, dtype=np.int32)
+        self._h('ss_adjoint_gradient', om.size, L.ptr(om, C.c_double), float(V), PRECISION[precision], npar, *ptrs,
+                L.ptr(Q, C.c_double), L.ptr(dQ, C.c_double), L.ptr(st, C.c_int))
+        return Q.view(np.complex128), dQ.view(np.complex128).reshape(om.size, npar), st
 
     def close(self):
         self._h.close()

@@ -50,7 +50,8 @@ def test_adjoint_backward_error_in_oracle_system(mid, precision):
     A, _ = o.system(w)
     kq = (o._T.T @ o.kts)[o.active]
     lam = g.solve_adjoint(w, precision)
-    assert _backward_error(A.T.tocsr(), lam, kq) < 1e-12
+    # FP64: direct solve + one refinement step; mixed: the Krylov target (1e-10)
+    assert _backward_error(A.T.tocsr(), lam, kq) < (1e-12 if precision == 'fp64' else 1e-10)
 
 
 def test_mixed_matches_fp64(mid):
