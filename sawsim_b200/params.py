@@ -25,8 +25,15 @@ import numpy as np
 
 from . import cases, cells, materials as mt
 
-GEOMETRY = ['pitch_um', 't_film_um', 't_sio2_um', 't_si_um']
 MATERIAL = ['euler_theta_deg', 'C11', 'C12', 'C13', 'C14', 'C33', 'C44']
+# layer stacks below the film: (name, tag, thickness in pitches, row fraction numerator /32)
+STACKS = {
+    'two_layer': dict(layers=[('film', 16, 0.6, 6), ('sio2', 22, 0.3, 3), ('si', 23, 3.0, None)], pml=(24, 6),
+                      materials=['sio2', 'si_cubic']),
+    'four_layer': dict(layers=[('film', 16, 0.5, 5), ('sio2', 22, 0.25, 3), ('polysi', 23, 0.5, 5), ('si', 24, 3.0, None)],
+                       pml=(25, 5), materials=['sio2', 'poly_si', 'si_cubic']),
+}
+GEOMETRY = ['pitch_um', 't_film_um', 't_sio2_um', 't_si_um']
 
 
 def _rx_derivative(angles_deg):
@@ -56,13 +63,16 @@ def rotation_tangent(crystal: mt.Material, angles_deg) -> mt.Material:
 
 @dataclass
 class Q9Model:
-    """The ME1 two-layer cell of ``cells.me1_two_layer_cell`` as a function of
-    GEOMETRY + MATERIAL parameters (defaults: pitch 1.085 um, film 0.6p, SiO2 0.3p,
-    Si 3p; PML thickness = pitch; electrodes 0.08 p0 thick)."""
+    """An ME1 Q9 cell as a function of its geometry (pitch and every layer
+    thickness, um) and MATERIAL parameters.  ``stack='two_layer'``: the cell of
+    ``cells.me1_two_layer_cell`` (film 0.6p, SiO2 0.3p, Si 3p); ``'four_layer'``:
+    ``cells.me1_four_layer_cell`` (film 0.5p, SiO2 0.25p, poly-Si 0.5p, Si 3p).
+    PML thickness = pitch; electrodes 0.08 p0 thick."""
 
     cols: int = 64
     rows: int = 256
     seed: int = 0
+    stack: str = 'two_layer'
     f0: float = 1.6e9
     f1: float = 2.0e9
     crystal: mt.Material = field(init=False)
@@ -79,28 +89,40 @@ class Q9Model:
         return dict(C11=C[0, 0], C12=C[0, 1], C13=C[0, 2], C14=C[0, 3], C33=C[2, 2], C44=C[3, 3])
 
     @property
+    def geometry(self):
+        return ['pitch_um'] + [f't_{name}_um' for name, *_ in STACKS[self.stack]['layers']]
+
+    @property
     def names(self):
-        return GEOMETRY + MATERIAL
+        return self.geometry + MATERIAL
 
     def defaults(self) -> np.ndarray:
         p = 1.085
         k = self.k3m
-        return np.array([p, 0.6 * p, 0.3 * p, 3 * p, float(self.euler[1]), k['C11'], k['C12'], k['C13'], k['C14'],
-                         k['C33'], k['C44']])
+        th = [t * p for _, _, t, _ in STACKS[self.stack]['layers']]
+        return np.array([p] + th + [float(self.euler[1]), k['C11'], k['C12'], k['C13'], k['C14'], k['C33'],
+                                    k['C44']])
 
     # ------------------------------------------------------------------ build
     def _cell(self, v):
-        p, tf, to, ts = v[:4]
-        r_film = self.rows * 3 // 16
-        r_ox = self.rows * 3 // 32
-        r_pml = self.rows * 3 // 16
-        r_si = self.rows - r_film - r_ox - r_pml
-        return cells.q9_cell(p, self.cols, [cells.Band(cells.TAG_PIEZO, tf, r_film), cells.Band(22, to, r_ox),
-                                            cells.Band(23, ts, r_si), cells.Band(24, p, r_pml)],
+        st = STACKS[self.stack]
+        ng = len(self.geometry)
+        p, th = v[0], v[1:ng]
+        pml_tag, pml_frac = st['pml']
+        r_pml = self.rows * pml_frac // 32
+        bands, used = [], r_pml
+        for (name, tag, _, frac), t in zip(st['layers'], th):
+            r = self.rows * frac // 32 if frac else None
+            bands.append([tag, t, r])
+            used += r or 0
+        for b in bands:
+            if b[2] is None:
+                b[2] = self.rows - used
+        return cells.q9_cell(p, self.cols, [cells.Band(*b) for b in bands] + [cells.Band(pml_tag, p, r_pml)],
                              cells.Band(cells.TAG_ELECTRODE, 0.08 * 1.085, 1))
 
     def _crystal_at(self, v):
-        k = dict(zip(MATERIAL[1:], v[5:]))
+        k = dict(zip(MATERIAL[1:], v[len(self.geometry) + 1:]))
         x = self.crystal
         C = mt.trigonal_3m(dict(k, e15=0, e22=0, e31=0, e33=0, eps11=1, eps33=1), x.rho).C
         return mt.Material(x.rho, C, x.e, x.eps)
@@ -110,9 +132,9 @@ class Q9Model:
         v = np.asarray(v, dtype=float)
         cell = self._cell(v)
         mesh = cases.mesh_from_msh(cell.msh())
-        angles = np.array([self.euler[0], v[4], self.euler[2]])
+        angles = np.array([self.euler[0], v[len(self.geometry)], self.euler[2]])
         piezo = mt.rotate(self._crystal_at(v), angles)
-        mats = [piezo, mt.al(), mt.sio2(), mt.si_cubic()]
+        mats = [piezo, mt.al()] + [getattr(mt, m)() for m in STACKS[self.stack]['materials']]
         idx = np.array([cell.tag_map[t] for t in mesh.elem_tag], dtype=np.int64)
         bottom = float(mesh.pos_m[:, 1].min())
         pml = [cases.PML(tag=cell.pml_tag, kind='y', yp=bottom, ya=cell.pml_top_um * 1e-6)]
@@ -126,10 +148,11 @@ class Q9Model:
         """Derivative seeds of every parameter at ``v`` (one dict per parameter)."""
         v = np.asarray(v, dtype=float)
         out = []
-        n_mat = 4
+        n_mat = 2 + len(STACKS[self.stack]['materials'])
+        it = len(self.geometry)
         for i, name in enumerate(self.names):
             s = dict(dpos=None, dC=None, de=None, deps=None, drho=None, dinner=None, douter=None)
-            if name in GEOMETRY:
+            if name in self.geometry:
                 h = 0.05 * v[i]
                 vp, vm = v.copy(), v.copy()
                 vp[i] += h
@@ -144,7 +167,7 @@ class Q9Model:
                 dC = np.zeros((n_mat, 6, 6), complex)
                 de = np.zeros((n_mat, 3, 6), complex)
                 deps = np.zeros((n_mat, 3, 3), complex)
-                angles = np.array([self.euler[0], v[4], self.euler[2]])
+                angles = np.array([self.euler[0], v[it], self.euler[2]])
                 if name == 'euler_theta_deg':
                     t = rotation_tangent(self._crystal_at(v), angles)
                     dC[0], de[0], deps[0] = t.C, t.e, t.eps
