@@ -312,27 +312,37 @@ __global__ void __launch_bounds__(THREADS, 1)
   __syncthreads();
   tc_fence_after();
   if (!abort_s) {
-    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +32 (tile rows), real
-    // columns 64 (w / 4) .. +64 (32 complex columns)
+    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +32 (tile rows) and real
+    // columns 64 (w / 4) .. +64 (32 complex columns) into a padded row-major
+    // staging tile in the (now idle) operand stages; then every warp updates
+    // whole rows of C with coalesced loads and stores
+    constexpr int SROW = BN * 8 + 8;                  // staging row stride (bytes)
+    unsigned char *stg = smem;
     const int row = 32 * (wid & 3) + lane;
-    const int r = tk.r0 + row;
     const int cb = 32 * (wid >> 2);
     float v[32];
 #pragma unroll
     for (int half = 0; half < 2; ++half) {
       const uint32_t taddr = tmem + ((uint32_t)(32 * (wid & 3)) << 16) + (uint32_t)(64 * (wid >> 2) + 32 * half);
       tmem_ld32(taddr, v);
-      if (r < tk.rhi) {
-        cf *crow = F + (int64_t)r * ld;
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int c = tk.c0 + cb + 16 * half + j;
-          if (c < tk.chi) {
-            cf d = crow[c];
-            d.x -= v[2 * j];
-            d.y -= v[2 * j + 1];
-            crow[c] = d;
-          }
+      for (int j = 0; j < 16; ++j)
+        *reinterpret_cast<float2 *>(stg + row * SROW + (cb + 16 * half + j) * 8) = make_float2(v[2 * j], v[2 * j + 1]);
+    }
+    __syncthreads();
+    for (int rr = wid; rr < BM; rr += THREADS / 32) {
+      const int r = tk.r0 + rr;
+      if (r >= tk.rhi) break;
+      cf *crow = F + (int64_t)r * ld + tk.c0;
+#pragma unroll
+      for (int h2 = 0; h2 < 2; ++h2) {
+        const int c = lane + 32 * h2;
+        if (tk.c0 + c < tk.chi) {
+          const float2 acc = *reinterpret_cast<const float2 *>(stg + rr * SROW + c * 8);
+          cf d = crow[c];
+          d.x -= acc.x;
+          d.y -= acc.y;
+          crow[c] = d;
         }
       }
     }
