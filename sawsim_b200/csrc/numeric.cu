@@ -536,6 +536,104 @@ __global__ void __launch_bounds__(256) front_gemm_kernel(FrontArgs<T> a, const G
     }
 }
 
+// FP64 complex tile C -= A B on the FP64 tensor cores (DMMA, mma.sync m8n8k4 f64):
+// 64x64 complex outputs per 128-thread CTA, a 32x32 complex warp tile (4x4 blocks
+// of 8x8), K in chunks of 8 complex staged by cp.async (double-buffered).  Each
+// 8x8x4 complex block is four real MMAs: Dr += Ar Br - Ai Bi, Di += Ar Bi + Ai Br.
+// Fragments (PTX m8n8k4 .f64): A[g][t], B[t][g], C[g][2t + i] with g = lane / 4,
+// t = lane % 4.
+constexpr int kDmmaBM = 64, kDmmaBN = 64, kDmmaBK = 8;
+constexpr int kDmmaAS = kDmmaBK + 1;          // A row stride in complex (+1: conflict-free fragment reads)
+
+__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+__device__ __forceinline__ void cp_async16_cd(uint32_t dst, const void *src, uint32_t bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+
+__global__ void __launch_bounds__(128) front_dmma_kernel(FrontArgs<double> a, const GemmTask *__restrict__ tasks) {
+  __shared__ __align__(16) cd As[2][kDmmaBM * kDmmaAS];
+  __shared__ __align__(16) cd Bs[2][kDmmaBK * kDmmaBN];
+  const GemmTask tk = tasks[blockIdx.x];
+  const int fq = blockIdx.y;
+  const int ld = a.ld[tk.f];
+  cd *F = a.arena + (int64_t)fq * a.stride + a.off[tk.f];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int wm = wid >> 1, wn = wid & 1;        // warp tile origin (32 x 32 complex)
+  const int g = lane >> 2, t = lane & 3;
+  double dr[4][4][2], di[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) dr[i][j][0] = dr[i][j][1] = di[i][j][0] = di[i][j][1] = 0.0;
+  auto issue = [&](int buf, int kb) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int idx = threadIdx.x + 128 * q;            // 0..511
+      {
+        const int r = idx >> 3, k = idx & 7;            // A: 64 rows x 8
+        const int gr = tk.r0 + r, gk = kb + k;
+        const bool ok = gr < tk.rhi && gk < tk.kk1;
+        cp_async16_cd((uint32_t)__cvta_generic_to_shared(&As[buf][r * kDmmaAS + k]),
+                      ok ? F + (int64_t)gr * ld + gk : F, ok ? 16u : 0u);
+      }
+      {
+        const int k = idx >> 6, c = idx & 63;           // B: 8 rows x 64
+        const int gk = kb + k, gc = tk.c0 + c;
+        const bool ok = gk < tk.kk1 && gc < tk.chi;
+        cp_async16_cd((uint32_t)__cvta_generic_to_shared(&Bs[buf][k * kDmmaBN + c]),
+                      ok ? F + (int64_t)gk * ld + gc : F, ok ? 16u : 0u);
+      }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  const int nk = (tk.kk1 - tk.kk0 + kDmmaBK - 1) / kDmmaBK;
+  issue(0, tk.kk0);
+  for (int kc = 0; kc < nk; ++kc) {
+    const int buf = kc & 1;
+    if (kc + 1 < nk) {
+      issue(buf ^ 1, tk.kk0 + (kc + 1) * kDmmaBK);
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kDmmaBK; kk += 4) {
+      cd av[4], bv[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) av[i] = As[buf][(wm * 32 + i * 8 + g) * kDmmaAS + kk + t];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) bv[j] = Bs[buf][(kk + t) * kDmmaBN + wn * 32 + j * 8 + g];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          dmma(dr[i][j][0], dr[i][j][1], av[i].x, bv[j].x);
+          dmma(dr[i][j][0], dr[i][j][1], -av[i].y, bv[j].y);
+          dmma(di[i][j][0], di[i][j][1], av[i].x, bv[j].y);
+          dmma(di[i][j][0], di[i][j][1], av[i].y, bv[j].x);
+        }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int r = tk.r0 + wm * 32 + i * 8 + g, c = tk.c0 + wn * 32 + j * 8 + 2 * t + e;
+        if (r < tk.rhi && c < tk.chi) {
+          cd &d = F[(int64_t)r * ld + c];
+          d = d - cd{dr[i][j][e], di[i][j][e]};
+        }
+      }
+}
+
 }  // namespace ss
 
 namespace ss {
@@ -967,14 +1065,15 @@ struct Plan {
   std::vector<Graph> graphs;
   std::vector<cudaEvent_t> ev;             // Schur GEMM timing, one pair per level (owned here so
                                            // that captured event-record nodes stay valid)
-  // Schur-tile autotuner (FP64): the second candidate's tasks, per-level pick,
-  // and the measured per-level times of the two candidates on full chunks
+  // Schur-tile autotuner (FP64): candidates 0 SIMT 128x64, 1 SIMT 64x64, 2 DMMA
+  // 64x64 (the 64x64 candidates share the second task list); per-level pick,
+  // decided once per plan by timing every candidate on every level before the
+  // first factorisation, so that every sweep of the plan runs the same tiles
   std::vector<int64_t> schur_ptr_b;
-  std::vector<char> pick;                  // per level: 0 kSquare, 1 kSquare64
+  std::vector<char> pick;                  // per level candidate
   std::vector<int> schur_level;            // level of each Schur launch, in launch order
-  std::vector<float> t_a, t_b;
-  int tune_stage = 2;                      // 0 time A, 1 time B, 2 tuned (or not tuned)
-  int tune_nb = 0;
+  std::vector<float> tune_ms;              // [candidate][level] measured times
+  bool tuned = true;
   ~Plan() {
     for (auto &g : graphs)
       if (g.exec) cudaGraphExecDestroy(g.exec);
@@ -1077,9 +1176,7 @@ Plan *build_plan(Handle &h, int small_m, bool tensor_schur) {
       sb.push_back((int64_t)P->tasks.size());
     }
     P->schur_ptr_b = sb;
-    P->t_a.assign(S.nlevel, 0.f);
-    P->t_b.assign(S.nlevel, 0.f);
-    P->tune_stage = 0;
+    P->tuned = false;
   }
   return P;
 }
@@ -1232,7 +1329,12 @@ struct Sweeper {
   explicit Sweeper(Handle &hh, Plan &pp) : h(hh), P(pp), ev(pp.ev) {
     if (ev.empty()) {
       ev.resize(2 * std::max(1, h.sym.nlevel));
-      for (auto &e : ev) cudaEventCreate(&e);
+      // recorded once outside any capture: the graphs' event-record nodes then
+      // re-record them at every replay and their elapsed times can be read
+      for (auto &e : ev) {
+        cudaEventCreate(&e);
+        cudaEventRecord(e, h.stream);
+      }
     }
   }
 
@@ -1281,8 +1383,11 @@ struct Sweeper {
   }
   // factorisation of a chunk as one graph replay
   int factor_graphed(int nb) {
-    // the tuner stage selects the Schur tiles baked into the graph
-    return graphed(10 * P.tune_stage, nb, {a.arena, a.piv, a.omega, a.Kc, a.Mc, a.Dc, a.nperturb, tc_err},
+    if (sizeof(T) == 8) {
+      const int rc = tune(nb);
+      if (rc) return rc;
+    }
+    return graphed(0, nb, {a.arena, a.piv, a.omega, a.Kc, a.Mc, a.Dc, a.nperturb, tc_err},
                    [&] { return factor(nb); });
   }
   // x <- A'^-1 b (kind 1) or A'^-T b (kind 2) through a graph over fixed staging buffers
@@ -1296,21 +1401,72 @@ struct Sweeper {
     return SS_OK;
   }
   // after the stream reached the end of factor(): add up the Schur GEMM time
-  void collect(int nb) {
-    // the autotuner times candidate A on the first full chunk, B on the second
-    const bool tuning = P.tune_stage < 2 && (P.tune_nb == 0 || P.tune_nb == nb);
+  void collect(int) {
     for (int i = 0; i < nev; ++i) {
       float ms = 0;
       cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]);
       schur_ms += ms;
-      if (tuning) (P.tune_stage == 0 ? P.t_a : P.t_b)[P.schur_level[i]] = ms;
-    }
-    if (tuning) {
-      P.tune_nb = nb;
-      if (++P.tune_stage == 2)
-        for (size_t l = 0; l < P.pick.size(); ++l) P.pick[l] = P.t_b[l] < P.t_a[l];
     }
     nev = 0;
+  }
+
+  // FP64 Schur update of level l with candidate tile c (0 SIMT 128x64, 1 SIMT
+  // 64x64, 2 DMMA 64x64)
+  void schur_launch(const FrontArgs<T> &b, int l, int c, int nb) {
+    const GemmTask *tasks = P.d_tasks.template as<GemmTask>();
+    if (c == 0) {
+      const int64_t t0 = P.schur_ptr[l], t1 = P.schur_ptr[l + 1];
+      front_gemm_kernel<T, kSquare><<<dim3((unsigned)(t1 - t0), nb), 256, 0, h.stream>>>(b, tasks + t0);
+      return;
+    }
+    const int64_t t0 = P.schur_ptr_b[l], t1 = P.schur_ptr_b[l + 1];
+    if (c == 1)
+      front_gemm_kernel<T, kSquare64><<<dim3((unsigned)(t1 - t0), nb), 256, 0, h.stream>>>(b, tasks + t0);
+    else if constexpr (sizeof(T) == 8)
+      front_dmma_kernel<<<dim3((unsigned)(t1 - t0), nb), 128, 0, h.stream>>>(b, tasks + t0);
+  }
+
+  // Autotuner: time every candidate on every level with Schur work, on the chunk's
+  // arena before its first factorisation (GEMM time does not depend on the
+  // values), and keep the fastest per level.  SS_SCHUR_TILE=0|1|2 forces one.
+  int tune(int nb) {
+    if (P.tuned) return SS_OK;
+    const Symbolic &S = h.sym;
+    const char *force = getenv("SS_SCHUR_TILE");
+    constexpr int NC = 3;
+    P.tune_ms.assign((size_t)NC * S.nlevel, 0.f);
+    if (!force) {
+      std::vector<cudaEvent_t> e(2 * NC * S.nlevel);
+      for (auto &x : e) SS_CK(cudaEventCreate(&x));
+      for (int c = 0; c < NC; ++c)
+        for (int l = 0; l < S.nlevel; ++l) {
+          if (P.schur_ptr[l + 1] == P.schur_ptr[l]) continue;
+          FrontArgs<T> b = a;
+          cudaEventRecord(e[2 * (c * S.nlevel + l)], h.stream);
+          schur_launch(b, l, c, nb);
+          cudaEventRecord(e[2 * (c * S.nlevel + l) + 1], h.stream);
+        }
+      SS_CK(cudaGetLastError());
+      SS_CK(cudaStreamSynchronize(h.stream));
+      for (int c = 0; c < NC; ++c)
+        for (int l = 0; l < S.nlevel; ++l) {
+          if (P.schur_ptr[l + 1] == P.schur_ptr[l]) continue;
+          cudaEventElapsedTime(&P.tune_ms[c * S.nlevel + l], e[2 * (c * S.nlevel + l)], e[2 * (c * S.nlevel + l) + 1]);
+        }
+      for (auto &x : e) cudaEventDestroy(x);
+    }
+    for (int l = 0; l < S.nlevel; ++l) {
+      int best = 0;
+      if (force) {
+        best = std::max(0, std::min(NC - 1, atoi(force)));
+      } else {
+        for (int c = 1; c < NC; ++c)
+          if (P.tune_ms[c * S.nlevel + l] < P.tune_ms[best * S.nlevel + l]) best = c;
+      }
+      P.pick[l] = (char)best;
+    }
+    P.tuned = true;
+    return SS_OK;
   }
 
   int factor(int nb) {
@@ -1354,15 +1510,11 @@ struct Sweeper {
       const int64_t t0 = P.schur_ptr[l], t1 = P.schur_ptr[l + 1];
       if (t1 > t0) {
         cudaEventRecordWithFlags(ev[2 * nev], h.stream, cudaEventRecordExternal);
-        const bool use_b = sizeof(T) == 8 && (P.tune_stage == 1 || (P.tune_stage == 2 && P.pick[l]));
         if (sizeof(T) == 4)
           tc::front_tc_gemm_kernel<<<dim3((unsigned)(t1 - t0), nb), tc::THREADS, tc::SMEM_BYTES, h.stream>>>(
               reinterpret_cast<cf *>(b.arena), b.stride, b.off, b.ld, tasks + t0, tc_err);
-        else if (use_b)
-          front_gemm_kernel<T, kSquare64><<<dim3((unsigned)(P.schur_ptr_b[l + 1] - P.schur_ptr_b[l]), nb), 256, 0,
-                                            h.stream>>>(b, tasks + P.schur_ptr_b[l]);
         else
-          front_gemm_kernel<T, kSquare><<<dim3((unsigned)(t1 - t0), nb), 256, 0, h.stream>>>(b, tasks + t0);
+          schur_launch(b, l, P.pick[l], nb);
         if ((int)P.schur_level.size() <= nev) P.schur_level.push_back(l);
         cudaEventRecordWithFlags(ev[2 * nev + 1], h.stream, cudaEventRecordExternal);
         ++nev;
@@ -1764,6 +1916,9 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
   h.st[17] = total_ms;
   h.st[14] = perturbed;
   h.st[15] = sw.launches;
+  h.st[20] = h.st[21] = h.st[22] = 0;
+  for (size_t l = 0; l < P.pick.size(); ++l)
+    if (P.schur_ptr[l + 1] > P.schur_ptr[l]) h.st[20 + P.pick[l]] += 1;
   {
     double tot = 0;
     if (iters)

@@ -160,7 +160,8 @@ class FrequencySolver:
         keys = ['n_active', 'n_fronts', 'max_front', 'factor_flops_per_point', 'nnz_lu', 'analyze_s',
                 'assemble_ms', 'sweep_ms', 'factor_ms', 'solve_ms', 'chunk', 'schur_gemm_ms',
                 'schur_gemm_flops', 'levels', 'perturbed_pivots', 'launches', 'schur_launches',
-                'sweep_device_ms', 'refine_solves', 'precision_used']
+                'sweep_device_ms', 'refine_solves', 'precision_used', 'schur_tile_simt128', 'schur_tile_simt64',
+                'schur_tile_dmma']
         return dict(zip(keys, out.tolist()))
 
     @property

@@ -65,3 +65,23 @@ def test_mixed_matches_fp64(mid):
     d = compare(resonances(f, Y64), resonances(f, Y32))
     for key in ('fr_diff_mhz', 'fa_diff_mhz'):
         assert d[key] is None or abs(d[key]) <= 1e-3
+
+
+@pytest.mark.parametrize('tile', [1, 2])
+def test_every_schur_tile_candidate_is_exact(mid, tile, monkeypatch):
+    """The autotuner's candidates (SIMT 128x64 / 64x64, FP64 tensor-core DMMA 64x64),
+    each forced on every level, give the same charges as the default choice."""
+    case, _, g = mid
+    f = np.linspace(case.freqs[0], case.freqs[-1], 5)
+    Q0, _, _ = g.charges(2 * np.pi * f, 1.0, 'fp64')
+    monkeypatch.setenv('SS_SCHUR_TILE', str(tile))
+    e = cases.engine_for(case)
+    try:
+        Q, st, _ = e.charges(2 * np.pi * f, 1.0, 'fp64')
+        s = e.stats()
+    finally:
+        e.close()
+    assert (st == 0).all()
+    counts = [s['schur_tile_simt128'], s['schur_tile_simt64'], s['schur_tile_dmma']]
+    assert counts[tile] > 0 and sum(counts) == counts[tile]
+    assert np.max(np.abs(Q - Q0) / np.abs(Q0)) < 1e-9
