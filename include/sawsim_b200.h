@@ -186,7 +186,8 @@ int ss_adjoint_gradient(ss_handle *h, int n_f, const double *omega, double V, in
  *  18 refinement / Krylov steps of the last ss_sweep (sum over points),
  *  19 precision the last ss_sweep ran in (SS_PREC_FP64 or SS_PREC_MIXED),
  *  20-22 levels whose Schur update uses the autotuner's candidate 0 (SIMT
- *  128x64), 1 (SIMT 64x64), 2 (FP64 tensor-core DMMA 64x64).
+ *  128x64), 1 (SIMT 64x64), 2 (FP64 tensor-core DMMA 64x64),
+ *  23 1 if the panel-step GEMMs use DMMA tiles (128x32 / 32x128), else 0.
  */
 int ss_stats(const ss_handle *h, double *out, int n);
 

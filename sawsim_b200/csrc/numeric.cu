@@ -537,12 +537,14 @@ __global__ void __launch_bounds__(256) front_gemm_kernel(FrontArgs<T> a, const G
 }
 
 // FP64 complex tile C -= A B on the FP64 tensor cores (DMMA, mma.sync m8n8k4 f64):
-// 64x64 complex outputs per 128-thread CTA, a 32x32 complex warp tile (4x4 blocks
-// of 8x8), K in chunks of 8 complex staged by cp.async (double-buffered).  Each
+// 4 warps in a WM x WN grid, each a 32x32 complex warp tile (4x4 blocks of 8x8), so
+// (32 WM) x (32 WN) complex outputs per 128-thread CTA (64x64 Schur tiles, 128x32
+// panel-column tiles, 32x128 U-row tiles); K in chunks of 8 complex staged by
+// cp.async (double-buffered).  Each
 // 8x8x4 complex block is four real MMAs: Dr += Ar Br - Ai Bi, Di += Ar Bi + Ai Br.
 // Fragments (PTX m8n8k4 .f64): A[g][t], B[t][g], C[g][2t + i] with g = lane / 4,
 // t = lane % 4.
-constexpr int kDmmaBM = 64, kDmmaBN = 64, kDmmaBK = 8;
+constexpr int kDmmaBK = 8;
 constexpr int kDmmaAS = kDmmaBK + 1;          // A row stride in complex (+1: conflict-free fragment reads)
 
 __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
@@ -554,7 +556,10 @@ __device__ __forceinline__ void cp_async16_cd(uint32_t dst, const void *src, uin
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
 }
 
+template <int WM, int WN>
 __global__ void __launch_bounds__(128) front_dmma_kernel(FrontArgs<double> a, const GemmTask *__restrict__ tasks) {
+  constexpr int kDmmaBM = 32 * WM, kDmmaBN = 32 * WN;
+  static_assert(WM * WN == 4, "four warps");
   __shared__ __align__(16) cd As[2][kDmmaBM * kDmmaAS];
   __shared__ __align__(16) cd Bs[2][kDmmaBK * kDmmaBN];
   const GemmTask tk = tasks[blockIdx.x];
@@ -562,7 +567,7 @@ __global__ void __launch_bounds__(128) front_dmma_kernel(FrontArgs<double> a, co
   const int ld = a.ld[tk.f];
   cd *F = a.arena + (int64_t)fq * a.stride + a.off[tk.f];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int wm = wid >> 1, wn = wid & 1;        // warp tile origin (32 x 32 complex)
+  const int wm = wid / WN, wn = wid % WN;       // warp tile origin (32 x 32 complex)
   const int g = lane >> 2, t = lane & 3;
   double dr[4][4][2], di[4][4][2];
 #pragma unroll
@@ -571,22 +576,22 @@ __global__ void __launch_bounds__(128) front_dmma_kernel(FrontArgs<double> a, co
     for (int j = 0; j < 4; ++j) dr[i][j][0] = dr[i][j][1] = di[i][j][0] = di[i][j][1] = 0.0;
   auto issue = [&](int buf, int kb) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int idx = threadIdx.x + 128 * q;            // 0..511
-      {
-        const int r = idx >> 3, k = idx & 7;            // A: 64 rows x 8
-        const int gr = tk.r0 + r, gk = kb + k;
-        const bool ok = gr < tk.rhi && gk < tk.kk1;
-        cp_async16_cd((uint32_t)__cvta_generic_to_shared(&As[buf][r * kDmmaAS + k]),
-                      ok ? F + (int64_t)gr * ld + gk : F, ok ? 16u : 0u);
-      }
-      {
-        const int k = idx >> 6, c = idx & 63;           // B: 8 rows x 64
-        const int gk = kb + k, gc = tk.c0 + c;
-        const bool ok = gk < tk.kk1 && gc < tk.chi;
-        cp_async16_cd((uint32_t)__cvta_generic_to_shared(&Bs[buf][k * kDmmaBN + c]),
-                      ok ? F + (int64_t)gk * ld + gc : F, ok ? 16u : 0u);
-      }
+    for (int q = 0; q < kDmmaBM * kDmmaBK / 128; ++q) {
+      const int idx = threadIdx.x + 128 * q;
+      const int r = idx / kDmmaBK, k = idx % kDmmaBK;   // A: BM rows x 8
+      const int gr = tk.r0 + r, gk = kb + k;
+      const bool ok = gr < tk.rhi && gk < tk.kk1;
+      cp_async16_cd((uint32_t)__cvta_generic_to_shared(&As[buf][r * kDmmaAS + k]),
+                    ok ? F + (int64_t)gr * ld + gk : F, ok ? 16u : 0u);
+    }
+#pragma unroll
+    for (int q = 0; q < kDmmaBK * kDmmaBN / 128; ++q) {
+      const int idx = threadIdx.x + 128 * q;
+      const int k = idx / kDmmaBN, c = idx % kDmmaBN;   // B: 8 rows x BN
+      const int gk = kb + k, gc = tk.c0 + c;
+      const bool ok = gk < tk.kk1 && gc < tk.chi;
+      cp_async16_cd((uint32_t)__cvta_generic_to_shared(&Bs[buf][k * kDmmaBN + c]),
+                    ok ? F + (int64_t)gk * ld + gc : F, ok ? 16u : 0u);
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
@@ -1060,7 +1065,7 @@ struct Plan {
     int nb;
     const void *key[8];
     cudaGraphExec_t exec = nullptr;
-    int launches = 0, schur_launches = 0, nev = 0;
+    int launches = 0, schur_launches = 0;
   };
   std::vector<Graph> graphs;
   std::vector<cudaEvent_t> ev;             // Schur GEMM timing, one pair per level (owned here so
@@ -1070,8 +1075,10 @@ struct Plan {
   // decided once per plan by timing every candidate on every level before the
   // first factorisation, so that every sweep of the plan runs the same tiles
   std::vector<int64_t> schur_ptr_b;
+  std::vector<int64_t> step_ptr_d;         // panel-step tasks in DMMA tiles (same indexing as step_ptr)
+  bool panel_dmma = false;                 // panel-step GEMMs on DMMA (tuned once per plan)
+  float panel_ms[2] = {0, 0};              // tuner's panel-GEMM times: SIMT, DMMA
   std::vector<char> pick;                  // per level candidate
-  std::vector<int> schur_level;            // level of each Schur launch, in launch order
   std::vector<float> tune_ms;              // [candidate][level] measured times
   bool tuned = true;
   ~Plan() {
@@ -1176,6 +1183,27 @@ Plan *build_plan(Handle &h, int small_m, bool tensor_schur) {
       sb.push_back((int64_t)P->tasks.size());
     }
     P->schur_ptr_b = sb;
+    // panel-step GEMMs in DMMA tiles: 128x32 for the panel columns, 32x128 for the
+    // U rows, in the (level, step) order of step_ptr
+    P->step_ptr_d.assign(1, (int64_t)P->tasks.size());
+    for (int l = 0; l < S.nlevel; ++l) {
+      for (int st = 0; st < P->nsteps[l]; ++st) {
+        const int j0 = st * kPanel;
+        for (int q = P->large_ptr[l]; q < P->large_ptr[l + 1]; ++q) {
+          const int f = P->fronts_large[q], k = S.k[f], m = S.m[f];
+          if (j0 >= k || j0 == 0) continue;
+          add_tiles(P->tasks, 128, 32, f, j0, m, j0, std::min(k, j0 + kPanel), 0, j0);
+        }
+        P->step_ptr_d.push_back((int64_t)P->tasks.size());
+        for (int q = P->large_ptr[l]; q < P->large_ptr[l + 1]; ++q) {
+          const int f = P->fronts_large[q], k = S.k[f], m = S.m[f];
+          if (j0 >= k || j0 == 0) continue;
+          const int j1 = std::min(k, j0 + kPanel);
+          if (j1 < m) add_tiles(P->tasks, 32, 128, f, j0, j1, j1, m, 0, j0);
+        }
+        P->step_ptr_d.push_back((int64_t)P->tasks.size());
+      }
+    }
     P->tuned = false;
   }
   return P;
@@ -1353,11 +1381,9 @@ struct Sweeper {
       SS_CK(cudaGraphLaunch(g.exec, h.stream));
       launches += g.launches;
       schur_launches += g.schur_launches;
-      nev = g.nev;
       return SS_OK;
     }
     const int l0 = launches, s0 = schur_launches;
-    nev = 0;
     cudaGraph_t graph = nullptr;
     SS_CK(cudaStreamBeginCapture(h.stream, cudaStreamCaptureModeThreadLocal));
     const int rc = body();
@@ -1376,7 +1402,6 @@ struct Sweeper {
     SS_CK(ie);
     g.launches = launches - l0;
     g.schur_launches = schur_launches - s0;
-    g.nev = nev;
     P.graphs.push_back(g);
     SS_CK(cudaGraphLaunch(g.exec, h.stream));
     return SS_OK;
@@ -1387,8 +1412,17 @@ struct Sweeper {
       const int rc = tune(nb);
       if (rc) return rc;
     }
-    return graphed(0, nb, {a.arena, a.piv, a.omega, a.Kc, a.Mc, a.Dc, a.nperturb, tc_err},
-                   [&] { return factor(nb); });
+    // every level's launch chain is one graph replay; the Schur update between
+    // levels is a direct, event-timed launch (timed kernel time of the dominant GEMM)
+    nev = 0;
+    for (int l = 0; l < h.sym.nlevel; ++l) {
+      int rc = graphed(100 + l, nb, {a.arena, a.piv, a.omega, a.Kc, a.Mc, a.Dc, a.nperturb, tc_err},
+                       [&] { return factor_level(l, nb); });
+      if (rc) return rc;
+      rc = schur_level(l, nb);
+      if (rc) return rc;
+    }
+    return SS_OK;
   }
   // x <- A'^-1 b (kind 1) or A'^-T b (kind 2) through a graph over fixed staging buffers
   int solve_graphed(int kind, int nb, const cd *b, cd *x) {
@@ -1410,6 +1444,29 @@ struct Sweeper {
     nev = 0;
   }
 
+  // panel-step GEMM of (level, step) slot q: which 0 = panel columns (skinny),
+  // 1 = U rows (short); SIMT tiles, or DMMA tiles when the tuner chose them
+  void panel_gemm(const FrontArgs<T> &b, int64_t q, int which, int nb) {
+    const GemmTask *tasks = P.d_tasks.template as<GemmTask>();
+    if constexpr (sizeof(T) == 8) {
+      if (P.panel_dmma) {
+        const int64_t t0 = P.step_ptr_d[q + which], t1 = P.step_ptr_d[q + which + 1];
+        if (t1 == t0) return;
+        if (which == 0)
+          front_dmma_kernel<4, 1><<<dim3((unsigned)(t1 - t0), nb), 128, 0, h.stream>>>(b, tasks + t0);
+        else
+          front_dmma_kernel<1, 4><<<dim3((unsigned)(t1 - t0), nb), 128, 0, h.stream>>>(b, tasks + t0);
+        return;
+      }
+    }
+    const int64_t t0 = P.step_ptr[q + which], t1 = P.step_ptr[q + which + 1];
+    if (t1 == t0) return;
+    if (which == 0)
+      front_gemm_kernel<T, kSkinny><<<dim3((unsigned)(t1 - t0), nb), 256, 0, h.stream>>>(b, tasks + t0);
+    else
+      front_gemm_kernel<T, kShort><<<dim3((unsigned)(t1 - t0), nb), 256, 0, h.stream>>>(b, tasks + t0);
+  }
+
   // FP64 Schur update of level l with candidate tile c (0 SIMT 128x64, 1 SIMT
   // 64x64, 2 DMMA 64x64)
   void schur_launch(const FrontArgs<T> &b, int l, int c, int nb) {
@@ -1423,7 +1480,7 @@ struct Sweeper {
     if (c == 1)
       front_gemm_kernel<T, kSquare64><<<dim3((unsigned)(t1 - t0), nb), 256, 0, h.stream>>>(b, tasks + t0);
     else if constexpr (sizeof(T) == 8)
-      front_dmma_kernel<<<dim3((unsigned)(t1 - t0), nb), 128, 0, h.stream>>>(b, tasks + t0);
+      front_dmma_kernel<2, 2><<<dim3((unsigned)(t1 - t0), nb), 128, 0, h.stream>>>(b, tasks + t0);
   }
 
   // Autotuner: time every candidate on every level with Schur work, on the chunk's
@@ -1454,6 +1511,33 @@ struct Sweeper {
           cudaEventElapsedTime(&P.tune_ms[c * S.nlevel + l], e[2 * (c * S.nlevel + l)], e[2 * (c * S.nlevel + l) + 1]);
         }
       for (auto &x : e) cudaEventDestroy(x);
+      // panel-step GEMMs: all of them once with SIMT tiles, once with DMMA tiles
+      cudaEvent_t pe[4];
+      for (auto &x : pe) SS_CK(cudaEventCreate(&x));
+      float pt[2] = {0, 0};
+      for (int c = 0; c < 2; ++c) {
+        P.panel_dmma = c == 1;
+        cudaEventRecord(pe[2 * c], h.stream);
+        for (int l = 0; l < S.nlevel; ++l) {
+          FrontArgs<T> b = a;
+          b.fronts = P.d_large.as<int>() + P.large_ptr[l];
+          for (int st = 0; st < P.nsteps[l]; ++st) {
+            const int64_t q = P.level_step0[l] + 2 * st;
+            panel_gemm(b, q, 0, nb);
+            panel_gemm(b, q, 1, nb);
+          }
+        }
+        cudaEventRecord(pe[2 * c + 1], h.stream);
+      }
+      SS_CK(cudaGetLastError());
+      SS_CK(cudaStreamSynchronize(h.stream));
+      for (int c = 0; c < 2; ++c) cudaEventElapsedTime(&pt[c], pe[2 * c], pe[2 * c + 1]);
+      for (auto &x : pe) cudaEventDestroy(x);
+      P.panel_dmma = pt[1] < pt[0];
+      P.panel_ms[0] = pt[0];
+      P.panel_ms[1] = pt[1];
+    } else {
+      P.panel_dmma = atoi(force) == 2;
     }
     for (int l = 0; l < S.nlevel; ++l) {
       int best = 0;
@@ -1469,9 +1553,10 @@ struct Sweeper {
     return SS_OK;
   }
 
-  int factor(int nb) {
-    const Symbolic &S = h.sym;
-    for (int l = 0; l < S.nlevel; ++l) {
+  // level l of the factorisation up to (not including) its Schur update: small
+  // fronts, large-front assembly and the panel steps
+  int factor_level(int l, int nb) {
+    {
       const int ns = P.small_ptr[l + 1] - P.small_ptr[l];
       if (ns) {
         FrontArgs<T> b = a;
@@ -1481,7 +1566,7 @@ struct Sweeper {
         ++launches;
       }
       const int nl = P.large_ptr[l + 1] - P.large_ptr[l];
-      if (!nl) continue;
+      if (!nl) return SS_OK;
       FrontArgs<T> b = a;
       b.fronts = P.d_large.as<int>() + P.large_ptr[l];
       const int ml = P.maxm_large[l];
@@ -1494,34 +1579,42 @@ struct Sweeper {
         const int64_t q = P.level_step0[l] + 2 * s;
         const int64_t g0 = P.step_ptr[q], g1 = P.step_ptr[q + 1], g2 = P.step_ptr[q + 2];
         if (g1 > g0) {   // panel columns <- earlier pivots
-          front_gemm_kernel<T, kSkinny><<<dim3((unsigned)(g1 - g0), nb), 256, 0, h.stream>>>(b, tasks + g0);
+          panel_gemm(b, q, 0, nb);
           ++launches;
         }
         front_panel_kernel<T><<<dim3(nl, nb), 256, 0, h.stream>>>(b, j0);
         front_l21_kernel<T><<<dim3(nl, nb, zc), 256, 0, h.stream>>>(b, j0);
         front_swap_trsm_kernel<T><<<dim3(nl, nb, zc), 256, 0, h.stream>>>(b, j0, 0);
         if (g2 > g1) {   // U row block <- earlier pivots
-          front_gemm_kernel<T, kShort><<<dim3((unsigned)(g2 - g1), nb), 256, 0, h.stream>>>(b, tasks + g1);
+          panel_gemm(b, q, 1, nb);
           ++launches;
         }
         front_swap_trsm_kernel<T><<<dim3(nl, nb, zc), 256, 0, h.stream>>>(b, j0, 1);
         launches += 4;
       }
-      const int64_t t0 = P.schur_ptr[l], t1 = P.schur_ptr[l + 1];
-      if (t1 > t0) {
-        cudaEventRecordWithFlags(ev[2 * nev], h.stream, cudaEventRecordExternal);
-        if (sizeof(T) == 4)
-          tc::front_tc_gemm_kernel<<<dim3((unsigned)(t1 - t0), nb), tc::THREADS, tc::SMEM_BYTES, h.stream>>>(
-              reinterpret_cast<cf *>(b.arena), b.stride, b.off, b.ld, tasks + t0, tc_err);
-        else
-          schur_launch(b, l, P.pick[l], nb);
-        if ((int)P.schur_level.size() <= nev) P.schur_level.push_back(l);
-        cudaEventRecordWithFlags(ev[2 * nev + 1], h.stream, cudaEventRecordExternal);
-        ++nev;
-        ++launches;
-        ++schur_launches;
-      }
     }
+    SS_CK(cudaGetLastError());
+    return SS_OK;
+  }
+
+  // Schur update of level l's large fronts, launched directly and timed by a pair
+  // of events on the launch stream
+  int schur_level(int l, int nb) {
+    const int64_t t0 = P.schur_ptr[l], t1 = P.schur_ptr[l + 1];
+    if (t1 == t0) return SS_OK;
+    FrontArgs<T> b = a;
+    b.fronts = P.d_large.as<int>() + P.large_ptr[l];
+    const GemmTask *tasks = P.d_tasks.as<GemmTask>();
+    cudaEventRecord(ev[2 * nev], h.stream);
+    if (sizeof(T) == 4)
+      tc::front_tc_gemm_kernel<<<dim3((unsigned)(t1 - t0), nb), tc::THREADS, tc::SMEM_BYTES, h.stream>>>(
+          reinterpret_cast<cf *>(b.arena), b.stride, b.off, b.ld, tasks + t0, tc_err);
+    else
+      schur_launch(b, l, P.pick[l], nb);
+    cudaEventRecord(ev[2 * nev + 1], h.stream);
+    ++nev;
+    ++launches;
+    ++schur_launches;
     SS_CK(cudaGetLastError());
     return SS_OK;
   }
@@ -1917,6 +2010,7 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
   h.st[14] = perturbed;
   h.st[15] = sw.launches;
   h.st[20] = h.st[21] = h.st[22] = 0;
+  h.st[23] = P.panel_dmma ? 1.0 : 0.0;
   for (size_t l = 0; l < P.pick.size(); ++l)
     if (P.schur_ptr[l + 1] > P.schur_ptr[l]) h.st[20 + P.pick[l]] += 1;
   {

@@ -161,7 +161,7 @@ class FrequencySolver:
                 'assemble_ms', 'sweep_ms', 'factor_ms', 'solve_ms', 'chunk', 'schur_gemm_ms',
                 'schur_gemm_flops', 'levels', 'perturbed_pivots', 'launches', 'schur_launches',
                 'sweep_device_ms', 'refine_solves', 'precision_used', 'schur_tile_simt128', 'schur_tile_simt64',
-                'schur_tile_dmma']
+                'schur_tile_dmma', 'panel_gemm_dmma']
         return dict(zip(keys, out.tolist()))
 
     @property

@@ -69,8 +69,9 @@ def test_mixed_matches_fp64(mid):
 
 @pytest.mark.parametrize('tile', [1, 2])
 def test_every_schur_tile_candidate_is_exact(mid, tile, monkeypatch):
-    """The autotuner's candidates (SIMT 128x64 / 64x64, FP64 tensor-core DMMA 64x64),
-    each forced on every level, give the same charges as the default choice."""
+    """The autotuner's candidates (SIMT 128x64 / 64x64, FP64 tensor-core DMMA 64x64;
+    SS_SCHUR_TILE=2 also puts the panel-step GEMMs on DMMA tiles), each forced on
+    every level, give the same charges as the default choice."""
     case, _, g = mid
     f = np.linspace(case.freqs[0], case.freqs[-1], 5)
     Q0, _, _ = g.charges(2 * np.pi * f, 1.0, 'fp64')
@@ -84,4 +85,5 @@ def test_every_schur_tile_candidate_is_exact(mid, tile, monkeypatch):
     assert (st == 0).all()
     counts = [s['schur_tile_simt128'], s['schur_tile_simt64'], s['schur_tile_dmma']]
     assert counts[tile] > 0 and sum(counts) == counts[tile]
+    assert s['panel_gemm_dmma'] == (1.0 if tile == 2 else 0.0)
     assert np.max(np.abs(Q - Q0) / np.abs(Q0)) < 1e-9
