@@ -219,19 +219,26 @@ class HexCase:
 
 
 HEX_CASES = {
-    # name: (nx, ny, nz, f0, f1, npoints)
-    'hex_8x4x48': (8, 4, 48, 1.6e9, 2.0e9, 101),
+    # name: (cell builder, nx, ny, nz, f0, f1, npoints)
+    'hex_8x4x48': ('double', 8, 4, 48, 1.6e9, 2.0e9, 101),
+    'hex_12x6x80': ('four', 12, 6, 80, 1.5e9, 2.1e9, 401),
 }
 
 
 def make_hex_case(name: str, seed: int = 0, nx=None, ny=None, nz=None, points=None) -> HexCase:
-    """Seeded synthetic double-layer Hex27 slab (see ``cells.hex_double_layer_slab``):
-    rotated 3m film, Al electrodes, SiO2 layer and SiO2 PML (z-stretch, frozen at
-    the top frequency, dmax 1e11, n 3, as src/sawsim/hex_models.py:75-77)."""
-    x0, y0, z0, fa, fb, npt = HEX_CASES[name]
-    cell = cells.hex_double_layer_slab(nx or x0, ny or y0, nz or z0)
+    """Seeded synthetic Hex27 slab: ``hex_8x4x48`` the double layer of
+    ``cells.hex_double_layer_slab`` (film / SiO2 / SiO2 PML), ``hex_12x6x80`` the four
+    layers of ``cells.hex_four_layer_slab`` (film / SiO2 / poly-Si / Si / Si PML); Al
+    electrodes; bottom PML z-stretch frozen at the top frequency, dmax 1e11, n 3, as
+    src/sawsim/hex_models.py:75-77."""
+    kind, x0, y0, z0, fa, fb, npt = HEX_CASES[name]
     piezo, euler = _crystal(seed)
-    mats = [piezo, mt.al(), mt.sio2()]
+    if kind == 'double':
+        cell = cells.hex_double_layer_slab(nx or x0, ny or y0, nz or z0)
+        mats = [piezo, mt.al(), mt.sio2()]
+    else:
+        cell = cells.hex_four_layer_slab(nx or x0, ny or y0, nz or z0)
+        mats = [piezo, mt.al(), mt.sio2(), mt.poly_si(), mt.si_cubic()]
     idx = np.array([cell.tag_map[int(t)] for t in cell.hex_tag], dtype=np.int64)
     pos_m = cell.POS * 1e-6
     bottom = float(pos_m[:, 2].min())

@@ -400,3 +400,18 @@ def hex_double_layer_slab(nx: int = 8, ny: int = 4, nz: int = 48, pitch_um: floa
     r_pml = nz - r_film - r_ox
     return hex_slab_cell(p, nx, ny, [Band(HEX_TAG_PIEZO, 0.6 * p, r_film), Band(HEX_TAG_LAYER, 1.4 * p, r_ox),
                                      Band(10, 2 * p, r_pml)], Band(HEX_TAG_ELECTRODE, 0.08 * p, 1), 0.5 * p)
+
+
+def hex_four_layer_slab(nx: int = 12, ny: int = 6, nz: int = 80, pitch_um: float = 1.085) -> HexCell:
+    """Four-layer Hex27 slab: 3m film 0.5p / SiO2 0.25p / poly-Si 0.5p / Si 1.75p / Si PML 1p
+    (z), aperture 0.5p, Al electrodes 0.08p (one layer) of width p/3 (metal ratio 1/3, so
+    that their edges fall on the p/6 cells of nx = 12).  ``nz`` layers split
+    1/8, 1/16, 1/8, 7/16, 1/4 (10/5/10/35/20 at 80).  Material order: 0 piezo, 1 Al,
+    2 SiO2, 3 poly-Si, 4 Si."""
+    p = pitch_um
+    r = [nz // 8, nz // 16, nz // 8]
+    r_pml = nz // 4
+    r_si = nz - sum(r) - r_pml
+    return hex_slab_cell(p, nx, ny, [Band(HEX_TAG_PIEZO, 0.5 * p, r[0]), Band(HEX_TAG_LAYER, 0.25 * p, r[1]),
+                                     Band(11, 0.5 * p, r[2]), Band(12, 1.75 * p, r_si), Band(13, p, r_pml)],
+                         Band(HEX_TAG_ELECTRODE, 0.08 * p, 1), 0.5 * p, metal_ratio=1.0 / 3.0)

@@ -323,12 +323,15 @@ __global__ void __launch_bounds__(256) front_assemble_large_kernel(FrontArgs<T> 
 template <class T>
 __global__ void __launch_bounds__(256) front_l21_kernel(FrontArgs<T> a, int j0) {
   __shared__ cplx<T> U[kPanel][kPanel];
+  __shared__ cplx<T> Uinv[kPanel];          // reciprocals of the diagonal, once per CTA
   const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
   const int k = a.k[f], m = a.m[f], ld = a.ld[f];
   if (j0 >= k) return;
   const int j1 = min(k, j0 + kPanel), w = j1 - j0;
   const cplx<T> *Fc = a.arena + (int64_t)fq * a.stride + a.off[f];
   for (int t = threadIdx.x; t < w * w; t += blockDim.x) U[t / w][t % w] = Fc[(int64_t)(j0 + t / w) * ld + j0 + t % w];
+  __syncthreads();
+  if (threadIdx.x < w) Uinv[threadIdx.x] = cdiv(cplx<T>{1, 0}, U[threadIdx.x][threadIdx.x]);
   __syncthreads();
   const int r = k + blockIdx.z * blockDim.x + threadIdx.x;
   if (r >= m) return;
@@ -343,7 +346,7 @@ __global__ void __launch_bounds__(256) front_l21_kernel(FrontArgs<T> a, int j0) 
     cplx<T> v = x[c];
 #pragma unroll
     for (int t = 0; t < c; ++t) v = cfms(v, x[t], U[t][c]);
-    x[c] = cdiv(v, U[c][c]);
+    x[c] = cmul(v, Uinv[c]);
   }
 #pragma unroll
   for (int c = 0; c < kPanel; ++c)

@@ -78,3 +78,21 @@ def test_solver_matches_reference(slab):
     # reference's own K and M, the oracle's solve reproduces its Q exactly.
     Q = eng.sweep(g['frequency_hz'])
     assert np.max(np.abs(Q - g['Q']) / np.abs(g['Q'])) < 2e-5
+
+
+def test_four_layer_slab_pairs_match_coordinates():
+    """The four-layer slab's front/back and left/right pairs sit at equal (x, z) /
+    (y, z) and one aperture / one period apart (the checks of hex_models.py:34-45)."""
+    c = cases.make_hex_case('hex_12x6x80', nx=12, ny=2, nz=16)
+    fix, zheng, fu, groups, two = c.bc
+    N = c.N
+    node = lambda d: d // 3 if d < 3 * N else d - 3 * N          # noqa: E731
+    g = np.array(groups)
+    m = np.array([node(d) for d in g[:, 0]])
+    s = np.array([node(d) for d in g[:, 1]])
+    P = c.pos_m
+    fb, lr = slice(0, two), slice(two, None)
+    assert np.allclose(P[m[fb]][:, [0, 2]], P[s[fb]][:, [0, 2]], atol=1e-13)
+    assert np.allclose(P[s[fb], 1] - P[m[fb], 1], c.cell.aperture_um * 1e-6, atol=1e-13)
+    assert np.allclose(P[m[lr]][:, [1, 2]], P[s[lr]][:, [1, 2]], atol=1e-13)
+    assert np.allclose(P[s[lr], 0] - P[m[lr], 0], c.cell.period_um * 1e-6, atol=1e-13)
