@@ -1176,6 +1176,7 @@ Plan *build_plan(Handle &h, int small_m, bool tensor_schur) {
   }
   P->schur_ptr = sp;
   P->pick.assign(S.nlevel, 0);
+  P->tuned = false;
   if (!tensor_schur) {
     std::vector<int64_t> sb(1, (int64_t)P->tasks.size());
     for (int l = 0; l < S.nlevel; ++l) {
@@ -1411,7 +1412,7 @@ struct Sweeper {
   }
   // factorisation of a chunk as one graph replay
   int factor_graphed(int nb) {
-    if (sizeof(T) == 8) {
+    {
       const int rc = tune(nb);
       if (rc) return rc;
     }
@@ -1474,6 +1475,20 @@ struct Sweeper {
   // 64x64, 2 DMMA 64x64)
   void schur_launch(const FrontArgs<T> &b, int l, int c, int nb) {
     const GemmTask *tasks = P.d_tasks.template as<GemmTask>();
+    if constexpr (sizeof(T) == 4) {
+      // complex64: candidate 0 one CTA per tile, 1 persistent warp-specialised CTAs
+      const int64_t t0 = P.schur_ptr[l], t1 = P.schur_ptr[l + 1];
+      if (c == 0) {
+        tc::front_tc_gemm_kernel<<<dim3((unsigned)(t1 - t0), nb), tc::THREADS, tc::SMEM_BYTES, h.stream>>>(
+            reinterpret_cast<cf *>(b.arena), b.stride, b.off, b.ld, tasks + t0, tc_err);
+      } else {
+        const int64_t items = (t1 - t0) * nb;
+        const unsigned grid = (unsigned)std::min<int64_t>(items, h.num_sms);
+        tc::front_tc_gemm_persistent<<<grid, tc::P_THREADS, tc::SMEM_BYTES, h.stream>>>(
+            reinterpret_cast<cf *>(b.arena), b.stride, b.off, b.ld, tasks + t0, (int)(t1 - t0), nb, tc_err);
+      }
+      return;
+    }
     if (c == 0) {
       const int64_t t0 = P.schur_ptr[l], t1 = P.schur_ptr[l + 1];
       front_gemm_kernel<T, kSquare><<<dim3((unsigned)(t1 - t0), nb), 256, 0, h.stream>>>(b, tasks + t0);
@@ -1492,8 +1507,8 @@ struct Sweeper {
   int tune(int nb) {
     if (P.tuned) return SS_OK;
     const Symbolic &S = h.sym;
-    const char *force = getenv("SS_SCHUR_TILE");
-    constexpr int NC = 3;
+    const char *force = getenv(sizeof(T) == 8 ? "SS_SCHUR_TILE" : "SS_SCHUR_TILE_C64");
+    constexpr int NC = sizeof(T) == 8 ? 3 : 2;
     P.tune_ms.assign((size_t)NC * S.nlevel, 0.f);
     if (!force) {
       std::vector<cudaEvent_t> e(2 * NC * S.nlevel);
@@ -1514,6 +1529,8 @@ struct Sweeper {
           cudaEventElapsedTime(&P.tune_ms[c * S.nlevel + l], e[2 * (c * S.nlevel + l)], e[2 * (c * S.nlevel + l) + 1]);
         }
       for (auto &x : e) cudaEventDestroy(x);
+      if constexpr (sizeof(T) == 4) goto picks;
+      {
       // panel-step GEMMs: all of them once with SIMT tiles, once with DMMA tiles
       cudaEvent_t pe[4];
       for (auto &x : pe) SS_CK(cudaEventCreate(&x));
@@ -1539,9 +1556,11 @@ struct Sweeper {
       P.panel_dmma = pt[1] < pt[0];
       P.panel_ms[0] = pt[0];
       P.panel_ms[1] = pt[1];
+      }
     } else {
-      P.panel_dmma = atoi(force) == 2;
+      P.panel_dmma = sizeof(T) == 8 && atoi(force) == 2;
     }
+  picks:
     for (int l = 0; l < S.nlevel; ++l) {
       int best = 0;
       if (force) {
@@ -1609,11 +1628,7 @@ struct Sweeper {
     b.fronts = P.d_large.as<int>() + P.large_ptr[l];
     const GemmTask *tasks = P.d_tasks.as<GemmTask>();
     cudaEventRecord(ev[2 * nev], h.stream);
-    if (sizeof(T) == 4)
-      tc::front_tc_gemm_kernel<<<dim3((unsigned)(t1 - t0), nb), tc::THREADS, tc::SMEM_BYTES, h.stream>>>(
-          reinterpret_cast<cf *>(b.arena), b.stride, b.off, b.ld, tasks + t0, tc_err);
-    else
-      schur_launch(b, l, P.pick[l], nb);
+    schur_launch(b, l, P.pick[l], nb);
     cudaEventRecord(ev[2 * nev + 1], h.stream);
     ++nev;
     ++launches;
@@ -1728,6 +1743,8 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
     SS_CK(cudaFuncSetAttribute(front_small_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                small_limit<T>() * small_limit<T>() * (int)sizeof(cplx<T>)));
     SS_CK(cudaFuncSetAttribute(tc::front_tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               tc::SMEM_BYTES));
+    SS_CK(cudaFuncSetAttribute(tc::front_tc_gemm_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                tc::SMEM_BYTES));
     // solve kernels stage a whole front vector in shared memory
     const int vec = (int)std::min<int64_t>(227 * 1024, (int64_t)S.max_m * (int64_t)sizeof(cplx<T>));

@@ -39,6 +39,7 @@ extern "C" int ss_create(ss_handle **out, int device) {
   if (!p) return SS_ENOMEM;
   p->h.device = device;
   cudaSetDevice(device);
+  cudaDeviceGetAttribute(&p->h.num_sms, cudaDevAttrMultiProcessorCount, device);
   if (cudaStreamCreateWithFlags(&p->h.stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete p;
     return SS_ECUDA;

@@ -63,6 +63,7 @@ struct Symbolic {
 
 struct Handle {
   int device = 0;
+  int num_sms = 148;                     // streaming multiprocessors of the device
   cudaStream_t stream = nullptr;
   std::string err;
   // mesh

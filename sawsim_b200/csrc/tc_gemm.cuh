@@ -158,12 +158,13 @@ __device__ __forceinline__ uint32_t sw_off(int r, int q) { return (uint32_t)(r *
 // complex (16-byte pieces: two complex, aligned because ld, the front offsets
 // and the chunk start are even), B 16 rows x 64 complex (8-byte pieces: the
 // column start k + 64 t may be odd).  Out-of-range pieces are zero-filled.
+template <int NT = THREADS>
 __device__ __forceinline__ void issue_chunk(unsigned char *raw, const cf *F, int ld, const GemmTask &tk, int kb) {
   const int t = threadIdx.x;
   const uint32_t ra = smem_u32(raw), rb = ra + RAW_A_BYTES;
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int idx = t + THREADS * i;        // 0..1023
+  for (int i = 0; i < 1024 / NT; ++i) {
+    const int idx = t + NT * i;             // 0..1023
     const int row = idx >> 3, q = idx & 7;  // q: pair of complex K columns
     const int r = tk.r0 + row, c = kb + 2 * q;
     const int valid = (r < tk.rhi) ? max(0, min(2, tk.kk1 - c)) : 0;
@@ -171,8 +172,8 @@ __device__ __forceinline__ void issue_chunk(unsigned char *raw, const cf *F, int
     cp_async16(ra + (uint32_t)(row * 128 + q * 16), src, (uint32_t)(valid * 8));
   }
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int idx = t + THREADS * i;        // 0..1023
+  for (int i = 0; i < 1024 / NT; ++i) {
+    const int idx = t + NT * i;             // 0..1023
     const int j = idx >> 6, cc = idx & 63;  // complex k-row, complex column
     const int r = kb + j, c = tk.c0 + cc;
     const bool ok = r < tk.kk1 && c < tk.chi;
@@ -181,12 +182,14 @@ __device__ __forceinline__ void issue_chunk(unsigned char *raw, const cf *F, int
 }
 
 // Raw tiles -> the four MMA operands (A hi/lo, B' hi/lo) in 128-byte swizzle.
+template <int NT = THREADS>
 __device__ __forceinline__ void convert_chunk(const unsigned char *raw, unsigned char *stage) {
   unsigned char *ahi = stage, *alo = stage + OPER_BYTES, *bhi = stage + 2 * OPER_BYTES, *blo = stage + 3 * OPER_BYTES;
   const int t = threadIdx.x;
+  constexpr int NW = NT / 32;
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int idx = t + THREADS * i;
+  for (int i = 0; i < 1024 / NT; ++i) {
+    const int idx = t + NT * i;
     const int row = idx >> 3, q = idx & 7;
     const float4 v = *reinterpret_cast<const float4 *>(raw + row * 128 + q * 16);
     const float4 h = make_float4(tf32_hi(v.x), tf32_hi(v.y), tf32_hi(v.z), tf32_hi(v.w));
@@ -198,9 +201,9 @@ __device__ __forceinline__ void convert_chunk(const unsigned char *raw, unsigned
   // (swizzle slot, half) pair of the rows 2cc / 2cc+1 twice (two wavefronts)
   const int lane = t & 31, wrp = t >> 5;
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
+  for (int i = 0; i < 1024 / NT; ++i) {
     const int j = 8 * (i & 1) + (lane & 7);
-    const int cc = 4 * (wrp + 8 * (i >> 1)) + (lane >> 3);
+    const int cc = 4 * (wrp + NW * (i >> 1)) + (lane >> 3);
     const float2 v = *reinterpret_cast<const float2 *>(raw + RAW_A_BYTES + j * RAW_B_STRIDE + cc * 8);
     const float hr = tf32_hi(v.x), hi = tf32_hi(v.y), nhi = tf32_hi(-v.y);
     const float lr = v.x - hr, li = v.y - hi, nli = -v.y - nhi;
@@ -352,6 +355,219 @@ __global__ void __launch_bounds__(THREADS, 1)
   if (wid == 0) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// Persistent, warp-specialised version: one CTA per SM walks the (tile,
+// frequency) items of a launch.  Warps 0-3 stream and convert operands (the
+// per-chunk pipeline above), warp 8 issues the MMAs, warps 4-7 drain the
+// accumulator.  Two TMEM accumulators (2 x 128 columns) let one tile's epilogue
+// overlap the next tile's loads and MMAs.  Handoffs are mbarriers:
+//   op_full[s]   producers -> MMA   (stage s converted)
+//   op_empty[s]  MMA -> producers   (tcgen05.commit: the MMAs reading s are done)
+//   acc_full[a]  MMA -> epilogue    (tcgen05.commit after an item's last chunk)
+//   acc_empty[a] epilogue -> MMA    (128 arrivals: accumulator a read out)
+// Every wait is bounded; on time-out the CTA records the error and every role
+// leaves its loop (bounded), the MMA role drains its commits, TMEM is freed.
+constexpr int P_THREADS = 288;
+constexpr int P_TMEM_COLS = 256;
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void producers_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+// barrier of the 128 producer threads that also ORs a flag across them, so that a
+// decision to stop is taken by all of them together
+__device__ __forceinline__ bool producers_sync_or(bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 q, %1, 0;\n\t"
+      "bar.red.or.pred p, 1, 128, q;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)v)
+      : "memory");
+  return r != 0;
+}
+
+__device__ __forceinline__ int item_chunks(const GemmTask &tk) { return (tk.kk1 - tk.kk0 + BKC - 1) / BKC; }
+
+__global__ void __launch_bounds__(P_THREADS, 1)
+    front_tc_gemm_persistent(cf *__restrict__ arena, int64_t stride, const int64_t *__restrict__ off,
+                             const int *__restrict__ ldv, const GemmTask *__restrict__ tasks, int ntasks, int nb,
+                             int *__restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
+  __shared__ __align__(8) uint64_t op_full[STAGES], op_empty[STAGES], acc_full[2], acc_empty[2], drain;
+  __shared__ uint32_t tmem_base_s;
+  __shared__ volatile int abort_s;
+  unsigned char *smem = reinterpret_cast<unsigned char *>(
+      (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  unsigned char *raw0 = smem + STAGES * STAGE_BYTES;
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t n_items = (int64_t)ntasks * nb;
+  if (threadIdx.x == 0) {
+    abort_s = *reinterpret_cast<volatile int *>(err);
+    for (int s2 = 0; s2 < STAGES; ++s2) {
+      mbar_init(smem_u32(&op_full[s2]), 1);
+      mbar_init(smem_u32(&op_empty[s2]), 1);
+    }
+    for (int a2 = 0; a2 < 2; ++a2) {
+      mbar_init(smem_u32(&acc_full[a2]), 1);
+      mbar_init(smem_u32(&acc_empty[a2]), 128);
+    }
+    mbar_init(smem_u32(&drain), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (abort_s) return;
+  if (wid == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)),
+                 "r"(P_TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_s;
+
+  if (wid < 4) {
+    // ---------------- producers: raw tiles by cp.async, conversion into the operand stages
+    int64_t gc = 0;   // chunks converted by this CTA
+    bool stop = false;
+    for (int64_t it = blockIdx.x; it < n_items && !stop; it += gridDim.x) {
+      const GemmTask tk = tasks[it % ntasks];
+      const int fq = (int)(it / ntasks);
+      const int ld = ldv[tk.f];
+      const cf *F = arena + (int64_t)fq * stride + off[tk.f];
+      const int nk = item_chunks(tk);
+      for (int c = 0; c < RAW_STAGES - 1; ++c) {
+        if (c < nk) issue_chunk<128>(raw0 + c * RAW_BYTES, F, ld, tk, tk.kk0 + c * BKC);
+        cp_async_commit();
+      }
+      for (int kc = 0; kc < nk; ++kc) {
+        const int cn = kc + RAW_STAGES - 1;
+        if (cn < nk) issue_chunk<128>(raw0 + (cn % RAW_STAGES) * RAW_BYTES, F, ld, tk, tk.kk0 + cn * BKC);
+        cp_async_commit();
+        cp_async_wait<RAW_STAGES - 1>();
+        const int s2 = (int)(gc % STAGES);
+        bool late = gc >= STAGES && !mbar_wait(smem_u32(&op_empty[s2]), (uint32_t)(((gc / STAGES) - 1) & 1));
+        // chunk kc in shared memory and stage s2 free, or every producer stops
+        if (producers_sync_or(late || abort_s)) {
+          abort_s = 1;
+          stop = true;
+          break;
+        }
+        convert_chunk<128>(raw0 + (kc % RAW_STAGES) * RAW_BYTES, smem + s2 * STAGE_BYTES);
+        fence_async_smem();
+        producers_sync();
+        if (threadIdx.x == 0) mbar_arrive(smem_u32(&op_full[s2]));
+        ++gc;
+      }
+      cp_async_wait<0>();
+      // raw stages free before the next item's prologue; stop together
+      if (producers_sync_or(stop || abort_s)) stop = true;
+    }
+    cp_async_wait<0>();
+  } else if (wid == 8) {
+    // ---------------- MMA issuer (one lane)
+    if (lane == 0) {
+      int64_t gc = 0, ac = 0;
+      bool issued = false;
+      for (int64_t it = blockIdx.x; it < n_items && !abort_s; it += gridDim.x) {
+        const GemmTask tk = tasks[it % ntasks];
+        const int nk = item_chunks(tk);
+        if (nk <= 0) continue;
+        const int a2 = (int)(ac & 1);
+        if (ac >= 2 && !mbar_wait(smem_u32(&acc_empty[a2]), (uint32_t)(((ac / 2) - 1) & 1))) {
+          abort_s = 1;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d = tmem + (uint32_t)(a2 * 128);
+        for (int kc = 0; kc < nk; ++kc) {
+          const int s2 = (int)(gc % STAGES);
+          if (!mbar_wait(smem_u32(&op_full[s2]), (uint32_t)((gc / STAGES) & 1))) {
+            abort_s = 1;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t base = smem_u32(smem + s2 * STAGE_BYTES);
+          const uint32_t ahi = base, alo = base + OPER_BYTES, bhi = base + 2 * OPER_BYTES, blo = base + 3 * OPER_BYTES;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const uint32_t ko = 32u * k;
+            mma_tf32(d, sw128_desc(ahi + ko), sw128_desc(bhi + ko), (kc > 0 || k > 0) ? 1u : 0u);
+            mma_tf32(d, sw128_desc(ahi + ko), sw128_desc(blo + ko), 1u);
+            mma_tf32(d, sw128_desc(alo + ko), sw128_desc(bhi + ko), 1u);
+          }
+          mma_commit(smem_u32(&op_empty[s2]));
+          issued = true;
+          ++gc;
+        }
+        if (abort_s) break;
+        mma_commit(smem_u32(&acc_full[a2]));
+        ++ac;
+      }
+      if (issued) {   // every MMA of this CTA complete before TMEM is freed
+        mma_commit(smem_u32(&drain));
+        if (!mbar_wait(smem_u32(&drain), 0u)) abort_s = 1;
+      }
+    }
+    __syncwarp();
+  } else {
+    // ---------------- epilogue warps 4-7: TMEM lanes 32 (wid - 4) .. +32, all 128 columns
+    const int q = wid - 4;
+    const int row = 32 * q + lane;
+    int64_t ac = 0;
+    for (int64_t it = blockIdx.x; it < n_items; it += gridDim.x) {
+      if (__any_sync(0xffffffffu, abort_s != 0)) break;     // warp-uniform (tcgen05.ld is .sync.aligned)
+      const GemmTask tk = tasks[it % ntasks];
+      if (item_chunks(tk) <= 0) continue;
+      const int fq = (int)(it / ntasks);
+      const int ld = ldv[tk.f];
+      cf *F = arena + (int64_t)fq * stride + off[tk.f];
+      const int a2 = (int)(ac & 1);
+      const bool ok = mbar_wait(smem_u32(&acc_full[a2]), (uint32_t)((ac / 2) & 1));
+      if (__any_sync(0xffffffffu, !ok)) {
+        abort_s = 1;
+        break;
+      }
+      tc_fence_after();
+      const int r = tk.r0 + row;
+      float v[32];
+#pragma unroll
+      for (int cb = 0; cb < 4; ++cb) {
+        const uint32_t taddr = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(a2 * 128 + 32 * cb);
+        tmem_ld32(taddr, v);
+        if (r < tk.rhi) {
+          cf *crow = F + (int64_t)r * ld;
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const int c = tk.c0 + 16 * cb + j;
+            if (c < tk.chi) {
+              cf dv = crow[c];
+              dv.x -= v[2 * j];
+              dv.y -= v[2 * j + 1];
+              crow[c] = dv;
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(smem_u32(&acc_empty[a2]));
+      ++ac;
+    }
+  }
+  if (abort_s && threadIdx.x == 0) atomicExch(err, 1);
+  tc_fence_before();
+  __syncthreads();
+  if (wid == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(P_TMEM_COLS) : "memory");
   }
 }
 

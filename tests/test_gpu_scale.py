@@ -87,3 +87,21 @@ def test_every_schur_tile_candidate_is_exact(mid, tile, monkeypatch):
     assert counts[tile] > 0 and sum(counts) == counts[tile]
     assert s['panel_gemm_dmma'] == (1.0 if tile == 2 else 0.0)
     assert np.max(np.abs(Q - Q0) / np.abs(Q0)) < 1e-9
+
+
+@pytest.mark.parametrize('tile', [0, 1])
+def test_every_complex64_schur_candidate_converges(mid, tile, monkeypatch):
+    """Both tcgen05 Schur kernels (one CTA per tile; persistent warp-specialised CTAs
+    with double-buffered TMEM accumulators), each forced on every level, give a
+    mixed sweep within 1e-6 of FP64."""
+    case, _, g = mid
+    f = np.linspace(case.freqs[0], case.freqs[-1], 5)
+    Q64, _, _ = g.charges(2 * np.pi * f, 1.0, 'fp64')
+    monkeypatch.setenv('SS_SCHUR_TILE_C64', str(tile))
+    e = cases.engine_for(case)
+    try:
+        Q, st, _ = e.charges(2 * np.pi * f, 1.0, 'mixed')
+    finally:
+        e.close()
+    assert (st == 0).all()
+    assert np.max(np.abs(Q - Q64) / np.abs(Q64)) < 1e-6
