@@ -162,14 +162,16 @@ int ss_solve_adjoint(ss_handle *h, double omega, int precision, double *lambda);
  * derivative; its charge is Q = kts . disp (sweep.py:303-305, :356-363) and the
  * element routine is piezo_fem.py:248-367.  A parameter is described by its
  * seeds (parameter-major, any pointer may be NULL = zero):
- *   dpos   n_params x n_nodes x 2       node velocities dX/dp (metres per unit p)
+ *   dpos   n_params x n_nodes x dim     node velocities dX/dp (metres per unit p;
+ *                                       dim 2 for Q9, 3 for Hex27)
  *   dC     n_params x n_mat x 6 x 6 x 2 d(material C)/dp, complex interleaved
  *   de     n_params x n_mat x 3 x 6 x 2
  *   deps   n_params x n_mat x 3 x 3 x 2
  *   drho   n_params x n_mat
  *   dinner, douter  n_params x n_regions x 3   d(PML bounds)/dp
- * Outputs: Q (n_f x 2) and dQ (n_f x n_params x 2).  Q9 meshes only; no
- * Rayleigh damping.  status: n_f per-point status as ss_sweep (may be NULL).
+ * Outputs: Q (n_f x 2) and dQ (n_f x n_params x 2).  Q9 and Hex27 meshes
+ * (saw3d/assembly.py:230-327 for the Hex27 element routine); no Rayleigh
+ * damping.  status: n_f per-point status as ss_sweep (may be NULL).
  */
 int ss_adjoint_gradient(ss_handle *h, int n_f, const double *omega, double V, int precision, int n_params,
                         const double *dpos, const double *dC, const double *de, const double *deps,

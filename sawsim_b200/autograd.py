@@ -1,7 +1,9 @@
 """PyTorch surface of the adjoint: Y11 as a differentiable function of cell parameters.
 
-``y11(params, model, freqs)`` returns the 2D admittance Y11 = -i w Q / V
-(src/sawsim/solver.py:128) of the cell ``model.build(params)`` at ``freqs`` (Hz)
+``y11(params, model, freqs)`` returns the admittance Y11 of the cell
+``model.build(params)`` at ``freqs`` (Hz): -i w Q / V for the 2D Q9 cells
+(src/sawsim/solver.py:128), +i w Q / V / aperture for the Hex27 slabs
+(src/sawsim/hex_solver.py:103)
 as a complex128 tensor; its backward pass returns dL/dparams from the adjoint
 gradient computed with the same factorisation (``ss_adjoint_gradient``).  Torch is
 only the autograd surface: the sweep and the gradient run in libsawsim_b200.so.
@@ -15,17 +17,19 @@ from . import cases
 
 
 def y11_and_jacobian(model, params, freqs, precision='fp64', V=1.0, device=0):
-    """(Y[n_f], dY/dp[n_f, n_params], status) at parameters ``params``."""
+    """(Y[n_f], dY/dp[n_f, n_params], status) at parameters ``params`` of a
+    ``params.Q9Model`` or ``params.HexModel`` (the model fixes the Y11 sign and
+    normalisation of its pipeline)."""
     p = np.asarray(params, dtype=float)
     case = model.build(p)
-    eng = cases.engine_for(case, device=device)
+    eng = model.engine(case, device=device)
     try:
         w = 2 * np.pi * np.asarray(freqs, dtype=float)
         Q, dQ, st = eng.gradient(w, model.seeds(p), V, precision)
     finally:
         eng.close()
-    Y = -1j * w * Q / V
-    dY = -1j * w[:, None] * dQ / V
+    Y = model.y11(w, Q, V, case)
+    dY = model.y11(w[:, None], dQ, V, case)
     return Y, dY, st
 
 

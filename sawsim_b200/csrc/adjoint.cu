@@ -1,5 +1,5 @@
-// Adjoint gradient of the charge: dQ/dp for parameters that move the Q9 mesh
-// nodes, the material tensors and the PML bounds.
+// Adjoint gradient of the charge: dQ/dp for parameters that move the mesh nodes
+// (Q9 or Hex27), the material tensors and the PML bounds.
 //
 // The reference has no derivative; its charge is Q = kts . disp with
 // kts = K^T s (src/sawsim/saw2d/sweep.py:303-305, :356-363) and disp[active]
@@ -10,44 +10,19 @@
 // DOFs) and s the + electrode indicator.  Rayleigh damping is not differentiated.
 //
 // dK_e/dp, dM_e/dp are recomputed on the fly by forward-mode differentiation
-// (dual numbers) of the Q9 element routine of piezo_fem.py:248-367 (the same
-// arithmetic as q9_element_kernel), seeded with the parameter's node velocities,
-// material-tensor derivatives and PML-bound derivatives.
+// (dual numbers) of the element routines: Q9 piezo_fem.py:248-367 (the
+// arithmetic of q9_element_kernel) and Hex27 saw3d/assembly.py:230-327
+// (hex27_tangent_kernel), seeded with the parameter's node velocities,
+// material-tensor derivatives and PML-bound derivatives.  For Hex27 the charge
+// is the same functional (bc_solve.py:141-175, Q from the unfolded K rows).
 #include "ss_internal.h"
 #include "dev_complex.cuh"
 #include "q9_element.cuh"
+#include "dual.cuh"
 
 #include <vector>
 
 namespace ss {
-
-// value and tangent
-struct dual {
-  double v, d;
-  __host__ __device__ dual(double a = 0.0, double b = 0.0) : v(a), d(b) {}
-};
-__device__ inline dual operator+(dual a, dual b) { return {a.v + b.v, a.d + b.d}; }
-__device__ inline dual operator-(dual a, dual b) { return {a.v - b.v, a.d - b.d}; }
-__device__ inline dual operator-(dual a) { return {-a.v, -a.d}; }
-__device__ inline dual operator*(dual a, dual b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
-__device__ inline dual operator/(dual a, dual b) { return {a.v / b.v, (a.d * b.v - a.v * b.d) / (b.v * b.v)}; }
-__device__ inline dual fabs(dual a) { return a.v < 0 ? -a : a; }
-__device__ inline bool operator>=(dual a, dual b) { return a.v >= b.v; }
-__device__ inline dual ipow(dual a, int n) {
-  dual r{1.0, 0.0};
-  for (int i = 0; i < n; ++i) r = r * a;
-  return r;
-}
-using cdu = cplx<dual>;
-__device__ inline cdu cdu_of(const double *v, const double *t) { return cdu{dual{v[0], t ? t[0] : 0.0}, dual{v[1], t ? t[1] : 0.0}}; }
-__device__ inline cd tangent(cdu a) { return cd{a.x.d, a.y.d}; }
-
-// Seeds of one parameter (device pointers, any may be null = zero).
-struct Seed {
-  const double *dpos;     // N x 2
-  const double *dC, *de, *deps, *drho;   // per material, complex interleaved like ss_set_materials
-  const double *dinner, *douter;         // per PML region x 3
-};
 
 __constant__ double c_gpa[3] = {-0.774596669241483, 0.0, 0.774596669241483};
 __constant__ double c_gwa[3] = {5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0};
@@ -86,27 +61,6 @@ __device__ inline void q9_shape_a(double x, double y, double *N, double *dx, dou
   dy[6] = 0.25 * (-2 * (x + 1) * (x - 1) * (2 * y + 1));
   dy[7] = 0.25 * (-4 * x * y * (x - 1));
   dy[8] = 0.25 * (8 * y * (x * x - 1));
-}
-
-// PML alphas in dual numbers (piezo_fem.py:222-242), Q9 clamp of the ratio
-__device__ inline void pml_alpha_dual(const PmlDev &P, const Seed &sd, int64_t e, const dual *xc, cdu *a) {
-  a[0] = a[1] = a[2] = cdu{dual{1.0}, dual{0.0}};
-  if (!P.elem_region) return;
-  const int r = P.elem_region[e];
-  if (r < 0) return;
-  for (int ax = 0; ax < 2; ++ax) {
-    if (!((P.axis[r] >> ax) & 1)) continue;
-    const dual o{P.outer[3 * r + ax], sd.douter ? sd.douter[3 * r + ax] : 0.0};
-    const dual in{P.inner[3 * r + ax], sd.dinner ? sd.dinner[3 * r + ax] : 0.0};
-    dual ratio = (xc[ax] - o) * (xc[ax] - o) / ((in - o) * (in - o));
-    if (P.clip) {
-      if (ratio.v < 0.0) ratio = dual{0.0};
-      if (ratio.v > 1.0) ratio = dual{1.0};
-    }
-    const dual d = dual{P.dmax[r]} * ipow(dual{1.0} - ratio, P.npow[r]);
-    // 1 + d / (i w) = 1 - i d / w
-    a[ax] = cdu{dual{1.0}, -(d / dual{P.omega})};
-  }
 }
 
 // Tangent element matrices dKel [e][A][B][81], dMel [e][81] of ne Q9 elements,
@@ -158,7 +112,7 @@ __global__ void __launch_bounds__(128) q9_tangent_kernel(int64_t ne, int nc, con
   }
   const int mi = emat[e];
   cdu alpha[3], sc[6];
-  const dual xc[2] = {X(8, 0), X(8, 1)};
+  const dual xc[3] = {X(8, 0), X(8, 1), dual{0.0}};
   pml_alpha_dual(pml, sd, e, xc, alpha);
   sc[0] = cdiv(cmul(alpha[1], alpha[2]), alpha[0]);
   sc[1] = alpha[2];
@@ -306,6 +260,60 @@ __global__ void __launch_bounds__(128) contract_kernel(int64_t ne, int nc, int n
   }
 }
 
+// Hex27: part[f][e] as contract_kernel for 108 element DOFs (u interleaved 3n + c,
+// phi at 3N + n).  The element's dK (16 x 729 complex) stays in global memory
+// (L1/L2-resident while the CTA works); frequencies go in groups of 4 whose
+// vectors are staged in shared memory; fixed-order reduction per frequency.
+constexpr int kHexFG = 4;
+__global__ void __launch_bounds__(256) contract_hex_kernel(int64_t ne, int64_t N, int nb, int64_t gdof,
+                                                           const int64_t *__restrict__ conn,
+                                                           const cd *__restrict__ dKel, const cd *__restrict__ dMel,
+                                                           const cd *__restrict__ d, const cd *__restrict__ m,
+                                                           const unsigned char *__restrict__ splus,
+                                                           const double *__restrict__ omega, cd *__restrict__ part) {
+  __shared__ cd s_d[kHexFG][108], s_w[kHexFG][108], s_m[kHexFG][108];
+  __shared__ cd s_r[kHexFG][108];
+  const int64_t e = blockIdx.x;
+  const int64_t *cn = conn + e * 27;
+  const cd *K = dKel + e * 16 * 729;
+  const cd *Me = dMel + e * 729;
+  for (int f0 = 0; f0 < nb; f0 += kHexFG) {
+    const int nf = min(kHexFG, nb - f0);
+    __syncthreads();
+    for (int t = threadIdx.x; t < nf * 108; t += blockDim.x) {
+      const int fi = t / 108, r = t % 108, A = r / 27, a = r % 27;
+      const int64_t g = A < 3 ? 3 * cn[a] + A : 3 * N + cn[a];
+      const cd dv = d[(int64_t)(f0 + fi) * gdof + g], mv = m[(int64_t)(f0 + fi) * gdof + g];
+      s_d[fi][r] = dv;
+      s_m[fi][r] = mv;
+      s_w[fi][r] = cd{(splus[g] ? 1.0 : 0.0) - mv.x, -mv.y};
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < nf * 108; t += blockDim.x) {
+      const int fi = t / 108, r = t % 108, A = r / 27, a = r % 27;
+      cd y{0.0, 0.0};
+      for (int B = 0; B < 4; ++B) {
+        const cd *row = K + (A * 4 + B) * 729 + a * 27;
+        for (int b = 0; b < 27; ++b) y = y + cmul(row[b], s_d[fi][B * 27 + b]);
+      }
+      cd acc = cmul(s_w[fi][r], y);
+      if (A < 3) {
+        cd ym{0.0, 0.0};
+        for (int b = 0; b < 27; ++b) ym = ym + cmul(Me[a * 27 + b], s_d[fi][A * 27 + b]);
+        const double w2 = omega[f0 + fi] * omega[f0 + fi];
+        acc = acc + cmul(s_m[fi][r], ym) * w2;
+      }
+      s_r[fi][r] = acc;
+    }
+    __syncthreads();
+    if (threadIdx.x < nf) {
+      cd acc{0.0, 0.0};
+      for (int r = 0; r < 108; ++r) acc = acc + s_r[threadIdx.x][r];
+      part[(int64_t)(f0 + threadIdx.x) * ne + e] = acc;
+    }
+  }
+}
+
 // out[f] = sum_e part[f][e], fixed-order tree per frequency
 __global__ void sum_rows_kernel(int64_t ne, const cd *__restrict__ part, cd *__restrict__ out) {
   __shared__ cd red[256];
@@ -332,10 +340,11 @@ int run_adjoint_gradient(Handle &h, int n_f, const double *omega, double V, int 
                          const double *dpos, const double *dC, const double *de, const double *deps,
                          const double *drho, const double *dinner, const double *douter, double *Q, double *dQ,
                          int *status) {
-  if (h.kind == SS_HEX27) return fail(h, SS_EINVAL, "adjoint gradient: Q9 meshes only");
   if (h.have_D && h.beta != 0.0) return fail(h, SS_EINVAL, "adjoint gradient: Rayleigh damping is not differentiated");
   if (!h.have_K) return fail(h, SS_ESTATE, "adjoint gradient: assemble first");
+  const bool hex = h.kind == SS_HEX27;
   const int nc = h.nc, ndisp = h.kind == SS_Q9_ME0 ? 2 : 3, nm = h.nmat[0], npml = h.npml;
+  const int npe = h.npe, dim = h.dim;
   const int64_t N = h.N, ne = h.ne, G = h.gdof, n = h.sym.n;
   // device copies of the mesh, materials and PML
   DBuf dp, dcn, dem, drh, dCm, deM, depsM, dax, dnp, dreg, ddm, din, dout;
@@ -370,7 +379,7 @@ int run_adjoint_gradient(Handle &h, int n_f, const double *omega, double V, int 
     return dupload(b, v);
   };
   DBuf sp, sC, se, seps, srho, sin, sout;
-  AD_CK(up(sp, dpos, (size_t)n_params * N * 2));
+  AD_CK(up(sp, dpos, (size_t)n_params * N * dim));
   AD_CK(up(sC, dC, (size_t)n_params * nm * 72));
   AD_CK(up(se, de, (size_t)n_params * nm * 36));
   AD_CK(up(seps, deps, (size_t)n_params * nm * 18));
@@ -389,8 +398,8 @@ int run_adjoint_gradient(Handle &h, int n_f, const double *omega, double V, int 
   DBuf dgn, dsp, dK, dM, dd, dm, dpart, dout2, dom;
   AD_CK(dupload(dgn, gnew));
   AD_CK(dupload(dsp, splus));
-  AD_CK(dalloc(dK, (size_t)ne * nc * nc * 81 * sizeof(cd)));
-  AD_CK(dalloc(dM, (size_t)ne * 81 * sizeof(cd)));
+  AD_CK(dalloc(dK, (size_t)ne * nc * nc * npe * npe * sizeof(cd)));
+  AD_CK(dalloc(dM, (size_t)ne * npe * npe * sizeof(cd)));
   SweepExtra ex;
   ex.per_chunk = [&](int c0, int nb, const cplx<double> *x, const cplx<double> *mu) -> int {
     AD_CK(dalloc(dd, (size_t)nb * G * sizeof(cd)));
@@ -405,19 +414,30 @@ int run_adjoint_gradient(Handle &h, int n_f, const double *omega, double V, int 
     std::vector<cd> out(nb);
     for (int p = 0; p < n_params; ++p) {
       Seed sd{};
-      sd.dpos = sp.p ? sp.as<double>() + (size_t)p * N * 2 : nullptr;
+      sd.dpos = sp.p ? sp.as<double>() + (size_t)p * N * dim : nullptr;
       sd.dC = sC.p ? sC.as<double>() + (size_t)p * nm * 72 : nullptr;
       sd.de = se.p ? se.as<double>() + (size_t)p * nm * 36 : nullptr;
       sd.deps = seps.p ? seps.as<double>() + (size_t)p * nm * 18 : nullptr;
       sd.drho = srho.p ? srho.as<double>() + (size_t)p * nm : nullptr;
       sd.dinner = sin.p ? sin.as<double>() + (size_t)p * npml * 3 : nullptr;
       sd.douter = sout.p ? sout.as<double>() + (size_t)p * npml * 3 : nullptr;
-      q9_tangent_kernel<<<(unsigned)((ne + 3) / 4), 128, 0, h.stream>>>(
-          ne, nc, dp.as<double>(), dcn.as<int64_t>(), dem.as<int32_t>(), drh.as<double>(), dCm.as<double>(),
-          deM.as<double>(), depsM.as<double>(), pml, sd, dK.as<cd>(), dM.as<cd>());
-      contract_kernel<<<(unsigned)ne, 128, 0, h.stream>>>(ne, nc, ndisp, N, nb, G, dcn.as<int64_t>(), dK.as<cd>(),
-                                                          dM.as<cd>(), dd.as<cd>(), dm.as<cd>(),
-                                                          dsp.as<unsigned char>(), dom.as<double>(), dpart.as<cd>());
+      if (hex) {
+        AD_CK(launch_hex27_tangent(h.stream, ne, dp.as<double>(), dcn.as<int64_t>(), dem.as<int32_t>(),
+                                   drh.as<double>(), dCm.as<double>(), deM.as<double>(), depsM.as<double>(), pml, sd,
+                                   dK.as<cd>(), dM.as<cd>()));
+        contract_hex_kernel<<<(unsigned)ne, 256, 0, h.stream>>>(ne, N, nb, G, dcn.as<int64_t>(), dK.as<cd>(),
+                                                                dM.as<cd>(), dd.as<cd>(), dm.as<cd>(),
+                                                                dsp.as<unsigned char>(), dom.as<double>(),
+                                                                dpart.as<cd>());
+      } else {
+        q9_tangent_kernel<<<(unsigned)((ne + 3) / 4), 128, 0, h.stream>>>(
+            ne, nc, dp.as<double>(), dcn.as<int64_t>(), dem.as<int32_t>(), drh.as<double>(), dCm.as<double>(),
+            deM.as<double>(), depsM.as<double>(), pml, sd, dK.as<cd>(), dM.as<cd>());
+        contract_kernel<<<(unsigned)ne, 128, 0, h.stream>>>(ne, nc, ndisp, N, nb, G, dcn.as<int64_t>(), dK.as<cd>(),
+                                                            dM.as<cd>(), dd.as<cd>(), dm.as<cd>(),
+                                                            dsp.as<unsigned char>(), dom.as<double>(),
+                                                            dpart.as<cd>());
+      }
       sum_rows_kernel<<<nb, 256, 0, h.stream>>>(ne, dpart.as<cd>(), dout2.as<cd>());
       AD_CK(cudaGetLastError());
       AD_CK(cudaMemcpyAsync(out.data(), dout2.p, nb * sizeof(cd), cudaMemcpyDeviceToHost, h.stream));

@@ -148,6 +148,13 @@ int run_adjoint_gradient(Handle &h, int n_f, const double *omega, double V, int 
                          const double *dpos, const double *dC, const double *de, const double *deps,
                          const double *drho, const double *dinner, const double *douter, double *Q, double *dQ,
                          int *status);
+// hex27.cu: tangent element matrices of a parameter (Seed: dual.cuh)
+struct Seed;
+struct PmlDev;
+cudaError_t launch_hex27_tangent(cudaStream_t st, int64_t ne, const double *pos, const int64_t *conn,
+                                 const int32_t *emat, const double *rho, const double *C, const double *e,
+                                 const double *eps, const PmlDev &pml, const Seed &sd, cplx<double> *dKel,
+                                 cplx<double> *dMel);
 // symbolic.cpp
 int build_global_pattern(Handle &h);
 int build_condensation(Handle &h);

@@ -144,6 +144,14 @@ class Q9Model:
                           dict(seed=self.seed, cols=self.cols, rows=self.rows))
         return case
 
+    def engine(self, case, device=0):
+        return cases.engine_for(case, device=device)
+
+    @staticmethod
+    def y11(w, Q, V, case):
+        """-i w Q / V (src/sawsim/solver.py:128)."""
+        return -1j * w * Q / V
+
     def seeds(self, v):
         """Derivative seeds of every parameter at ``v`` (one dict per parameter)."""
         v = np.asarray(v, dtype=float)
@@ -179,5 +187,87 @@ class Q9Model:
                     M = mt.bond_matrix(a)
                     dC[0] = M @ unit.C @ M.T
                 s['dC'], s['de'], s['deps'] = dC, de, deps
+            out.append(s)
+        return out
+
+
+@dataclass
+class HexModel:
+    """A Hex27 slab (``cells.hex_double_layer_slab`` or ``hex_four_layer_slab``) as a
+    function of ``pitch_um`` (the period: x scales, aperture, depths and electrode
+    height stay) and ``t_film_um`` (the piezo film thickness: the film stretches,
+    everything below it moves down, PML bounds included)."""
+
+    nx: int = 8
+    ny: int = 4
+    nz: int = 48
+    seed: int = 0
+    stack: str = 'double'
+    crystal: mt.Material = field(init=False)
+    euler: np.ndarray = field(init=False)
+
+    def __post_init__(self):
+        self.crystal, self.euler = mt.seeded_3m(self.seed)
+
+    names = ['pitch_um', 't_film_um']
+
+    def _layers(self):
+        p = 1.085
+        if self.stack == 'double':
+            nz = self.nz
+            r = [nz // 6, nz // 3]
+            return [(cells.HEX_TAG_PIEZO, 0.6 * p, r[0]), (cells.HEX_TAG_LAYER, 1.4 * p, r[1]),
+                    (10, 2 * p, nz - sum(r))], 0.5, ['sio2']
+        nz = self.nz
+        r = [nz // 8, nz // 16, nz // 8]
+        r_pml = nz // 4
+        return [(cells.HEX_TAG_PIEZO, 0.5 * p, r[0]), (cells.HEX_TAG_LAYER, 0.25 * p, r[1]), (11, 0.5 * p, r[2]),
+                (12, 1.75 * p, nz - sum(r) - r_pml), (13, p, r_pml)], 1.0 / 3.0, ['sio2', 'poly_si', 'si_cubic']
+
+    def defaults(self) -> np.ndarray:
+        return np.array([1.085, self._layers()[0][0][1]])
+
+    def _cell(self, v):
+        p0 = 1.085
+        layers, ratio, _ = self._layers()
+        bands = [cells.Band(tag, v[1] if i == 0 else t, rows) for i, (tag, t, rows) in enumerate(layers)]
+        return cells.hex_slab_cell(v[0], self.nx, self.ny, bands, cells.Band(cells.HEX_TAG_ELECTRODE, 0.08 * p0, 1),
+                                   0.5 * p0, metal_ratio=ratio)
+
+    def build(self, v):
+        v = np.asarray(v, dtype=float)
+        cell = self._cell(v)
+        piezo = mt.rotate(self.crystal, self.euler)
+        mats = [piezo, mt.al()] + [getattr(mt, m)() for m in self._layers()[2]]
+        idx = np.array([cell.tag_map[int(t)] for t in cell.hex_tag], dtype=np.int64)
+        pos_m = cell.POS * 1e-6
+        bottom = float(pos_m[:, 2].min())
+        pml = [cases.PML(tag=cell.pml_tag, kind='z', za=cell.pml_top_um * 1e-6, zp=bottom)]
+        bc = cases.bc_periodic_3d(cell.sets, pos_m, pos_m.shape[0])
+        return cases.HexCase('hex_param', cell, pos_m, cell.HEXAS27, mats, idx, pml, bc, np.linspace(1.6e9, 2.0e9, 5),
+                             dict(seed=self.seed, nx=self.nx, ny=self.ny, nz=self.nz))
+
+    def engine(self, case, device=0):
+        return cases.hex_engine_for(case, device=device)
+
+    @staticmethod
+    def y11(w, Q, V, case):
+        """+i w Q / V / aperture (src/sawsim/hex_solver.py:103)."""
+        return 1j * w * Q / V / (case.cell.aperture_um * 1e-6)
+
+    def seeds(self, v):
+        v = np.asarray(v, dtype=float)
+        out = []
+        for i in range(len(self.names)):
+            h = 0.05 * v[i]
+            vp, vm = v.copy(), v.copy()
+            vp[i] += h
+            vm[i] -= h
+            cp, cm = self._cell(vp), self._cell(vm)
+            s = dict(dpos=(cp.POS - cm.POS) * 1e-6 / (2 * h))
+            zb = lambda c: np.array([[0.0, 0.0, c.pml_bottom_um * 1e-6]])     # noqa: E731
+            zt = lambda c: np.array([[0.0, 0.0, c.pml_top_um * 1e-6]])        # noqa: E731
+            s['douter'] = (zb(cp) - zb(cm)) / (2 * h)
+            s['dinner'] = (zt(cp) - zt(cm)) / (2 * h)
             out.append(s)
         return out

@@ -86,3 +86,41 @@ def test_torch_backward(jac):
     loss.backward()
     expect = (2 * np.conj(Y)[:, None] * dY).real.sum(0)
     assert np.allclose(p.grad.numpy(), expect, rtol=1e-10, atol=0)
+
+
+@pytest.fixture(scope='module')
+def hex_jac(built_lib):
+    from sawsim_b200.autograd import y11_and_jacobian
+    model = params.HexModel(8, 2, 12, stack='double')
+    v = model.defaults()
+    f = np.linspace(1.6e9, 2.0e9, 4)
+    Y, dY, st = y11_and_jacobian(model, v, f, 'fp64')
+    assert (st == 0).all()
+    return model, v, f, Y, dY
+
+
+def _y_hex(model, v, f):
+    case = model.build(v)
+    eng = model.engine(case)
+    try:
+        Q, st, _ = eng.charges(2 * np.pi * f, 1.0, 'fp64')
+    finally:
+        eng.close()
+    return model.y11(2 * np.pi * f, Q, 1.0, case)
+
+
+@pytest.mark.parametrize('i', [0, 1], ids=['pitch_um', 't_film_um'])
+def test_hex_adjoint_matches_finite_differences(hex_jac, i):
+    """Hex27 slab (config-5 parameters: pitch and film thickness): the adjoint
+    Jacobian of Y11 = +i w Q / V / aperture against central differences."""
+    model, v, f, Y, dY = hex_jac
+    fd = _fd(_y_hex, model, v, f, i)
+    assert np.max(np.abs(dY[:, i] - fd)) <= 1e-4 * np.max(np.abs(fd))
+
+
+def test_hex_mixed_gradient_matches_fp64(hex_jac):
+    from sawsim_b200.autograd import y11_and_jacobian
+    model, v, f, Y, dY = hex_jac
+    Y32, dY32, st = y11_and_jacobian(model, v, f, 'mixed')
+    assert (st == 0).all()
+    assert np.max(np.abs(dY32 - dY)) <= 1e-6 * np.max(np.abs(dY))
