@@ -199,6 +199,19 @@ def workload_name(c):
             f'{c.freqs[0] / 1e9:.1f}-{c.freqs[-1] / 1e9:.1f} GHz, seed {i["seed"]}')
 
 
+def schur_kernel_name(s, used):
+    """The Schur-update kernels the plan's autotuner picked, with their level counts."""
+    if used == 'mixed':
+        names = ['tc::front_tc_gemm_kernel (tcgen05 3xTF32, one CTA per tile)',
+                 'tc::front_tc_gemm_persistent (tcgen05 3xTF32, warp-specialised)']
+    else:
+        names = ['front_gemm_kernel<double> SIMT 128x64', 'front_gemm_kernel<double> SIMT 64x64',
+                 'front_dmma_kernel<2,2> (FP64 DMMA 64x64)']
+    keys = ['schur_tile_simt128', 'schur_tile_simt64', 'schur_tile_dmma']
+    parts = [f'{n} on {int(s[k])} levels' for n, k in zip(names, keys) if s.get(k, 0) > 0]
+    return 'Schur update F22 -= F21 F12: ' + ', '.join(parts)
+
+
 def b200_arm(a, rank, world, local):
     import torch
     import torch.distributed as dist
@@ -305,9 +318,7 @@ def b200_arm(a, rank, world, local):
                     e2e=dict(value=world * nf * a.steps / wall, unit='points/s', h2d_bytes_per_step=8 * nf,
                              d2h_bytes_per_step=16 * nf + 8 * nf),
                     gpu_launches=launches,
-                    roofline=dict(kernel=('front_tc_gemm_kernel (tcgen05 3xTF32 Schur update F22 -= F21 F12)'
-                                          if used == 'mixed' else
-                                          'front_gemm_kernel<double> (Schur update F22 -= F21 F12)'),
+                    roofline=dict(kernel=schur_kernel_name(s, used),
                                   bound='tensor',
                                   achieved=achieved, peak=peak, unit='TFLOP/s',
                                   frac=(achieved / peak) if achieved else None, traffic=None, peak_note=peak_note,

@@ -190,17 +190,21 @@ __device__ int block_argmax(int lo, int hi, Get get, T *sv, int *si) {
 // Fronts small enough for shared memory: one CTA per (front, frequency) assembles
 // the front (arrowhead entries of A'(w) + extend-add of the children's update
 // blocks), eliminates its k pivots with row pivoting restricted to the k
-// fully-summed rows, and writes factors and update block to the arena.
+// fully-summed rows, and writes factors and update block to the arena.  Every
+// row-wise loop is one warp per row with the lanes along the columns (no
+// per-element index division; conflict-free shared accesses).
+constexpr int kSmallThreads = 512;
 template <class T>
-__global__ void __launch_bounds__(256) front_small_kernel(FrontArgs<T> a) {
+__global__ void __launch_bounds__(kSmallThreads) front_small_kernel(FrontArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T> *F = reinterpret_cast<cplx<T> *>(smem_raw);
-  __shared__ T s_v[8];
-  __shared__ int s_i[8];
+  __shared__ T s_v[kSmallThreads / 32];
+  __shared__ int s_i[kSmallThreads / 32];
   __shared__ cplx<T> s_pivot;
   const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
   const int k = a.k[f], m = a.m[f], ld = a.ld[f];
   const double w = a.omega[fq];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   cplx<T> *arena = a.arena + (int64_t)fq * a.stride;
   for (int t = threadIdx.x; t < m * m; t += blockDim.x) F[t] = cplx<T>{0, 0};
   __syncthreads();
@@ -214,22 +218,24 @@ __global__ void __launch_bounds__(256) front_small_kernel(FrontArgs<T> a) {
     const int kc = a.k[ch], nn = a.m[ch] - kc, ldc = a.ld[ch];
     const cplx<T> *CB = arena + a.off[ch] + (int64_t)kc * ldc + kc;
     const int *rel = a.relpos + a.relpos_ptr[ch];
-    for (int t = threadIdx.x; t < nn * nn; t += blockDim.x) {
-      const int i = t / nn, j = t - i * nn;
-      cplx<T> &d = F[rel[i] * m + rel[j]];
-      d = d + CB[(int64_t)i * ldc + j];
+    for (int i = wid; i < nn; i += nw) {
+      cplx<T> *d = F + rel[i] * m;
+      const cplx<T> *src = CB + (int64_t)i * ldc;
+      for (int j = lane; j < nn; j += 32) d[rel[j]] = d[rel[j]] + src[j];
     }
     __syncthreads();
   }
   int *piv = a.piv + (int64_t)fq * a.n + a.p0[f];
   for (int j = 0; j < k; ++j) {
     const int p = block_argmax<T>(j, k, [&](int r) { return F[r * m + j]; }, s_v, s_i);
-    if (p != j)
+    if (p != j) {   // p is the same in every thread
       for (int c = threadIdx.x; c < m; c += blockDim.x) {
         const cplx<T> t = F[j * m + c];
         F[j * m + c] = F[p * m + c];
         F[p * m + c] = t;
       }
+      __syncthreads();   // the swapped pivot row is read below
+    }
     if (threadIdx.x == 0) {
       piv[j] = p;
       cplx<T> pv = F[j * m + j];
@@ -242,43 +248,49 @@ __global__ void __launch_bounds__(256) front_small_kernel(FrontArgs<T> a) {
     }
     __syncthreads();
     const cplx<T> inv = cdiv(cplx<T>{1, 0}, s_pivot);
-    for (int r = j + 1 + threadIdx.x; r < m; r += blockDim.x) F[r * m + j] = cmul(F[r * m + j], inv);
-    __syncthreads();
-    const int nr = m - j - 1;
-    for (int t = threadIdx.x; t < nr * nr; t += blockDim.x) {
-      const int r = j + 1 + t / nr, c = j + 1 + t % nr;
-      F[r * m + c] = cfms(F[r * m + c], F[r * m + j], F[j * m + c]);
+    // rows below the pivot: multiplier, then the rank-1 update of the row
+    const cplx<T> *prow = F + j * m;
+    for (int r = j + 1 + wid; r < m; r += nw) {
+      cplx<T> *row = F + r * m;
+      const cplx<T> l = cmul(row[j], inv);
+      for (int c = j + 1 + lane; c < m; c += 32) row[c] = cfms(row[c], l, prow[c]);
+      __syncwarp();
+      if (lane == 0) row[j] = l;
     }
     __syncthreads();
   }
   cplx<T> *G = arena + a.off[f];
-  for (int t = threadIdx.x; t < m * m; t += blockDim.x) G[(int64_t)(t / m) * ld + t % m] = F[t];
+  for (int r = wid; r < m; r += nw)
+    for (int c = lane; c < m; c += 32) G[(int64_t)r * ld + c] = F[r * m + c];
 }
 
 }  // namespace ss
 
 namespace ss {
 
-constexpr int kRowChunk = 32;   // rows per CTA in the large-front assembly
 constexpr int kPanel = 32;      // panel width of the blocked partial LU
 
-// Large fronts, assembly in global memory: CTA (front, frequency, row chunk)
-// zeroes its rows, drops in the arrowhead entries of those rows, then adds the
-// children's update rows that map into them (children in order: deterministic).
+// Large fronts: CTA (front, frequency, block of `rows` rows) assembles its rows in
+// shared memory -- zeroes, arrowhead entries of A'(w), then the children's update
+// rows that map into them (children in order: deterministic) -- and writes each
+// row to the arena once, coalesced.  Per element: one arena write, the child
+// update blocks read once.
+constexpr int kAsmSmemTarget = 64 * 1024;   // shared bytes per CTA (several CTAs per SM)
+constexpr int kAsmSmemMax = 200 * 1024;     // wider fronts use front_assemble_wide_kernel
 template <class T>
-__global__ void __launch_bounds__(256) front_assemble_large_kernel(FrontArgs<T> a) {
+__global__ void __launch_bounds__(256) front_assemble_large_kernel(FrontArgs<T> a, int rows) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T> *S = reinterpret_cast<cplx<T> *>(smem_raw);
   const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
-  const int k = a.k[f], m = a.m[f], ld = a.ld[f];
-  const int r0 = blockIdx.z * kRowChunk;
+  const int m = a.m[f], ld = a.ld[f];
+  const int r0 = blockIdx.z * rows;
   if (r0 >= m) return;
-  const int r1 = min(m, r0 + kRowChunk);
+  const int r1 = min(m, r0 + rows);
   const double w = a.omega[fq];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   cplx<T> *arena = a.arena + (int64_t)fq * a.stride;
   cplx<T> *F = arena + a.off[f];
-  for (int t = threadIdx.x; t < (r1 - r0) * m; t += blockDim.x) {
-    const int r = r0 + t / m, c = t % m;
-    F[(int64_t)r * ld + c] = cplx<T>{0, 0};
-  }
+  for (int t = threadIdx.x; t < (r1 - r0) * m; t += blockDim.x) S[t] = cplx<T>{0, 0};
   __syncthreads();
   {
     // arrow entries are sorted by row position
@@ -294,8 +306,10 @@ __global__ void __launch_bounds__(256) front_assemble_large_kernel(FrontArgs<T> 
       int64_t mid = (b + e) / 2;
       if (a.arrow_pos[mid] / ld < r1) b = mid + 1; else e = mid;
     }
-    for (int64_t q = q0 + threadIdx.x; q < b; q += blockDim.x)
-      F[a.arrow_pos[q]] = to_t<T>(a_entry(a.Kc, a.Mc, a.Dc, a.arrow_slot[q], w, a.beta));
+    for (int64_t q = q0 + threadIdx.x; q < b; q += blockDim.x) {
+      const int pos = a.arrow_pos[q];
+      S[(pos / ld - r0) * m + pos % ld] = to_t<T>(a_entry(a.Kc, a.Mc, a.Dc, a.arrow_slot[q], w, a.beta));
+    }
   }
   __syncthreads();
   for (int64_t cc = a.child_ptr[f]; cc < a.child_ptr[f + 1]; ++cc) {
@@ -309,10 +323,54 @@ __global__ void __launch_bounds__(256) front_assemble_large_kernel(FrontArgs<T> 
     while (b < e) { int mid = (b + e) / 2; if (rel[mid] < r1) b = mid + 1; else e = mid; }
     const int i1 = b;
     const cplx<T> *CB = arena + a.off[ch] + (int64_t)kc * ldc + kc;
-    for (int t = threadIdx.x; t < (i1 - i0) * nn; t += blockDim.x) {
-      const int i = i0 + t / nn, j = t % nn;
-      cplx<T> &d = F[(int64_t)rel[i] * ld + rel[j]];
-      d = d + CB[(int64_t)i * ldc + j];
+    for (int i = i0 + wid; i < i1; i += nw) {
+      cplx<T> *d = S + (rel[i] - r0) * m;
+      const cplx<T> *src = CB + (int64_t)i * ldc;
+      for (int j = lane; j < nn; j += 32) d[rel[j]] = d[rel[j]] + src[j];
+    }
+    __syncthreads();
+  }
+  for (int r = r0 + wid; r < r1; r += nw) {
+    const cplx<T> *src = S + (r - r0) * m;
+    cplx<T> *dst = F + (int64_t)r * ld;
+    for (int c = lane; c < m; c += 32) dst[c] = src[c];
+  }
+}
+
+// Fronts wider than the shared-memory rows allow: the same assembly directly in
+// the arena (rows of 32 per CTA).
+constexpr int kRowChunk = 32;
+template <class T>
+__global__ void __launch_bounds__(256) front_assemble_wide_kernel(FrontArgs<T> a) {
+  const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
+  const int m = a.m[f], ld = a.ld[f];
+  const int r0 = blockIdx.z * kRowChunk;
+  if (r0 >= m) return;
+  const int r1 = min(m, r0 + kRowChunk);
+  const double w = a.omega[fq];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  cplx<T> *arena = a.arena + (int64_t)fq * a.stride;
+  cplx<T> *F = arena + a.off[f];
+  for (int r = r0 + wid; r < r1; r += nw)
+    for (int c = lane; c < m; c += 32) F[(int64_t)r * ld + c] = cplx<T>{0, 0};
+  __syncthreads();
+  for (int64_t q = a.arrow_ptr[f] + threadIdx.x; q < a.arrow_ptr[f + 1]; q += blockDim.x) {
+    const int pos = a.arrow_pos[q];
+    const int r = pos / ld;
+    if (r >= r0 && r < r1) F[pos] = to_t<T>(a_entry(a.Kc, a.Mc, a.Dc, a.arrow_slot[q], w, a.beta));
+  }
+  __syncthreads();
+  for (int64_t cc = a.child_ptr[f]; cc < a.child_ptr[f + 1]; ++cc) {
+    const int ch = a.child[cc];
+    const int kc = a.k[ch], nn = a.m[ch] - kc, ldc = a.ld[ch];
+    const int *rel = a.relpos + a.relpos_ptr[ch];
+    const cplx<T> *CB = arena + a.off[ch] + (int64_t)kc * ldc + kc;
+    for (int i = wid; i < nn; i += nw) {
+      const int r = rel[i];
+      if (r < r0 || r >= r1) continue;
+      cplx<T> *d = F + (int64_t)r * ld;
+      const cplx<T> *src = CB + (int64_t)i * ldc;
+      for (int j = lane; j < nn; j += 32) d[rel[j]] = d[rel[j]] + src[j];
     }
     __syncthreads();
   }
@@ -399,6 +457,67 @@ __global__ void __launch_bounds__(256) front_panel_kernel(FrontArgs<T> a, int j0
     }
     __syncthreads();
   }
+}
+
+// The same panel LU with the panel block -- rows [j0, k) x columns [j0, j1) -- held
+// in shared memory (row stride kPanel + 1 complex: row and column walks are both
+// conflict-free); one warp per row for the multipliers and the rank-1 update.
+// Operation for operation the arithmetic of front_panel_kernel.
+constexpr int kPanelThreads = 512;
+constexpr int kPanelSmemMax = 224 * 1024;
+template <class T>
+__global__ void __launch_bounds__(kPanelThreads) front_panel_smem_kernel(FrontArgs<T> a, int j0) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T> *P = reinterpret_cast<cplx<T> *>(smem_raw);
+  constexpr int PS = kPanel + 1;
+  __shared__ T s_v[kPanelThreads / 32];
+  __shared__ int s_i[kPanelThreads / 32];
+  __shared__ cplx<T> s_pivot;
+  const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
+  const int k = a.k[f], ld = a.ld[f];
+  if (j0 >= k) return;
+  const int w = min(k, j0 + kPanel) - j0, R = k - j0;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  cplx<T> *F = a.arena + (int64_t)fq * a.stride + a.off[f] + (int64_t)j0 * ld + j0;
+  int *piv = a.piv + (int64_t)fq * a.n + a.p0[f] + j0;
+  for (int r = wid; r < R; r += nw)
+    if (lane < w) P[r * PS + lane] = F[(int64_t)r * ld + lane];
+  __syncthreads();
+  for (int j = 0; j < w; ++j) {
+    const int p = block_argmax<T>(j, R, [&](int r) { return P[r * PS + j]; }, s_v, s_i);
+    if (p != j) {   // p is the same in every thread
+      if (threadIdx.x < w) {
+        const cplx<T> t = P[j * PS + threadIdx.x];
+        P[j * PS + threadIdx.x] = P[p * PS + threadIdx.x];
+        P[p * PS + threadIdx.x] = t;
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      piv[j] = j0 + p;
+      cplx<T> pv = P[j * PS + j];
+      if (cabs1(pv) < a.tiny) {
+        pv = cplx<T>{a.tiny, (T)0};
+        P[j * PS + j] = pv;
+        atomicAdd(a.nperturb + fq, 1);
+      }
+      s_pivot = pv;
+    }
+    __syncthreads();
+    const cplx<T> inv = cdiv(cplx<T>{1, 0}, s_pivot);
+    const int c = j + 1 + lane;
+    const cplx<T> pc = c < w ? P[j * PS + c] : cplx<T>{0, 0};
+    for (int r = j + 1 + wid; r < R; r += nw) {
+      cplx<T> *row = P + r * PS;
+      const cplx<T> l = cmul(row[j], inv);
+      if (c < w) row[c] = cfms(row[c], l, pc);
+      __syncwarp();
+      if (lane == 0) row[j] = l;
+    }
+    __syncthreads();
+  }
+  for (int r = wid; r < R; r += nw)
+    if (lane < w) F[(int64_t)r * ld + lane] = P[r * PS + lane];
 }
 
 // mode 0: apply the panel's row swaps to every column outside it (one thread per
@@ -527,16 +646,24 @@ __global__ void __launch_bounds__(256) front_gemm_kernel(FrontArgs<T> a, const G
     }
     __syncthreads();
   }
+  // epilogue: per output row, all TN loads of C first, then the stores
 #pragma unroll
-  for (int i = 0; i < TM; ++i)
+  for (int i = 0; i < TM; ++i) {
+    const int r = tk.r0 + ty + TY * i;
+    const bool rok = r < tk.rhi;
+    cplx<T> *Fr = F + (int64_t)(rok ? r : tk.r0) * ld;
+    cplx<T> cv[TN];
 #pragma unroll
     for (int j = 0; j < TN; ++j) {
-      const int r = tk.r0 + ty + TY * i, c = tk.c0 + tx + TX * j;
-      if (r < tk.rhi && c < tk.chi) {
-        cplx<T> &d = F[(int64_t)r * ld + c];
-        d = d - acc[i][j];
-      }
+      const int c = tk.c0 + tx + TX * j;
+      cv[j] = (rok && c < tk.chi) ? Fr[c] : cplx<T>{0, 0};
     }
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+      const int c = tk.c0 + tx + TX * j;
+      if (rok && c < tk.chi) Fr[c] = cv[j] - acc[i][j];
+    }
+  }
 }
 
 // FP64 complex tile C -= A B on the FP64 tensor cores (DMMA, mma.sync m8n8k4 f64):
@@ -548,7 +675,12 @@ __global__ void __launch_bounds__(256) front_gemm_kernel(FrontArgs<T> a, const G
 // Fragments (PTX m8n8k4 .f64): A[g][t], B[t][g], C[g][2t + i] with g = lane / 4,
 // t = lane % 4.
 constexpr int kDmmaBK = 8;
-constexpr int kDmmaAS = kDmmaBK + 1;          // A row stride in complex (+1: conflict-free fragment reads)
+// shared layouts (complex): A rows of 8 with the halves of odd rows swapped
+// (column k stored at k ^ 4), B rows padded by 2 (32 bytes off a 128-byte line):
+// each 8-lane phase of a 16-byte fragment load then hits eight distinct 16-byte
+// slots (conflict-free)
+constexpr int kDmmaAS = kDmmaBK;
+__device__ __forceinline__ int dmma_acol(int r, int k) { return k ^ ((r & 1) << 2); }
 
 __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
@@ -560,11 +692,11 @@ __device__ __forceinline__ void cp_async16_cd(uint32_t dst, const void *src, uin
 }
 
 template <int WM, int WN>
-__global__ void __launch_bounds__(128) front_dmma_kernel(FrontArgs<double> a, const GemmTask *__restrict__ tasks) {
-  constexpr int kDmmaBM = 32 * WM, kDmmaBN = 32 * WN;
+__global__ void __launch_bounds__(128, 3) front_dmma_kernel(FrontArgs<double> a, const GemmTask *__restrict__ tasks) {
+  constexpr int kDmmaBM = 32 * WM, kDmmaBN = 32 * WN, kDmmaBS = kDmmaBN + 2;
   static_assert(WM * WN == 4, "four warps");
   __shared__ __align__(16) cd As[2][kDmmaBM * kDmmaAS];
-  __shared__ __align__(16) cd Bs[2][kDmmaBK * kDmmaBN];
+  __shared__ __align__(16) cd Bs[2][kDmmaBK * kDmmaBS];
   const GemmTask tk = tasks[blockIdx.x];
   const int fq = blockIdx.y;
   const int ld = a.ld[tk.f];
@@ -584,7 +716,7 @@ __global__ void __launch_bounds__(128) front_dmma_kernel(FrontArgs<double> a, co
       const int r = idx / kDmmaBK, k = idx % kDmmaBK;   // A: BM rows x 8
       const int gr = tk.r0 + r, gk = kb + k;
       const bool ok = gr < tk.rhi && gk < tk.kk1;
-      cp_async16_cd((uint32_t)__cvta_generic_to_shared(&As[buf][r * kDmmaAS + k]),
+      cp_async16_cd((uint32_t)__cvta_generic_to_shared(&As[buf][r * kDmmaAS + dmma_acol(r, k)]),
                     ok ? F + (int64_t)gr * ld + gk : F, ok ? 16u : 0u);
     }
 #pragma unroll
@@ -593,7 +725,7 @@ __global__ void __launch_bounds__(128) front_dmma_kernel(FrontArgs<double> a, co
       const int k = idx / kDmmaBN, c = idx % kDmmaBN;   // B: 8 rows x BN
       const int gk = kb + k, gc = tk.c0 + c;
       const bool ok = gk < tk.kk1 && gc < tk.chi;
-      cp_async16_cd((uint32_t)__cvta_generic_to_shared(&Bs[buf][k * kDmmaBN + c]),
+      cp_async16_cd((uint32_t)__cvta_generic_to_shared(&Bs[buf][k * kDmmaBS + c]),
                     ok ? F + (int64_t)gk * ld + gc : F, ok ? 16u : 0u);
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
@@ -611,40 +743,68 @@ __global__ void __launch_bounds__(128) front_dmma_kernel(FrontArgs<double> a, co
     __syncthreads();
 #pragma unroll
     for (int kk = 0; kk < kDmmaBK; kk += 4) {
-      cd av[4], bv[4];
+      cd av[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) av[i] = As[buf][(wm * 32 + i * 8 + g) * kDmmaAS + kk + t];
+      for (int i = 0; i < 4; ++i) {
+        const int ar = wm * 32 + i * 8 + g;
+        av[i] = As[buf][ar * kDmmaAS + dmma_acol(ar, kk + t)];
+      }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) bv[j] = Bs[buf][(kk + t) * kDmmaBN + wn * 32 + j * 8 + g];
+      for (int j = 0; j < 4; ++j) {
+        const cd bv = Bs[buf][(kk + t) * kDmmaBS + wn * 32 + j * 8 + g];
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          dmma(dr[i][j][0], dr[i][j][1], av[i].x, bv[j].x);
-          dmma(dr[i][j][0], dr[i][j][1], -av[i].y, bv[j].y);
-          dmma(di[i][j][0], di[i][j][1], av[i].x, bv[j].y);
-          dmma(di[i][j][0], di[i][j][1], av[i].y, bv[j].x);
+        for (int i = 0; i < 4; ++i) {
+          dmma(dr[i][j][0], dr[i][j][1], av[i].x, bv.x);
+          dmma(dr[i][j][0], dr[i][j][1], -av[i].y, bv.y);
+          dmma(di[i][j][0], di[i][j][1], av[i].x, bv.y);
+          dmma(di[i][j][0], di[i][j][1], av[i].y, bv.x);
         }
+      }
     }
     __syncthreads();
   }
+  // epilogue: per fragment row, all eight C loads first, then the stores (one
+  // memory round trip per row instead of one per element)
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 4; ++i) {
+    const int r = tk.r0 + wm * 32 + i * 8 + g;
+    const bool rok = r < tk.rhi;
+    cd *Fr = F + (int64_t)(rok ? r : tk.r0) * ld;
+    cd cv[4][2];
 #pragma unroll
     for (int j = 0; j < 4; ++j)
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
-        const int r = tk.r0 + wm * 32 + i * 8 + g, c = tk.c0 + wn * 32 + j * 8 + 2 * t + e;
-        if (r < tk.rhi && c < tk.chi) {
-          cd &d = F[(int64_t)r * ld + c];
-          d = d - cd{dr[i][j][e], di[i][j][e]};
-        }
+        const int c = tk.c0 + wn * 32 + j * 8 + 2 * t + e;
+        cv[j][e] = (rok && c < tk.chi) ? Fr[c] : cd{0.0, 0.0};
       }
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int c = tk.c0 + wn * 32 + j * 8 + 2 * t + e;
+        if (rok && c < tk.chi) Fr[c] = cv[j][e] - cd{dr[i][j][e], di[i][j][e]};
+      }
+  }
 }
 
 }  // namespace ss
 
 namespace ss {
+
+// Triangular solves stage each 32x32 diagonal block in shared memory (row stride
+// 33: row and column walks conflict-free) with one coalesced pass of all threads,
+// so that warp 0's sequential block solve reads shared memory instead of making a
+// chain of dependent global loads.
+constexpr int kDiagS = 33;
+constexpr int kDiagElems = 32 * kDiagS;
+template <class T>
+__device__ __forceinline__ void stage_diag(cplx<T> *D, const cplx<T> *F, int ld, int jb, int bw) {
+  for (int t = threadIdx.x; t < bw * 32; t += blockDim.x) {
+    const int i = t >> 5, j = t & 31;
+    if (j < bw) D[i * kDiagS + j] = F[(int64_t)(jb + i) * ld + jb + j];
+  }
+}
 
 // Forward substitution for one level: CTA per (front, frequency).  v = b[pivots] +
 // children's update vectors; apply the front's row swaps; solve L11; the update
@@ -654,7 +814,8 @@ __global__ void __launch_bounds__(256) front_fwd_kernel(FrontArgs<T> a, const cd
                                                         cd *__restrict__ x, cplx<T> *__restrict__ wv,
                                                         int64_t wstride) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  cplx<T> *v = reinterpret_cast<cplx<T> *>(smem_raw);
+  cplx<T> *D = reinterpret_cast<cplx<T> *>(smem_raw);
+  cplx<T> *v = D + kDiagElems;
   const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
   const int k = a.k[f], m = a.m[f], ld = a.ld[f];
   const cplx<T> *F = a.arena + (int64_t)fq * a.stride + a.off[f];
@@ -688,13 +849,15 @@ __global__ void __launch_bounds__(256) front_fwd_kernel(FrontArgs<T> a, const cd
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int jb = 0; jb < k; jb += 32) {
     const int je = min(k, jb + 32), bw = je - jb;
+    stage_diag(D, F, ld, jb, bw);
+    __syncthreads();
     if (wid == 0) {
       cplx<T> x = lane < bw ? v[jb + lane] : cplx<T>{0, 0};
       for (int t = 0; t < bw - 1; ++t) {
         cplx<T> xt;
         xt.x = __shfl_sync(0xffffffffu, x.x, t);
         xt.y = __shfl_sync(0xffffffffu, x.y, t);
-        if (lane > t && lane < bw) x = cfms(x, F[(int64_t)(jb + lane) * ld + jb + t], xt);
+        if (lane > t && lane < bw) x = cfms(x, D[lane * kDiagS + t], xt);
       }
       if (lane < bw) v[jb + lane] = x;
     }
@@ -783,14 +946,13 @@ __global__ void __launch_bounds__(256) front_bwd_u12_kernel(FrontArgs<T> a, cd *
 template <class T>
 __global__ void __launch_bounds__(256) front_bwd_kernel(FrontArgs<T> a, cd *__restrict__ x) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  cplx<T> *z = reinterpret_cast<cplx<T> *>(smem_raw);
+  cplx<T> *D = reinterpret_cast<cplx<T> *>(smem_raw);
+  cplx<T> *z = D + kDiagElems;
   const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
-  const int k = a.k[f], m = a.m[f], ld = a.ld[f];
+  const int k = a.k[f], ld = a.ld[f];
   const cplx<T> *F = a.arena + (int64_t)fq * a.stride + a.off[f];
   const int64_t p0 = a.p0[f];
   cd *xf = x + (int64_t)fq * a.n;
-  const int64_t *rows = a.rows + a.rows_ptr[f];
-  (void)rows;
   for (int i = threadIdx.x; i < k; i += blockDim.x) z[i] = to_t<T>(xf[p0 + i]);   // y - U12 x_U
   __syncthreads();
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -798,14 +960,16 @@ __global__ void __launch_bounds__(256) front_bwd_kernel(FrontArgs<T> a, cd *__re
   // then every warp updates the rows above it
   for (int je = k; je > 0; je -= 32) {
     const int jb = max(0, je - 32), bw = je - jb;
+    stage_diag(D, F, ld, jb, bw);
+    __syncthreads();
     if (wid == 0) {
       cplx<T> x = lane < bw ? z[jb + lane] : cplx<T>{0, 0};
       for (int t = bw - 1; t >= 0; --t) {
-        if (lane == t) x = cdiv(x, F[(int64_t)(jb + t) * ld + jb + t]);
+        if (lane == t) x = cdiv(x, D[t * kDiagS + t]);
         cplx<T> xt;
         xt.x = __shfl_sync(0xffffffffu, x.x, t);
         xt.y = __shfl_sync(0xffffffffu, x.y, t);
-        if (lane < t) x = cfms(x, F[(int64_t)(jb + lane) * ld + jb + t], xt);
+        if (lane < t) x = cfms(x, D[lane * kDiagS + t], xt);
       }
       if (lane < bw) z[jb + lane] = x;
     }
@@ -838,7 +1002,8 @@ __global__ void __launch_bounds__(256) front_tfwd_kernel(FrontArgs<T> a, const c
                                                          cd *__restrict__ x, cplx<T> *__restrict__ wv,
                                                          int64_t wstride) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  cplx<T> *v = reinterpret_cast<cplx<T> *>(smem_raw);
+  cplx<T> *D = reinterpret_cast<cplx<T> *>(smem_raw);
+  cplx<T> *v = D + kDiagElems;
   const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
   const int k = a.k[f], m = a.m[f], ld = a.ld[f];
   const cplx<T> *F = a.arena + (int64_t)fq * a.stride + a.off[f];
@@ -860,14 +1025,16 @@ __global__ void __launch_bounds__(256) front_tfwd_kernel(FrontArgs<T> a, const c
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (int jb = 0; jb < k; jb += 32) {
     const int je = min(k, jb + 32), bw = je - jb;
+    stage_diag(D, F, ld, jb, bw);
+    __syncthreads();
     if (wid == 0) {
       cplx<T> xv = lane < bw ? v[jb + lane] : cplx<T>{0, 0};
       for (int t = 0; t < bw; ++t) {
-        if (lane == t) xv = cdiv(xv, F[(int64_t)(jb + t) * ld + jb + t]);
+        if (lane == t) xv = cdiv(xv, D[t * kDiagS + t]);
         cplx<T> xt;
         xt.x = __shfl_sync(0xffffffffu, xv.x, t);
         xt.y = __shfl_sync(0xffffffffu, xv.y, t);
-        if (lane > t && lane < bw) xv = cfms(xv, F[(int64_t)(jb + t) * ld + jb + lane], xt);
+        if (lane > t && lane < bw) xv = cfms(xv, D[t * kDiagS + lane], xt);
       }
       if (lane < bw) v[jb + lane] = xv;
     }
@@ -938,7 +1105,8 @@ __global__ void __launch_bounds__(256) front_tbwd_l21_kernel(FrontArgs<T> a, cd 
 template <class T>
 __global__ void __launch_bounds__(256) front_tbwd_kernel(FrontArgs<T> a, cd *__restrict__ x) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  cplx<T> *z = reinterpret_cast<cplx<T> *>(smem_raw);
+  cplx<T> *D = reinterpret_cast<cplx<T> *>(smem_raw);
+  cplx<T> *z = D + kDiagElems;
   const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
   const int k = a.k[f], ld = a.ld[f];
   const cplx<T> *F = a.arena + (int64_t)fq * a.stride + a.off[f];
@@ -949,13 +1117,15 @@ __global__ void __launch_bounds__(256) front_tbwd_kernel(FrontArgs<T> a, cd *__r
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (int je = k; je > 0; je -= 32) {
     const int jb = max(0, je - 32), bw = je - jb;
+    stage_diag(D, F, ld, jb, bw);
+    __syncthreads();
     if (wid == 0) {
       cplx<T> xv = lane < bw ? z[jb + lane] : cplx<T>{0, 0};
       for (int t = bw - 1; t > 0; --t) {
         cplx<T> xt;
         xt.x = __shfl_sync(0xffffffffu, xv.x, t);
         xt.y = __shfl_sync(0xffffffffu, xv.y, t);
-        if (lane < t) xv = cfms(xv, F[(int64_t)(jb + t) * ld + jb + lane], xt);
+        if (lane < t) xv = cfms(xv, D[t * kDiagS + lane], xt);
       }
       if (lane < bw) z[jb + lane] = xv;
     }
@@ -1053,6 +1223,7 @@ struct Plan {
   std::vector<int> small_maxm;             // per level max m among small fronts
   std::vector<int> nsteps;                 // per level panel steps of the large fronts
   std::vector<int> maxm_large;             // per level
+  std::vector<int> maxk_large;             // per level max k among large fronts
   std::vector<int64_t> step_ptr;           // per (level, step): tasks of that step (flattened)
   std::vector<int64_t> level_step0;        // first (level, step) index of level l
   std::vector<int64_t> schur_ptr;          // per level: Schur tasks
@@ -1135,6 +1306,7 @@ Plan *build_plan(Handle &h, int small_m, bool tensor_schur) {
     P->large_ptr.push_back((int)P->fronts_large.size());
     P->small_maxm.push_back(mm);
     P->maxm_large.push_back(ml);
+    P->maxk_large.push_back(kmax);
     const int ns = (kmax + kPanel - 1) / kPanel;
     P->nsteps.push_back(ns);
     P->level_step0.push_back((int64_t)P->step_ptr.size() - 1);
@@ -1297,7 +1469,14 @@ struct SweepOpts {
 };
 
 template <class T>
-static int small_limit() { return sizeof(T) == 8 ? 96 : 128; }  // cd: 96^2*16, cf: 128^2*8 bytes
+static int small_limit() { return sizeof(T) == 8 ? 112 : 128; }  // cd: 112^2*16, cf: 128^2*8 bytes
+// rows per CTA of the shared-memory front assembly for fronts up to m wide (0: too wide)
+template <class T>
+static int asm_rows(int m) {
+  const int row = m * (int)sizeof(cplx<T>);
+  if (row > kAsmSmemMax) return 0;
+  return std::max(1, std::min(32, kAsmSmemTarget / row));
+}
 
 // equilibration at angular frequency w (Ruiz, 3 sweeps)
 static int equilibrate(Handle &h, double w) {
@@ -1347,6 +1526,7 @@ static int equilibrate(Handle &h, double w) {
 
 template <class T>
 struct Sweeper {
+  static constexpr size_t kDiagBytes = (size_t)kDiagElems * sizeof(cplx<T>);
   Handle &h;
   Plan &P;
   FrontArgs<T> a{};
@@ -1584,7 +1764,7 @@ struct Sweeper {
         FrontArgs<T> b = a;
         b.fronts = P.d_small.as<int>() + P.small_ptr[l];
         const int mm = P.small_maxm[l];
-        front_small_kernel<T><<<dim3(ns, nb), 256, (size_t)mm * mm * sizeof(cplx<T>), h.stream>>>(b);
+        front_small_kernel<T><<<dim3(ns, nb), kSmallThreads, (size_t)mm * mm * sizeof(cplx<T>), h.stream>>>(b);
         ++launches;
       }
       const int nl = P.large_ptr[l + 1] - P.large_ptr[l];
@@ -1592,7 +1772,12 @@ struct Sweeper {
       FrontArgs<T> b = a;
       b.fronts = P.d_large.as<int>() + P.large_ptr[l];
       const int ml = P.maxm_large[l];
-      front_assemble_large_kernel<T><<<dim3(nl, nb, (ml + kRowChunk - 1) / kRowChunk), 256, 0, h.stream>>>(b);
+      const int rows = asm_rows<T>(ml);
+      if (rows > 0)
+        front_assemble_large_kernel<T><<<dim3(nl, nb, (ml + rows - 1) / rows), 256,
+                                         (size_t)rows * ml * sizeof(cplx<T>), h.stream>>>(b, rows);
+      else
+        front_assemble_wide_kernel<T><<<dim3(nl, nb, (ml + kRowChunk - 1) / kRowChunk), 256, 0, h.stream>>>(b);
       ++launches;
       const GemmTask *tasks = P.d_tasks.as<GemmTask>();
       const unsigned zc = (unsigned)((ml + 255) / 256);
@@ -1604,7 +1789,11 @@ struct Sweeper {
           panel_gemm(b, q, 0, nb);
           ++launches;
         }
-        front_panel_kernel<T><<<dim3(nl, nb), 256, 0, h.stream>>>(b, j0);
+        const size_t psm = (size_t)std::max(0, P.maxk_large[l] - j0) * (kPanel + 1) * sizeof(cplx<T>);
+        if (psm <= (size_t)kPanelSmemMax)
+          front_panel_smem_kernel<T><<<dim3(nl, nb), kPanelThreads, psm, h.stream>>>(b, j0);
+        else
+          front_panel_kernel<T><<<dim3(nl, nb), 256, 0, h.stream>>>(b, j0);
         front_l21_kernel<T><<<dim3(nl, nb, zc), 256, 0, h.stream>>>(b, j0);
         front_swap_trsm_kernel<T><<<dim3(nl, nb, zc), 256, 0, h.stream>>>(b, j0, 0);
         if (g2 > g1) {   // U row block <- earlier pivots
@@ -1646,7 +1835,7 @@ struct Sweeper {
       FrontArgs<T> c = a;
       c.fronts = h.d_level_fronts.as<int>() + S.level_ptr[l];
       const int nf = (int)(S.level_ptr[l + 1] - S.level_ptr[l]);
-      front_fwd_kernel<T><<<dim3(nf, nb), 256, sm, h.stream>>>(c, b, x, wv, wstride);
+      front_fwd_kernel<T><<<dim3(nf, nb), 256, sm + kDiagBytes, h.stream>>>(c, b, x, wv, wstride);
       ++launches;
       if (P.lvl_maxu[l] > 0) {
         const unsigned z = (unsigned)((P.lvl_maxu[l] + kSolveRows - 1) / kSolveRows);
@@ -1663,7 +1852,7 @@ struct Sweeper {
         front_bwd_u12_kernel<T><<<dim3(nf, nb, z), 256, (size_t)P.lvl_maxu[l] * sizeof(cplx<T>), h.stream>>>(c, x);
         ++launches;
       }
-      front_bwd_kernel<T><<<dim3(nf, nb), 256, smk, h.stream>>>(c, x);
+      front_bwd_kernel<T><<<dim3(nf, nb), 256, smk + kDiagBytes, h.stream>>>(c, x);
       ++launches;
     }
     SS_CK(cudaGetLastError());
@@ -1678,7 +1867,7 @@ struct Sweeper {
       FrontArgs<T> c = a;
       c.fronts = h.d_level_fronts.as<int>() + S.level_ptr[l];
       const int nf = (int)(S.level_ptr[l + 1] - S.level_ptr[l]);
-      front_tfwd_kernel<T><<<dim3(nf, nb), 256, sm, h.stream>>>(c, cvec, mu, wv, wstride);
+      front_tfwd_kernel<T><<<dim3(nf, nb), 256, sm + kDiagBytes, h.stream>>>(c, cvec, mu, wv, wstride);
       ++launches;
       if (P.lvl_maxu[l] > 0) {
         const unsigned z = (unsigned)((P.lvl_maxu[l] + 255) / 256);
@@ -1695,7 +1884,7 @@ struct Sweeper {
         front_tbwd_l21_kernel<T><<<dim3(nf, nb, z), 256, (size_t)P.lvl_maxu[l] * sizeof(cplx<T>), h.stream>>>(c, mu);
         ++launches;
       }
-      front_tbwd_kernel<T><<<dim3(nf, nb), 256, smk, h.stream>>>(c, mu);
+      front_tbwd_kernel<T><<<dim3(nf, nb), 256, smk + kDiagBytes, h.stream>>>(c, mu);
       ++launches;
     }
     SS_CK(cudaGetLastError());
@@ -1742,19 +1931,27 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
     SS_CK(dupload(P->d_tasks, P->tasks));
     SS_CK(cudaFuncSetAttribute(front_small_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                small_limit<T>() * small_limit<T>() * (int)sizeof(cplx<T>)));
+    SS_CK(cudaFuncSetAttribute(front_assemble_large_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               kAsmSmemMax));
+    SS_CK(cudaFuncSetAttribute(front_panel_smem_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               kPanelSmemMax));
     SS_CK(cudaFuncSetAttribute(tc::front_tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                tc::SMEM_BYTES));
     SS_CK(cudaFuncSetAttribute(tc::front_tc_gemm_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                tc::SMEM_BYTES));
     // solve kernels stage a whole front vector in shared memory
+    // (the four triangular kernels also hold one staged 32x32 diagonal block)
     const int vec = (int)std::min<int64_t>(227 * 1024, (int64_t)S.max_m * (int64_t)sizeof(cplx<T>));
+    const int vecd = (int)std::min<int64_t>(227 * 1024, vec + (int64_t)kDiagElems * sizeof(cplx<T>));
+    if (vecd > 48 * 1024) {
+      SS_CK(cudaFuncSetAttribute(front_fwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vecd));
+      SS_CK(cudaFuncSetAttribute(front_tfwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vecd));
+      SS_CK(cudaFuncSetAttribute(front_bwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vecd));
+      SS_CK(cudaFuncSetAttribute(front_tbwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vecd));
+    }
     if (vec > 48 * 1024) {
-      SS_CK(cudaFuncSetAttribute(front_fwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vec));
-      SS_CK(cudaFuncSetAttribute(front_tfwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vec));
       SS_CK(cudaFuncSetAttribute(front_fwd_l21_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vec));
       SS_CK(cudaFuncSetAttribute(front_tfwd_u12_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vec));
-      SS_CK(cudaFuncSetAttribute(front_bwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vec));
-      SS_CK(cudaFuncSetAttribute(front_tbwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vec));
       SS_CK(cudaFuncSetAttribute(front_bwd_u12_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vec));
       SS_CK(cudaFuncSetAttribute(front_tbwd_l21_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vec));
     }
@@ -2031,6 +2228,11 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
   h.st[15] = sw.launches;
   h.st[20] = h.st[21] = h.st[22] = 0;
   h.st[23] = P.panel_dmma ? 1.0 : 0.0;
+  h.st[24] = P.panel_ms[0];
+  h.st[25] = P.panel_ms[1];
+  h.st[26] = (double)P.fronts_small.size();
+  h.st[27] = 0;
+  for (float t : P.tune_ms) h.st[27] += t;
   for (size_t l = 0; l < P.pick.size(); ++l)
     if (P.schur_ptr[l + 1] > P.schur_ptr[l]) h.st[20 + P.pick[l]] += 1;
   {

@@ -308,7 +308,7 @@ extern "C" int ss_solve_fields(ss_handle *hp, double omega, double V, double *di
 
 extern "C" int ss_stats(const ss_handle *hp, double *out, int n) {
   if (!hp || !out || n < 0) return SS_EINVAL;
-  for (int i = 0; i < n && i < 24; ++i) out[i] = hp->h.st[i];
+  for (int i = 0; i < n && i < 28; ++i) out[i] = hp->h.st[i];
   return SS_OK;
 }
 

@@ -127,7 +127,7 @@ struct Handle {
   DBuf dKs, dMs, dDs;                    // equilibrated condensed values
   double scale_w = -1;                   // frequency the scaling was computed at
   // stats
-  double st[24] = {0};
+  double st[28] = {0};
 };
 
 // ---------------------------------------------------------------- kernels

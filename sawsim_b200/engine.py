@@ -155,13 +155,14 @@ class FrequencySolver:
 
     # ------------------------------------------------------------------ queries
     def stats(self) -> dict:
-        out = np.zeros(24)
-        self._h('ss_stats', L.ptr(out, C.c_double), 24)
+        out = np.zeros(28)
+        self._h('ss_stats', L.ptr(out, C.c_double), 28)
         keys = ['n_active', 'n_fronts', 'max_front', 'factor_flops_per_point', 'nnz_lu', 'analyze_s',
                 'assemble_ms', 'sweep_ms', 'factor_ms', 'solve_ms', 'chunk', 'schur_gemm_ms',
                 'schur_gemm_flops', 'levels', 'perturbed_pivots', 'launches', 'schur_launches',
                 'sweep_device_ms', 'refine_solves', 'precision_used', 'schur_tile_simt128', 'schur_tile_simt64',
-                'schur_tile_dmma', 'panel_gemm_dmma']
+                'schur_tile_dmma', 'panel_gemm_dmma', 'panel_tune_simt_ms', 'panel_tune_dmma_ms', 'small_fronts',
+                'schur_tune_ms']
         return dict(zip(keys, out.tolist()))
 
     @property
