@@ -200,7 +200,8 @@ __global__ void __launch_bounds__(kSmallThreads) front_small_kernel(FrontArgs<T>
   cplx<T> *F = reinterpret_cast<cplx<T> *>(smem_raw);
   __shared__ T s_v[kSmallThreads / 32];
   __shared__ int s_i[kSmallThreads / 32];
-  __shared__ cplx<T> s_pivot;
+  __shared__ T s_cv[2][kSmallThreads / 32];      // per-warp pivot candidates, by pivot parity
+  __shared__ int s_ci[2][kSmallThreads / 32];
   const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
   const int k = a.k[f], m = a.m[f], ld = a.ld[f];
   const double w = a.omega[fq];
@@ -225,9 +226,15 @@ __global__ void __launch_bounds__(kSmallThreads) front_small_kernel(FrontArgs<T>
     }
     __syncthreads();
   }
+  // One barrier per pivot: while a warp updates its rows for pivot j, lane 0
+  // (which owns column j + 1) keeps the largest |F[r][j+1]| over its rows r < k;
+  // after the barrier every thread reduces the warps' candidates to the same next
+  // pivot row (largest modulus, lowest row on ties), as a block-wide argmax would.
   int *piv = a.piv + (int64_t)fq * a.n + a.p0[f];
+  int p = k > 0 ? block_argmax<T>(0, k, [&](int r) { return F[r * m]; }, s_v, s_i) : 0;
+  bool pert_prev = false;
+  cplx<T> pv_prev{0, 0};
   for (int j = 0; j < k; ++j) {
-    const int p = block_argmax<T>(j, k, [&](int r) { return F[r * m + j]; }, s_v, s_i);
     if (p != j) {   // p is the same in every thread
       for (int c = threadIdx.x; c < m; c += blockDim.x) {
         const cplx<T> t = F[j * m + c];
@@ -236,29 +243,53 @@ __global__ void __launch_bounds__(kSmallThreads) front_small_kernel(FrontArgs<T>
       }
       __syncthreads();   // the swapped pivot row is read below
     }
+    cplx<T> pv = F[j * m + j];
+    const bool pert = cabs1(pv) < a.tiny;
+    if (pert) pv = cplx<T>{a.tiny, (T)0};
     if (threadIdx.x == 0) {
       piv[j] = p;
-      cplx<T> pv = F[j * m + j];
-      if (cabs1(pv) < a.tiny) {
-        pv = cplx<T>{a.tiny, (T)0};
-        F[j * m + j] = pv;
-        atomicAdd(a.nperturb + fq, 1);
-      }
-      s_pivot = pv;
+      if (pert) atomicAdd(a.nperturb + fq, 1);
     }
-    __syncthreads();
-    const cplx<T> inv = cdiv(cplx<T>{1, 0}, s_pivot);
+    const cplx<T> inv = cdiv(cplx<T>{1, 0}, pv);
     // rows below the pivot: multiplier, then the rank-1 update of the row
     const cplx<T> *prow = F + j * m;
+    T best = (T)-1;
+    int bi = j + 1;
     for (int r = j + 1 + wid; r < m; r += nw) {
       cplx<T> *row = F + r * m;
       const cplx<T> l = cmul(row[j], inv);
       for (int c = j + 1 + lane; c < m; c += 32) row[c] = cfms(row[c], l, prow[c]);
       __syncwarp();
-      if (lane == 0) row[j] = l;
+      if (lane == 0) {
+        row[j] = l;
+        if (r < k && j + 1 < k) {
+          const T v = cabs1(row[j + 1]);
+          if (v > best) best = v, bi = r;
+        }
+      }
     }
+    if (lane == 0) {
+      s_cv[j & 1][wid] = best;
+      s_ci[j & 1][wid] = bi;
+    }
+    // the previous pivot's perturbed diagonal is read by no one any more
+    if (pert_prev && threadIdx.x == 0) F[(j - 1) * m + j - 1] = pv_prev;
+    pert_prev = pert;
+    pv_prev = pv;
     __syncthreads();
+    if (j + 1 < k) {
+      T bv = (T)-1;
+      int bq = j + 1;
+      for (int q = 0; q < nw; ++q) {
+        const T v = s_cv[j & 1][q];
+        const int i = s_ci[j & 1][q];
+        if (v > bv || (v == bv && i < bq)) bv = v, bq = i;
+      }
+      p = bq;
+    }
   }
+  if (pert_prev && threadIdx.x == 0) F[(k - 1) * m + k - 1] = pv_prev;
+  __syncthreads();
   cplx<T> *G = arena + a.off[f];
   for (int r = wid; r < m; r += nw)
     for (int c = lane; c < m; c += 32) G[(int64_t)r * ld + c] = F[r * m + c];
@@ -270,27 +301,25 @@ namespace ss {
 
 constexpr int kPanel = 32;      // panel width of the blocked partial LU
 
-// Large fronts: CTA (front, frequency, block of `rows` rows) assembles its rows in
-// shared memory -- zeroes, arrowhead entries of A'(w), then the children's update
-// rows that map into them (children in order: deterministic) -- and writes each
-// row to the arena once, coalesced.  Per element: one arena write, the child
-// update blocks read once.
-constexpr int kAsmSmemTarget = 64 * 1024;   // shared bytes per CTA (several CTAs per SM)
-constexpr int kAsmSmemMax = 200 * 1024;     // wider fronts use front_assemble_wide_kernel
+constexpr int kRowChunk = 32;   // rows per CTA in the large-front assembly
+
+// Large fronts, assembly in global memory: CTA (front, frequency, row chunk)
+// zeroes its rows, drops in the arrowhead entries of those rows, then adds the
+// children's update rows that map into them (children in order: deterministic).
 template <class T>
-__global__ void __launch_bounds__(256) front_assemble_large_kernel(FrontArgs<T> a, int rows) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  cplx<T> *S = reinterpret_cast<cplx<T> *>(smem_raw);
+__global__ void __launch_bounds__(256) front_assemble_large_kernel(FrontArgs<T> a) {
   const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
-  const int m = a.m[f], ld = a.ld[f];
-  const int r0 = blockIdx.z * rows;
+  const int k = a.k[f], m = a.m[f], ld = a.ld[f];
+  const int r0 = blockIdx.z * kRowChunk;
   if (r0 >= m) return;
-  const int r1 = min(m, r0 + rows);
+  const int r1 = min(m, r0 + kRowChunk);
   const double w = a.omega[fq];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   cplx<T> *arena = a.arena + (int64_t)fq * a.stride;
   cplx<T> *F = arena + a.off[f];
-  for (int t = threadIdx.x; t < (r1 - r0) * m; t += blockDim.x) S[t] = cplx<T>{0, 0};
+  for (int t = threadIdx.x; t < (r1 - r0) * m; t += blockDim.x) {
+    const int r = r0 + t / m, c = t % m;
+    F[(int64_t)r * ld + c] = cplx<T>{0, 0};
+  }
   __syncthreads();
   {
     // arrow entries are sorted by row position
@@ -306,10 +335,8 @@ __global__ void __launch_bounds__(256) front_assemble_large_kernel(FrontArgs<T> 
       int64_t mid = (b + e) / 2;
       if (a.arrow_pos[mid] / ld < r1) b = mid + 1; else e = mid;
     }
-    for (int64_t q = q0 + threadIdx.x; q < b; q += blockDim.x) {
-      const int pos = a.arrow_pos[q];
-      S[(pos / ld - r0) * m + pos % ld] = to_t<T>(a_entry(a.Kc, a.Mc, a.Dc, a.arrow_slot[q], w, a.beta));
-    }
+    for (int64_t q = q0 + threadIdx.x; q < b; q += blockDim.x)
+      F[a.arrow_pos[q]] = to_t<T>(a_entry(a.Kc, a.Mc, a.Dc, a.arrow_slot[q], w, a.beta));
   }
   __syncthreads();
   for (int64_t cc = a.child_ptr[f]; cc < a.child_ptr[f + 1]; ++cc) {
@@ -323,54 +350,10 @@ __global__ void __launch_bounds__(256) front_assemble_large_kernel(FrontArgs<T> 
     while (b < e) { int mid = (b + e) / 2; if (rel[mid] < r1) b = mid + 1; else e = mid; }
     const int i1 = b;
     const cplx<T> *CB = arena + a.off[ch] + (int64_t)kc * ldc + kc;
-    for (int i = i0 + wid; i < i1; i += nw) {
-      cplx<T> *d = S + (rel[i] - r0) * m;
-      const cplx<T> *src = CB + (int64_t)i * ldc;
-      for (int j = lane; j < nn; j += 32) d[rel[j]] = d[rel[j]] + src[j];
-    }
-    __syncthreads();
-  }
-  for (int r = r0 + wid; r < r1; r += nw) {
-    const cplx<T> *src = S + (r - r0) * m;
-    cplx<T> *dst = F + (int64_t)r * ld;
-    for (int c = lane; c < m; c += 32) dst[c] = src[c];
-  }
-}
-
-// Fronts wider than the shared-memory rows allow: the same assembly directly in
-// the arena (rows of 32 per CTA).
-constexpr int kRowChunk = 32;
-template <class T>
-__global__ void __launch_bounds__(256) front_assemble_wide_kernel(FrontArgs<T> a) {
-  const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
-  const int m = a.m[f], ld = a.ld[f];
-  const int r0 = blockIdx.z * kRowChunk;
-  if (r0 >= m) return;
-  const int r1 = min(m, r0 + kRowChunk);
-  const double w = a.omega[fq];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  cplx<T> *arena = a.arena + (int64_t)fq * a.stride;
-  cplx<T> *F = arena + a.off[f];
-  for (int r = r0 + wid; r < r1; r += nw)
-    for (int c = lane; c < m; c += 32) F[(int64_t)r * ld + c] = cplx<T>{0, 0};
-  __syncthreads();
-  for (int64_t q = a.arrow_ptr[f] + threadIdx.x; q < a.arrow_ptr[f + 1]; q += blockDim.x) {
-    const int pos = a.arrow_pos[q];
-    const int r = pos / ld;
-    if (r >= r0 && r < r1) F[pos] = to_t<T>(a_entry(a.Kc, a.Mc, a.Dc, a.arrow_slot[q], w, a.beta));
-  }
-  __syncthreads();
-  for (int64_t cc = a.child_ptr[f]; cc < a.child_ptr[f + 1]; ++cc) {
-    const int ch = a.child[cc];
-    const int kc = a.k[ch], nn = a.m[ch] - kc, ldc = a.ld[ch];
-    const int *rel = a.relpos + a.relpos_ptr[ch];
-    const cplx<T> *CB = arena + a.off[ch] + (int64_t)kc * ldc + kc;
-    for (int i = wid; i < nn; i += nw) {
-      const int r = rel[i];
-      if (r < r0 || r >= r1) continue;
-      cplx<T> *d = F + (int64_t)r * ld;
-      const cplx<T> *src = CB + (int64_t)i * ldc;
-      for (int j = lane; j < nn; j += 32) d[rel[j]] = d[rel[j]] + src[j];
+    for (int t = threadIdx.x; t < (i1 - i0) * nn; t += blockDim.x) {
+      const int i = i0 + t / nn, j = t % nn;
+      cplx<T> &d = F[(int64_t)rel[i] * ld + rel[j]];
+      d = d + CB[(int64_t)i * ldc + j];
     }
     __syncthreads();
   }
@@ -1468,14 +1451,18 @@ struct SweepOpts {
   double tol = kKrylovTol;
 };
 
+// Fronts with m up to this are factored whole in shared memory (one CTA each);
+// wider ones take the level-batched panel path.  The ceiling is what one CTA's
+// shared memory holds (112^2 x 16 bytes, 160^2 x 8 bytes); SS_SMALL_FRONT_M
+// overrides the default (a tuning knob).  On the 262k-DOF ME1 cell the batched
+// path is as fast as the one-CTA kernel up to m = 96 and faster beyond it (one
+// CTA per SM at these shared-memory sizes leaves the pivot chain exposed).
 template <class T>
-static int small_limit() { return sizeof(T) == 8 ? 112 : 128; }  // cd: 112^2*16, cf: 128^2*8 bytes
-// rows per CTA of the shared-memory front assembly for fronts up to m wide (0: too wide)
-template <class T>
-static int asm_rows(int m) {
-  const int row = m * (int)sizeof(cplx<T>);
-  if (row > kAsmSmemMax) return 0;
-  return std::max(1, std::min(32, kAsmSmemTarget / row));
+static int small_limit() {
+  const int cap = sizeof(T) == 8 ? 112 : 160;
+  int v = sizeof(T) == 8 ? 96 : 128;
+  if (const char *e = getenv("SS_SMALL_FRONT_M")) v = atoi(e);
+  return std::max(0, std::min(cap, v));
 }
 
 // equilibration at angular frequency w (Ruiz, 3 sweeps)
@@ -1772,12 +1759,7 @@ struct Sweeper {
       FrontArgs<T> b = a;
       b.fronts = P.d_large.as<int>() + P.large_ptr[l];
       const int ml = P.maxm_large[l];
-      const int rows = asm_rows<T>(ml);
-      if (rows > 0)
-        front_assemble_large_kernel<T><<<dim3(nl, nb, (ml + rows - 1) / rows), 256,
-                                         (size_t)rows * ml * sizeof(cplx<T>), h.stream>>>(b, rows);
-      else
-        front_assemble_wide_kernel<T><<<dim3(nl, nb, (ml + kRowChunk - 1) / kRowChunk), 256, 0, h.stream>>>(b);
+      front_assemble_large_kernel<T><<<dim3(nl, nb, (ml + kRowChunk - 1) / kRowChunk), 256, 0, h.stream>>>(b);
       ++launches;
       const GemmTask *tasks = P.d_tasks.as<GemmTask>();
       const unsigned zc = (unsigned)((ml + 255) / 256);
@@ -1931,8 +1913,6 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
     SS_CK(dupload(P->d_tasks, P->tasks));
     SS_CK(cudaFuncSetAttribute(front_small_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                small_limit<T>() * small_limit<T>() * (int)sizeof(cplx<T>)));
-    SS_CK(cudaFuncSetAttribute(front_assemble_large_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               kAsmSmemMax));
     SS_CK(cudaFuncSetAttribute(front_panel_smem_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                kPanelSmemMax));
     SS_CK(cudaFuncSetAttribute(tc::front_tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
