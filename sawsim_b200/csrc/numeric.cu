@@ -301,18 +301,21 @@ namespace ss {
 
 constexpr int kPanel = 32;      // panel width of the blocked partial LU
 
-constexpr int kRowChunk = 32;   // rows per CTA in the large-front assembly
+// rows per CTA of the large-front assembly: about 16k elements per CTA, at least
+// 32 rows, a whole front when it is that small (narrow fronts would otherwise
+// make hundreds of thousands of near-empty CTAs)
+static inline int asm_rows(int maxm) { return std::max(32, std::min(maxm, 16384 / std::max(1, maxm))); }
 
 // Large fronts, assembly in global memory: CTA (front, frequency, row chunk)
 // zeroes its rows, drops in the arrowhead entries of those rows, then adds the
 // children's update rows that map into them (children in order: deterministic).
 template <class T>
-__global__ void __launch_bounds__(256) front_assemble_large_kernel(FrontArgs<T> a) {
+__global__ void __launch_bounds__(256) front_assemble_large_kernel(FrontArgs<T> a, int rows) {
   const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
   const int k = a.k[f], m = a.m[f], ld = a.ld[f];
-  const int r0 = blockIdx.z * kRowChunk;
+  const int r0 = blockIdx.z * rows;
   if (r0 >= m) return;
-  const int r1 = min(m, r0 + kRowChunk);
+  const int r1 = min(m, r0 + rows);
   const double w = a.omega[fq];
   cplx<T> *arena = a.arena + (int64_t)fq * a.stride;
   cplx<T> *F = arena + a.off[f];
@@ -1759,10 +1762,14 @@ struct Sweeper {
       FrontArgs<T> b = a;
       b.fronts = P.d_large.as<int>() + P.large_ptr[l];
       const int ml = P.maxm_large[l];
-      front_assemble_large_kernel<T><<<dim3(nl, nb, (ml + kRowChunk - 1) / kRowChunk), 256, 0, h.stream>>>(b);
+      const int ar = asm_rows(ml);
+      front_assemble_large_kernel<T><<<dim3(nl, nb, (ml + ar - 1) / ar), 256, 0, h.stream>>>(b, ar);
       ++launches;
       const GemmTask *tasks = P.d_tasks.as<GemmTask>();
-      const unsigned zc = (unsigned)((ml + 255) / 256);
+      // row/column-parallel panel kernels: CTAs no wider than the level's fronts
+      // (narrow fronts then run more CTAs per SM instead of idle threads)
+      const int bs = ml <= 64 ? 64 : ml <= 128 ? 128 : 256;
+      const unsigned zc = (unsigned)((ml + bs - 1) / bs);
       for (int s = 0; s < P.nsteps[l]; ++s) {
         const int j0 = s * kPanel;
         const int64_t q = P.level_step0[l] + 2 * s;
@@ -1772,17 +1779,19 @@ struct Sweeper {
           ++launches;
         }
         const size_t psm = (size_t)std::max(0, P.maxk_large[l] - j0) * (kPanel + 1) * sizeof(cplx<T>);
+        const int prow = P.maxk_large[l] - j0;   // panel rows of the widest front
+        const int pth = prow <= 64 ? 128 : prow <= 160 ? 256 : kPanelThreads;
         if (psm <= (size_t)kPanelSmemMax)
-          front_panel_smem_kernel<T><<<dim3(nl, nb), kPanelThreads, psm, h.stream>>>(b, j0);
+          front_panel_smem_kernel<T><<<dim3(nl, nb), pth, psm, h.stream>>>(b, j0);
         else
           front_panel_kernel<T><<<dim3(nl, nb), 256, 0, h.stream>>>(b, j0);
-        front_l21_kernel<T><<<dim3(nl, nb, zc), 256, 0, h.stream>>>(b, j0);
-        front_swap_trsm_kernel<T><<<dim3(nl, nb, zc), 256, 0, h.stream>>>(b, j0, 0);
+        front_l21_kernel<T><<<dim3(nl, nb, zc), bs, 0, h.stream>>>(b, j0);
+        front_swap_trsm_kernel<T><<<dim3(nl, nb, zc), bs, 0, h.stream>>>(b, j0, 0);
         if (g2 > g1) {   // U row block <- earlier pivots
           panel_gemm(b, q, 1, nb);
           ++launches;
         }
-        front_swap_trsm_kernel<T><<<dim3(nl, nb, zc), 256, 0, h.stream>>>(b, j0, 1);
+        front_swap_trsm_kernel<T><<<dim3(nl, nb, zc), bs, 0, h.stream>>>(b, j0, 1);
         launches += 4;
       }
     }

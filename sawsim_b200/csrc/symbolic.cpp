@@ -423,7 +423,8 @@ int build_symbolic(Handle &h) {
   for (int64_t v = 0; v < nsv; ++v) std::copy(sadj[v].begin(), sadj[v].end(), aj.begin() + ap[v]);
   sadj.clear();
 
-  const int leaf = h.dim == 3 ? 8 : 12;
+  int leaf = h.dim == 3 ? 8 : 12;
+  if (const char *e = getenv("SS_ND_LEAF")) leaf = std::max(1, atoi(e));
   ND nd(ap, aj, h.sv_xyz, h.dim, leaf, nsv);
   std::vector<int64_t> all(nsv);
   std::iota(all.begin(), all.end(), 0);
