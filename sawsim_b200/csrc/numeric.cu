@@ -353,10 +353,30 @@ __global__ void __launch_bounds__(256) front_assemble_large_kernel(FrontArgs<T> 
     while (b < e) { int mid = (b + e) / 2; if (rel[mid] < r1) b = mid + 1; else e = mid; }
     const int i1 = b;
     const cplx<T> *CB = arena + a.off[ch] + (int64_t)kc * ldc + kc;
-    for (int t = threadIdx.x; t < (i1 - i0) * nn; t += blockDim.x) {
-      const int i = i0 + t / nn, j = t % nn;
-      cplx<T> &d = F[(int64_t)rel[i] * ld + rel[j]];
-      d = d + CB[(int64_t)i * ldc + j];
+    // four elements per thread and pass, every load issued before any store (the
+    // targets of one child are distinct), so that each thread keeps several
+    // memory requests in flight
+    constexpr int U = 4;
+    const int tot = (i1 - i0) * nn;
+    for (int t0 = threadIdx.x; t0 < tot; t0 += U * blockDim.x) {
+      cplx<T> *dp[U];
+      cplx<T> cv[U], dv[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int t = t0 + u * blockDim.x;
+        dp[u] = nullptr;
+        if (t < tot) {
+          const int i = i0 + t / nn, j = t % nn;
+          dp[u] = F + (int64_t)rel[i] * ld + rel[j];
+          cv[u] = CB[(int64_t)i * ldc + j];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (dp[u]) dv[u] = *dp[u];
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (dp[u]) *dp[u] = dv[u] + cv[u];
     }
     __syncthreads();
   }
@@ -808,6 +828,8 @@ __global__ void __launch_bounds__(256) front_fwd_kernel(FrontArgs<T> a, const cd
   const int64_t p0 = a.p0[f];
   for (int i = threadIdx.x; i < m; i += blockDim.x)
     v[i] = i < k ? to_t<T>(b[(int64_t)fq * a.n + p0 + i]) : cplx<T>{0, 0};
+  int *sp = reinterpret_cast<int *>(v + m);   // this front's pivots, loaded in parallel
+  for (int j = threadIdx.x; j < k; j += blockDim.x) sp[j] = a.piv[(int64_t)fq * a.n + p0 + j];
   __syncthreads();
   cplx<T> *w = wv + (int64_t)fq * wstride;
   for (int64_t cc = a.child_ptr[f]; cc < a.child_ptr[f + 1]; ++cc) {
@@ -819,9 +841,8 @@ __global__ void __launch_bounds__(256) front_fwd_kernel(FrontArgs<T> a, const cd
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    const int *piv = a.piv + (int64_t)fq * a.n + p0;
     for (int j = 0; j < k; ++j) {
-      const int p = piv[j];
+      const int p = sp[j];
       if (p != j) {
         const cplx<T> t = v[j];
         v[j] = v[p];
@@ -950,8 +971,10 @@ __global__ void __launch_bounds__(256) front_bwd_kernel(FrontArgs<T> a, cd *__re
     __syncthreads();
     if (wid == 0) {
       cplx<T> x = lane < bw ? z[jb + lane] : cplx<T>{0, 0};
+      // each lane's diagonal reciprocal up front: the chain below multiplies
+      const cplx<T> rd = lane < bw ? cdiv(cplx<T>{1, 0}, D[lane * kDiagS + lane]) : cplx<T>{0, 0};
       for (int t = bw - 1; t >= 0; --t) {
-        if (lane == t) x = cdiv(x, D[t * kDiagS + t]);
+        if (lane == t) x = cmul(x, rd);
         cplx<T> xt;
         xt.x = __shfl_sync(0xffffffffu, x.x, t);
         xt.y = __shfl_sync(0xffffffffu, x.y, t);
@@ -1015,8 +1038,9 @@ __global__ void __launch_bounds__(256) front_tfwd_kernel(FrontArgs<T> a, const c
     __syncthreads();
     if (wid == 0) {
       cplx<T> xv = lane < bw ? v[jb + lane] : cplx<T>{0, 0};
+      const cplx<T> rd = lane < bw ? cdiv(cplx<T>{1, 0}, D[lane * kDiagS + lane]) : cplx<T>{0, 0};
       for (int t = 0; t < bw; ++t) {
-        if (lane == t) xv = cdiv(xv, D[t * kDiagS + t]);
+        if (lane == t) xv = cmul(xv, rd);
         cplx<T> xt;
         xt.x = __shfl_sync(0xffffffffu, xv.x, t);
         xt.y = __shfl_sync(0xffffffffu, xv.y, t);
@@ -1099,6 +1123,8 @@ __global__ void __launch_bounds__(256) front_tbwd_kernel(FrontArgs<T> a, cd *__r
   const int64_t p0 = a.p0[f];
   cd *xf = x + (int64_t)fq * a.n;
   for (int i = threadIdx.x; i < k; i += blockDim.x) z[i] = to_t<T>(xf[p0 + i]);
+  int *sp = reinterpret_cast<int *>(z + k);   // this front's pivots, loaded in parallel
+  for (int j = threadIdx.x; j < k; j += blockDim.x) sp[j] = a.piv[(int64_t)fq * a.n + p0 + j];
   __syncthreads();
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (int je = k; je > 0; je -= 32) {
@@ -1124,9 +1150,8 @@ __global__ void __launch_bounds__(256) front_tbwd_kernel(FrontArgs<T> a, cd *__r
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    const int *piv = a.piv + (int64_t)fq * a.n + p0;
     for (int j = k - 1; j >= 0; --j) {
-      const int p = piv[j];
+      const int p = sp[j];
       if (p != j) {
         const cplx<T> t = z[j];
         z[j] = z[p];
@@ -1519,6 +1544,12 @@ struct Sweeper {
   static constexpr size_t kDiagBytes = (size_t)kDiagElems * sizeof(cplx<T>);
   Handle &h;
   Plan &P;
+  size_t pivb = 0;   // shared bytes for one front's pivot list (solve kernels)
+  // CTA width of a level's solve kernels: no wider than its widest front
+  int solve_threads(int l) const {
+    const int w = P.lvl_maxk[l] + P.lvl_maxu[l];
+    return w <= 64 ? 64 : w <= 128 ? 128 : 256;
+  }
   FrontArgs<T> a{};
   int64_t wstride = 0;
   int launches = 0, schur_launches = 0;
@@ -1529,6 +1560,7 @@ struct Sweeper {
   cplx<T> *stage_wv = nullptr;               // solve workspace baked into the solve graphs
   cd *stage_b = nullptr, *stage_x = nullptr; // solve input / output staging for the graphs
   explicit Sweeper(Handle &hh, Plan &pp) : h(hh), P(pp), ev(pp.ev) {
+    pivb = ((size_t)std::max(1, h.sym.max_k) * sizeof(int) + 15) / 16 * 16;
     if (ev.empty()) {
       ev.resize(2 * std::max(1, h.sym.nlevel));
       // recorded once outside any capture: the graphs' event-record nodes then
@@ -1826,11 +1858,12 @@ struct Sweeper {
       FrontArgs<T> c = a;
       c.fronts = h.d_level_fronts.as<int>() + S.level_ptr[l];
       const int nf = (int)(S.level_ptr[l + 1] - S.level_ptr[l]);
-      front_fwd_kernel<T><<<dim3(nf, nb), 256, sm + kDiagBytes, h.stream>>>(c, b, x, wv, wstride);
+      const int bs = solve_threads(l);
+      front_fwd_kernel<T><<<dim3(nf, nb), bs, sm + kDiagBytes + pivb, h.stream>>>(c, b, x, wv, wstride);
       ++launches;
       if (P.lvl_maxu[l] > 0) {
         const unsigned z = (unsigned)((P.lvl_maxu[l] + kSolveRows - 1) / kSolveRows);
-        front_fwd_l21_kernel<T><<<dim3(nf, nb, z), 256, smk, h.stream>>>(c, x, wv, wstride);
+        front_fwd_l21_kernel<T><<<dim3(nf, nb, z), bs, smk, h.stream>>>(c, x, wv, wstride);
         ++launches;
       }
     }
@@ -1838,12 +1871,13 @@ struct Sweeper {
       FrontArgs<T> c = a;
       c.fronts = h.d_level_fronts.as<int>() + S.level_ptr[l];
       const int nf = (int)(S.level_ptr[l + 1] - S.level_ptr[l]);
+      const int bs = solve_threads(l);
       if (P.lvl_maxu[l] > 0) {
         const unsigned z = (unsigned)((P.lvl_maxk[l] + kSolveRows - 1) / kSolveRows);
-        front_bwd_u12_kernel<T><<<dim3(nf, nb, z), 256, (size_t)P.lvl_maxu[l] * sizeof(cplx<T>), h.stream>>>(c, x);
+        front_bwd_u12_kernel<T><<<dim3(nf, nb, z), bs, (size_t)P.lvl_maxu[l] * sizeof(cplx<T>), h.stream>>>(c, x);
         ++launches;
       }
-      front_bwd_kernel<T><<<dim3(nf, nb), 256, smk + kDiagBytes, h.stream>>>(c, x);
+      front_bwd_kernel<T><<<dim3(nf, nb), bs, smk + kDiagBytes, h.stream>>>(c, x);
       ++launches;
     }
     SS_CK(cudaGetLastError());
@@ -1858,7 +1892,7 @@ struct Sweeper {
       FrontArgs<T> c = a;
       c.fronts = h.d_level_fronts.as<int>() + S.level_ptr[l];
       const int nf = (int)(S.level_ptr[l + 1] - S.level_ptr[l]);
-      front_tfwd_kernel<T><<<dim3(nf, nb), 256, sm + kDiagBytes, h.stream>>>(c, cvec, mu, wv, wstride);
+      front_tfwd_kernel<T><<<dim3(nf, nb), solve_threads(l), sm + kDiagBytes, h.stream>>>(c, cvec, mu, wv, wstride);
       ++launches;
       if (P.lvl_maxu[l] > 0) {
         const unsigned z = (unsigned)((P.lvl_maxu[l] + 255) / 256);
@@ -1875,7 +1909,7 @@ struct Sweeper {
         front_tbwd_l21_kernel<T><<<dim3(nf, nb, z), 256, (size_t)P.lvl_maxu[l] * sizeof(cplx<T>), h.stream>>>(c, mu);
         ++launches;
       }
-      front_tbwd_kernel<T><<<dim3(nf, nb), 256, smk + kDiagBytes, h.stream>>>(c, mu);
+      front_tbwd_kernel<T><<<dim3(nf, nb), solve_threads(l), smk + kDiagBytes + pivb, h.stream>>>(c, mu);
       ++launches;
     }
     SS_CK(cudaGetLastError());
@@ -1931,7 +1965,8 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
     // solve kernels stage a whole front vector in shared memory
     // (the four triangular kernels also hold one staged 32x32 diagonal block)
     const int vec = (int)std::min<int64_t>(227 * 1024, (int64_t)S.max_m * (int64_t)sizeof(cplx<T>));
-    const int vecd = (int)std::min<int64_t>(227 * 1024, vec + (int64_t)kDiagElems * sizeof(cplx<T>));
+    const int vecd = (int)std::min<int64_t>(227 * 1024, vec + (int64_t)kDiagElems * sizeof(cplx<T>) +
+                                                           ((int64_t)std::max(1, S.max_k) * 4 + 15) / 16 * 16);
     if (vecd > 48 * 1024) {
       SS_CK(cudaFuncSetAttribute(front_fwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vecd));
       SS_CK(cudaFuncSetAttribute(front_tfwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vecd));
