@@ -37,6 +37,7 @@ CPU_SAMPLE = {'me0_16x64': [dict(cols=8, rows=32), dict(cols=16, rows=64)],
               'me1_64x256': [dict(cols=16, rows=64), dict(cols=32, rows=128)],
               'me1_128x512': [dict(cols=16, rows=64), dict(cols=32, rows=128)],
               'hex_8x4x48': [dict(nx=8, ny=1, nz=12), dict(nx=8, ny=2, nz=24)]}
+SCHUR_DRAM_BYTES_PER_POINT = {'me1_64x256': 6.16e9}
 METRIC = 'Y11 points/s, 1 B200: batched FP32-TC+refine vs FP64 sweep, fr/fa within 1 kHz'
 
 
@@ -286,6 +287,12 @@ def b200_arm(a, rank, world, local):
     s = eng.stats()
     pk, pk_kind = peaks()
     schur_flops_launch = s['schur_gemm_flops'] / max(1.0, s['schur_launches'])
+    # DRAM bytes of the Schur update per frequency point, from an ncu capture of the
+    # same kernels (profiles/schur_fp64_me1_64x256_traffic.md; 1 and 2 points: the
+    # bytes grow in proportion to the points), scaled to the launches of this run
+    traffic = None
+    if used == 'fp64' and a.case in SCHUR_DRAM_BYTES_PER_POINT:
+        traffic = SCHUR_DRAM_BYTES_PER_POINT[a.case] * nf / max(1.0, s['schur_launches'])
     schur_ms_launch = float(np.mean(schur_ms)) / max(1.0, s['schur_launches'])
     if used == 'mixed':
         peak = pk.get('bf16_tflops', 1590.0) / 2
@@ -321,7 +328,8 @@ def b200_arm(a, rank, world, local):
                     roofline=dict(kernel=schur_kernel_name(s, used),
                                   bound='tensor',
                                   achieved=achieved, peak=peak, unit='TFLOP/s',
-                                  frac=(achieved / peak) if achieved else None, traffic=None, peak_note=peak_note,
+                                  frac=(achieved / peak) if achieved else None, traffic=traffic, traffic_unit='bytes per launch',
+                                  peak_note=peak_note,
                                   flops_per_launch=schur_flops_launch),
                     clocks=clk.summary(), cpu_baseline=cpu)
     return line
