@@ -249,6 +249,7 @@ def b200_arm(a, rank, world, local):
                 Q_all = gather_charges(Q, n_total, rank, world)
             wall_s.append(time.perf_counter() - t)
             s = eng.stats()
+            s_timed = s
             dev_ms.append(s['sweep_device_ms'])
             schur_ms.append(s['schur_gemm_ms'])
             launches += int(s['launches'])
@@ -284,7 +285,7 @@ def b200_arm(a, rank, world, local):
         t = torch.tensor([dev, wall], device='cuda', dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dev, wall = t.tolist()
-    s = eng.stats()
+    s = s_timed           # counters of the last timed sweep (not of the FP64 accuracy check)
     pk, pk_kind = peaks()
     schur_flops_launch = s['schur_gemm_flops'] / max(1.0, s['schur_launches'])
     # DRAM bytes of the Schur update per frequency point, from an ncu capture of the
@@ -316,6 +317,8 @@ def b200_arm(a, rank, world, local):
                     data='synthetic',
                     config=dict(workload=workload_name(c),
                                 precision=a.precision, precision_used=used, accuracy=acc,
+                                auto_probe=('probed on the first (warm-up) sweep of the band; the repeated sweeps '
+                                            'keep the decision' if a.precision == 'auto' else None),
                                 n_active=int(st0['n_active']), fronts=int(st0['n_fronts']),
                                 factor_gflop_per_point=st0['factor_flops_per_point'] / 1e9,
                                 setup_s=setup_s, analyze_s=st0['analyze_s'], assemble_ms=st0['assemble_ms'],

@@ -46,7 +46,9 @@ typedef struct ss_handle ss_handle;
                               FP64 residual, FP64 flexible GMRES on the primal and
                               the adjoint, dual-weighted charge correction       */
 #define SS_PREC_AUTO   2   /* probe MIXED on the two band ends with 12 Krylov
-                              steps; MIXED if both converge, else FP64           */
+                              steps; MIXED if both converge, else FP64; the
+                              decision is kept for the same two end
+                              frequencies until the system changes               */
 
 /* matrix selectors for ss_set_csr / ss_export_csr */
 #define SS_MAT_K    0      /* global stiffness                                   */

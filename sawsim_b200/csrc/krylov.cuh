@@ -109,9 +109,6 @@ __global__ void combine_kernel(int64_t n, int nb, const int *__restrict__ kf, co
   x[(int64_t)f * n + R] = acc;
 }
 
-struct KrylovWork {
-  DBuf V, Z, w, h, hn, y, kf, sc;
-};
 
 // FGMRES(m) with up to `restarts` cycles; x holds the initial guess on entry.
 // precond(src, dst) applies M^-1 to nb vectors.  Returns the number of

@@ -1997,9 +1997,13 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
   const bool need_adjoint = correct || (ex && ex->per_chunk);
   const double per = (double)S.arena * sizeof(cplx<T>) + n * 4.0 + W * (double)sizeof(cplx<T>) + n * 64.0 + krylov +
                      (need_adjoint ? 32.0 * n : 0.0) + 32.0 * n + 256;
-  KrylovWork kw;
+  // the Krylov workspace persists in the handle; a sweep without Krylov steps
+  // gives its memory back to the fronts
+  KrylovWork &kw = h.kw;
+  if (!(sizeof(T) == 4 || getenv("SS_FP64_KRYLOV") != nullptr)) kw.release();
   size_t fr = 0, tot = 0;
   SS_CK(cudaMemGetInfo(&fr, &tot));
+  fr += kw.bytes();
   // device work buffers persist in the handle: repeated sweeps reuse them
   DBuf &arena = h.wk[0], &piv = h.wk[1], &wv = h.wk[2], &b = h.wk[3], &x = h.wk[4], &r = h.wk[5], &dx = h.wk[6],
        &dom = h.wk[7], &npert = h.wk[8], &nrm = h.wk[9], &dQ = h.wk[10], &mu = h.wk[11], &cvec = h.wk[12];
@@ -2270,14 +2274,18 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
 
 // SS_PREC_AUTO: a probe of the mixed sweep on the band's two end points with a
 // short Krylov budget (12 steps each for the primal and the adjoint); if both
-// converge the whole sweep runs
-// mixed, otherwise FP64 (the complex64 factors of a cell whose conditioning
-// defeats FP32 would need many Krylov steps per point).
+// converge the whole sweep runs mixed, otherwise FP64 (the complex64 factors of a
+// cell whose conditioning defeats FP32 would need many Krylov steps per point).
+// The decision is kept for the band's end points until the system changes, so a
+// repeated sweep of the same band probes once.
 int run_sweep(Handle &h, int n_f, const double *omega, double V, int precision, double *Q, int *status,
               int *iters, double *disp_out, const SweepExtra *ex) {
   SweepOpts opt;
   int rc;
   double probe_ms = 0, probe_launches = 0;
+  if (precision == SS_PREC_AUTO && n_f > 0 && h.auto_prec >= 0 && h.auto_w0 == omega[0] &&
+      h.auto_w1 == omega[n_f - 1])
+    precision = h.auto_prec;
   if (precision == SS_PREC_AUTO && n_f > 0) {
     const double ends[2] = {omega[0], omega[n_f - 1]};
     double q[4];
@@ -2288,6 +2296,9 @@ int run_sweep(Handle &h, int n_f, const double *omega, double V, int precision, 
     rc = sweep_impl<float>(h, n_f > 1 ? 2 : 1, ends, V, q, st, it, nullptr, nullptr, probe);
     if (rc) return rc;
     precision = (st[0] == SS_OK && st[1] == SS_OK) ? SS_PREC_MIXED : SS_PREC_FP64;
+    h.auto_w0 = omega[0];
+    h.auto_w1 = omega[n_f - 1];
+    h.auto_prec = precision;
     probe_ms = h.st[17];
     probe_launches = h.st[15];
   }
@@ -2305,6 +2316,7 @@ int run_sweep(Handle &h, int n_f, const double *omega, double V, int precision, 
 
 namespace ss {
 void free_plans(Handle &h) {
+  h.auto_prec = -1;
   for (int i = 0; i < 2; ++i) {
     delete static_cast<Plan *>(h.plan[i]);
     h.plan[i] = nullptr;

@@ -25,6 +25,14 @@ struct DBuf {
   template <class T> T *as() const { return reinterpret_cast<T *>(p); }
 };
 
+// FGMRES workspace (basis, preconditioned basis, Hessenberg data); held by the
+// handle so that repeated mixed sweeps reuse it
+struct KrylovWork {
+  DBuf V, Z, w, h, hn, y, kf, sc;
+  size_t bytes() const { return V.bytes + Z.bytes + w.bytes + h.bytes + hn.bytes + y.bytes + kf.bytes + sc.bytes; }
+  void release() { V.release(); Z.release(); w.release(); h.release(); hn.release(); y.release(); kf.release(); sc.release(); }
+};
+
 // Allocate (or grow) a device buffer; returns cudaError_t.
 cudaError_t dalloc(DBuf &b, size_t bytes);
 template <class T>
@@ -124,6 +132,11 @@ struct Handle {
   DBuf dct_ptr, dct_idx, dct_src;        // transposed condensed pattern (new order) and value slots
   size_t arena_chunk = 0;
   void *plan[2] = {nullptr, nullptr};   // factorisation plans per precision
+  KrylovWork kw;                         // FGMRES workspace of the mixed sweeps
+  // SS_PREC_AUTO's decision for the last probed band (its two end frequencies);
+  // dropped with the plans whenever the system changes
+  double auto_w0 = 0, auto_w1 = 0;
+  int auto_prec = -1;
   DBuf dKs, dMs, dDs;                    // equilibrated condensed values
   double scale_w = -1;                   // frequency the scaling was computed at
   // stats

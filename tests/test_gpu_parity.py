@@ -130,3 +130,14 @@ def test_auto_precision_picks_a_converging_mode(pair):
     assert (st == 0).all()
     assert int(g.stats()['precision_used']) in (0, 1)
     assert np.max(np.abs(Qa - Q64) / np.abs(Q64)) < 1e-6
+    # the decision is kept for the same band: a repeated AUTO sweep runs the same
+    # mode without probing (fewer launches) and gives the same charges
+    used, launches = int(g.stats()['precision_used']), g.stats()['launches']
+    Qb, st, _ = g.charges(w, 1.0, 'auto')
+    assert (st == 0).all()
+    assert int(g.stats()['precision_used']) == used
+    assert g.stats()['launches'] < launches
+    assert np.max(np.abs(Qa - Qb) / np.abs(Qa)) < 1e-12
+    # another band probes again
+    g.charges(w[:3], 1.0, 'auto')
+    assert int(g.stats()['precision_used']) in (0, 1)
