@@ -383,9 +383,14 @@ __global__ void __launch_bounds__(256) front_assemble_large_kernel(FrontArgs<T> 
 }
 
 // Rows [k, m) of the panel columns: L21[:, j0:j1] = F21[:, j0:j1] U_jj^-1 (each
-// row independent, one thread per row; U_jj staged in shared memory).
+// row independent, one thread per row; U_jj and its diagonal reciprocals staged in
+// shared memory).  The 32 columns go in two halves of 16 held in registers: the
+// second half first takes the first half's finished values back from the row
+// (still in L1) in the order t = 0, 1, ..., so every entry sees the operations of a
+// single 32-column substitution in the same order.
 template <class T>
 __global__ void __launch_bounds__(256) front_l21_kernel(FrontArgs<T> a, int j0) {
+  constexpr int H = kPanel / 2;
   __shared__ cplx<T> U[kPanel][kPanel];
   __shared__ cplx<T> Uinv[kPanel];          // reciprocals of the diagonal, once per CTA
   const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
@@ -400,21 +405,31 @@ __global__ void __launch_bounds__(256) front_l21_kernel(FrontArgs<T> a, int j0) 
   const int r = k + blockIdx.z * blockDim.x + threadIdx.x;
   if (r >= m) return;
   cplx<T> *row = a.arena + (int64_t)fq * a.stride + a.off[f] + (int64_t)r * ld + j0;
-  cplx<T> x[kPanel];
+  for (int h0 = 0; h0 < w; h0 += H) {
+    const int hw = min(H, w - h0);
+    cplx<T> x[H];
 #pragma unroll
-  for (int c = 0; c < kPanel; ++c)
-    if (c < w) x[c] = row[c];
+    for (int c = 0; c < H; ++c)
+      if (c < hw) x[c] = row[h0 + c];
+    // the finished columns left of this half
+    for (int t = 0; t < h0; ++t) {
+      const cplx<T> xt = row[t];
 #pragma unroll
-  for (int c = 0; c < kPanel; ++c) {
-    if (c >= w) break;
-    cplx<T> v = x[c];
+      for (int c = 0; c < H; ++c)
+        if (c < hw) x[c] = cfms(x[c], xt, U[t][h0 + c]);
+    }
 #pragma unroll
-    for (int t = 0; t < c; ++t) v = cfms(v, x[t], U[t][c]);
-    x[c] = cmul(v, Uinv[c]);
+    for (int c = 0; c < H; ++c) {
+      if (c >= hw) break;
+      cplx<T> v = x[c];
+#pragma unroll
+      for (int t = 0; t < c; ++t) v = cfms(v, x[t], U[h0 + t][h0 + c]);
+      x[c] = cmul(v, Uinv[h0 + c]);
+    }
+#pragma unroll
+    for (int c = 0; c < H; ++c)
+      if (c < hw) row[h0 + c] = x[c];
   }
-#pragma unroll
-  for (int c = 0; c < kPanel; ++c)
-    if (c < w) row[c] = x[c];
 }
 
 // Unblocked LU of panel columns [j0, j1) over the fully-summed rows [j0, k).
@@ -526,11 +541,39 @@ __global__ void __launch_bounds__(kPanelThreads) front_panel_smem_kernel(FrontAr
     if (lane < w) F[(int64_t)r * ld + lane] = P[r * PS + lane];
 }
 
-// mode 0: apply the panel's row swaps to every column outside it (one thread per
-// column).  mode 1: solve the unit-lower diagonal block into the row block
-// U[j0:j1, j1:m) (one thread per column, L_jj staged in shared memory).
+// The panel's row swaps applied to every column outside it (one thread per
+// column; the panel's pivots read once into shared memory).
 template <class T>
-__global__ void __launch_bounds__(256) front_swap_trsm_kernel(FrontArgs<T> a, int j0, int mode) {
+__global__ void __launch_bounds__(256) front_swap_kernel(FrontArgs<T> a, int j0) {
+  __shared__ int sp[kPanel];
+  const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
+  const int k = a.k[f], m = a.m[f], ld = a.ld[f];
+  if (j0 >= k) return;
+  const int j1 = min(k, j0 + kPanel), w = j1 - j0;
+  cplx<T> *F = a.arena + (int64_t)fq * a.stride + a.off[f];
+  if (threadIdx.x < w) sp[threadIdx.x] = a.piv[(int64_t)fq * a.n + a.p0[f] + j0 + threadIdx.x];
+  __syncthreads();
+  const int idx = blockIdx.z * blockDim.x + threadIdx.x;
+  if (idx >= m - w) return;
+  const int c = idx < j0 ? idx : idx + w;
+  for (int j = j0; j < j1; ++j) {
+    const int p = sp[j - j0];
+    if (p != j) {
+      const cplx<T> t = F[(int64_t)j * ld + c];
+      F[(int64_t)j * ld + c] = F[(int64_t)p * ld + c];
+      F[(int64_t)p * ld + c] = t;
+    }
+  }
+}
+
+// The unit-lower diagonal block solved into the row block U[j0:j1, j1:m) (one
+// thread per column, L_jj staged in shared memory).  The 32 rows go in two halves
+// of 16 held in registers: the second half first takes the first half's finished
+// values back from the arena (still in L1) in the order t = 0, 1, ..., so every
+// entry sees the same operations in the same order as a single 32-row pass.
+template <class T>
+__global__ void __launch_bounds__(256) front_u12_trsm_kernel(FrontArgs<T> a, int j0) {
+  constexpr int H = kPanel / 2;
   __shared__ cplx<T> L[kPanel][kPanel];
   const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
   const int k = a.k[f], m = a.m[f], ld = a.ld[f];
@@ -538,39 +581,36 @@ __global__ void __launch_bounds__(256) front_swap_trsm_kernel(FrontArgs<T> a, in
   const int j1 = min(k, j0 + kPanel), w = j1 - j0;
   cplx<T> *F = a.arena + (int64_t)fq * a.stride + a.off[f];
   const int idx = blockIdx.z * blockDim.x + threadIdx.x;
-  if (mode == 0) {
-    if (idx >= m - w) return;
-    const int c = idx < j0 ? idx : idx + w;
-    const int *piv = a.piv + (int64_t)fq * a.n + a.p0[f];
-    for (int j = j0; j < j1; ++j) {
-      const int p = piv[j];
-      if (p != j) {
-        const cplx<T> t = F[(int64_t)j * ld + c];
-        F[(int64_t)j * ld + c] = F[(int64_t)p * ld + c];
-        F[(int64_t)p * ld + c] = t;
-      }
-    }
-    return;
-  }
   for (int t = threadIdx.x; t < w * w; t += blockDim.x) L[t / w][t % w] = F[(int64_t)(j0 + t / w) * ld + j0 + t % w];
   __syncthreads();
   const int c = j1 + idx;
   if (c >= m) return;
-  cplx<T> v[kPanel];
+  cplx<T> *col = F + (int64_t)j0 * ld + c;
+  for (int h0 = 0; h0 < w; h0 += H) {
+    const int hw = min(H, w - h0);
+    cplx<T> v[H];
 #pragma unroll
-  for (int i = 0; i < kPanel; ++i)
-    if (i < w) v[i] = F[(int64_t)(j0 + i) * ld + c];
+    for (int i = 0; i < H; ++i)
+      if (i < hw) v[i] = col[(int64_t)(h0 + i) * ld];
+    // the finished rows above this half
+    for (int t = 0; t < h0; ++t) {
+      const cplx<T> xt = col[(int64_t)t * ld];
 #pragma unroll
-  for (int i = 1; i < kPanel; ++i) {
-    if (i >= w) break;
-    cplx<T> x = v[i];
+      for (int i = 0; i < H; ++i)
+        if (i < hw) v[i] = cfms(v[i], L[h0 + i][t], xt);
+    }
 #pragma unroll
-    for (int t = 0; t < i; ++t) x = cfms(x, L[i][t], v[t]);
-    v[i] = x;
+    for (int i = 1; i < H; ++i) {
+      if (i >= hw) break;
+      cplx<T> x = v[i];
+#pragma unroll
+      for (int t = 0; t < i; ++t) x = cfms(x, L[h0 + i][h0 + t], v[t]);
+      v[i] = x;
+    }
+#pragma unroll
+    for (int i = 0; i < H; ++i)
+      if (i < hw) col[(int64_t)(h0 + i) * ld] = v[i];
   }
-#pragma unroll
-  for (int i = 0; i < kPanel; ++i)
-    if (i < w) F[(int64_t)(j0 + i) * ld + c] = v[i];
 }
 
 constexpr int kGemmBK = 8;
@@ -1818,12 +1858,12 @@ struct Sweeper {
         else
           front_panel_kernel<T><<<dim3(nl, nb), 256, 0, h.stream>>>(b, j0);
         front_l21_kernel<T><<<dim3(nl, nb, zc), bs, 0, h.stream>>>(b, j0);
-        front_swap_trsm_kernel<T><<<dim3(nl, nb, zc), bs, 0, h.stream>>>(b, j0, 0);
+        front_swap_kernel<T><<<dim3(nl, nb, zc), bs, 0, h.stream>>>(b, j0);
         if (g2 > g1) {   // U row block <- earlier pivots
           panel_gemm(b, q, 1, nb);
           ++launches;
         }
-        front_swap_trsm_kernel<T><<<dim3(nl, nb, zc), bs, 0, h.stream>>>(b, j0, 1);
+        front_u12_trsm_kernel<T><<<dim3(nl, nb, zc), bs, 0, h.stream>>>(b, j0);
         launches += 4;
       }
     }
