@@ -18,24 +18,45 @@ struct MatOp {
   const int64_t *rp, *ci, *vp;
 };
 
-// y_f = A'(w_f) x_f   (or A'(w_f)^T x_f with the transposed pattern)
+// y_f = A'(w_f) x_f   (or A'(w_f)^T x_f with the transposed pattern).  A thread
+// owns a row for a block of kSpmvFreqs frequencies, so that the row's K, M (and D)
+// values and column indices are read once per block instead of once per
+// frequency; each frequency's sum runs over the row in the same order as a
+// one-frequency product.
 __global__ void spmv_kernel(int64_t n, int nb, const int64_t *__restrict__ rp, const int64_t *__restrict__ ci,
                             const int64_t *__restrict__ vp, const cd *__restrict__ K, const cd *__restrict__ M,
                             const cd *__restrict__ D, const double *__restrict__ omega, double beta,
                             const cd *__restrict__ x, cd *__restrict__ y) {
   const int64_t R = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int f = blockIdx.y;
-  if (R >= n || f >= nb) return;
-  const double w = omega[f], w2 = w * w;
-  const cd *xf = x + (int64_t)f * n;
-  cd acc{0.0, 0.0};
+  const int f0 = blockIdx.y * kSpmvFreqs;
+  if (R >= n || f0 >= nb) return;
+  const int nf = min(kSpmvFreqs, nb - f0);
+  double w2[kSpmvFreqs], wb[kSpmvFreqs];
+  cd acc[kSpmvFreqs];
+#pragma unroll
+  for (int q = 0; q < kSpmvFreqs; ++q) {
+    const double w = q < nf ? omega[f0 + q] : 0.0;
+    w2[q] = w * w;
+    wb[q] = w * beta;
+    acc[q] = cd{0.0, 0.0};
+  }
+  const cd *xb = x + (int64_t)f0 * n;
   for (int64_t t = rp[R]; t < rp[R + 1]; ++t) {
     const int64_t s = vp ? vp[t] : t;
-    cd a = K[s] - M[s] * w2;
-    if (D) a = a + cmul(cd{0.0, w * beta}, D[s]);
-    acc = acc + cmul(a, xf[ci[t]]);
+    const int64_t j = ci[t];
+    const cd Ks = K[s], Ms = M[s];
+    const cd Ds = D ? D[s] : cd{0.0, 0.0};
+#pragma unroll
+    for (int q = 0; q < kSpmvFreqs; ++q)
+      if (q < nf) {
+        cd a = Ks - Ms * w2[q];
+        if (D) a = a + cmul(cd{0.0, wb[q]}, Ds);
+        acc[q] = acc[q] + cmul(a, xb[(int64_t)q * n + j]);
+      }
   }
-  y[(int64_t)f * n + R] = acc;
+#pragma unroll
+  for (int q = 0; q < kSpmvFreqs; ++q)
+    if (q < nf) y[(int64_t)(f0 + q) * n + R] = acc[q];
 }
 
 __device__ inline cd block_reduce_cd(cd v, cd *red) {
@@ -148,7 +169,7 @@ int fgmres(Handle &h, KrylovWork &kw, const MatOp &op, int nb, int m, int restar
   std::vector<char> done(nb);
   for (int cyc = 0; cyc < restarts; ++cyc) {
     // r = b - A x  -> V_0
-    spmv_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, op.rp, op.ci, op.vp, Kc, Mc,
+    spmv_kernel<<<dim3(vb, spmv_blocks(nb)), 256, 0, h.stream>>>(n, nb, op.rp, op.ci, op.vp, Kc, Mc,
                                                     Dc, d_omega, h.beta, x, w);
     KCK(cudaMemcpyAsync(V, b, vec, cudaMemcpyDeviceToDevice, h.stream));
     {
@@ -179,7 +200,7 @@ int fgmres(Handle &h, KrylovWork &kw, const MatOp &op, int nb, int m, int restar
       cd *Vj = V + (size_t)j * nb * n, *Zj = Z + (size_t)j * nb * n;
       int rc = precond(Vj, Zj);
       if (rc) return rc;
-      spmv_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, op.rp, op.ci, op.vp, Kc,
+      spmv_kernel<<<dim3(vb, spmv_blocks(nb)), 256, 0, h.stream>>>(n, nb, op.rp, op.ci, op.vp, Kc,
                                                       Mc, Dc, d_omega, h.beta, Zj, w);
       // classical Gram-Schmidt, twice
       for (int pass = 0; pass < 2; ++pass) {
@@ -254,7 +275,7 @@ int fgmres(Handle &h, KrylovWork &kw, const MatOp &op, int nb, int m, int restar
     KCK(cudaGetLastError());
   }
   // final true residual check
-  spmv_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, op.rp, op.ci, op.vp, Kc, Mc, Dc,
+  spmv_kernel<<<dim3(vb, spmv_blocks(nb)), 256, 0, h.stream>>>(n, nb, op.rp, op.ci, op.vp, Kc, Mc, Dc,
                                                   d_omega, h.beta, x, w);
   {
     std::vector<cd> one(nb, cd{1.0, 0.0});

@@ -100,25 +100,44 @@ __global__ void charge_kernel(int64_t n, const cd *__restrict__ kq, const double
   if (threadIdx.x == 0) Q[f] = red[0] + Qz[0] * V;
 }
 
-// r[f] = b[f] - A'(w_f) x[f]   (scaled system, FP64), and per-row |r|, |x| maxima
+// r[f] = b[f] - A'(w_f) x[f]   (scaled system, FP64); a thread owns a row for a
+// block of kSpmvFreqs frequencies (the row's matrix data read once per block; each
+// frequency's sum in the order of a one-frequency product).
 // (vp: value slot of each pattern entry, for the transposed operator; nullptr = own slot)
 __global__ void residual_kernel(int64_t n, int nb, const int64_t *__restrict__ rp, const int64_t *__restrict__ ci,
                                 const int64_t *__restrict__ vp, const cd *__restrict__ K, const cd *__restrict__ M,
                                 const cd *__restrict__ D, const double *__restrict__ omega, double beta,
                                 const cd *__restrict__ b, const cd *__restrict__ x, cd *__restrict__ r) {
   const int64_t R = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int f = blockIdx.y;
-  if (R >= n || f >= nb) return;
-  const double w = omega[f], w2 = w * w;
-  const cd *xf = x + (int64_t)f * n;
-  cd acc = b[(int64_t)f * n + R];
+  const int f0 = blockIdx.y * kSpmvFreqs;
+  if (R >= n || f0 >= nb) return;
+  const int nf = min(kSpmvFreqs, nb - f0);
+  double w2[kSpmvFreqs], wb[kSpmvFreqs];
+  cd acc[kSpmvFreqs];
+#pragma unroll
+  for (int q = 0; q < kSpmvFreqs; ++q) {
+    const double w = q < nf ? omega[f0 + q] : 0.0;
+    w2[q] = w * w;
+    wb[q] = w * beta;
+    acc[q] = q < nf ? b[(int64_t)(f0 + q) * n + R] : cd{0.0, 0.0};
+  }
+  const cd *xb = x + (int64_t)f0 * n;
   for (int64_t t = rp[R]; t < rp[R + 1]; ++t) {
     const int64_t s = vp ? vp[t] : t;
-    cd a = K[s] - M[s] * w2;
-    if (D) a = a + cmul(cd{0.0, w * beta}, D[s]);
-    acc = acc - cmul(a, xf[ci[t]]);
+    const int64_t j = ci[t];
+    const cd Ks = K[s], Ms = M[s];
+    const cd Ds = D ? D[s] : cd{0.0, 0.0};
+#pragma unroll
+    for (int q = 0; q < kSpmvFreqs; ++q)
+      if (q < nf) {
+        cd a = Ks - Ms * w2[q];
+        if (D) a = a + cmul(cd{0.0, wb[q]}, Ds);
+        acc[q] = acc[q] - cmul(a, xb[(int64_t)q * n + j]);
+      }
   }
-  r[(int64_t)f * n + R] = acc;
+#pragma unroll
+  for (int q = 0; q < kSpmvFreqs; ++q)
+    if (q < nf) r[(int64_t)(f0 + q) * n + R] = acc[q];
 }
 
 }  // namespace ss
@@ -2162,7 +2181,7 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
     }
     if (getenv("SS_DEBUG_IR")) {
       // backward error of the direct solve: |b - A x| / |b|, and the solution size
-      residual_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, h.dc_ptr.as<int64_t>(), h.dc_idx.as<int64_t>(), nullptr,
+      residual_kernel<<<dim3(vb, spmv_blocks(nb)), 256, 0, h.stream>>>(n, nb, h.dc_ptr.as<int64_t>(), h.dc_idx.as<int64_t>(), nullptr,
                                                           a.Kc, a.Mc, a.Dc, dom.as<double>(), h.beta, b.as<cd>(),
                                                           x.as<cd>(), r.as<cd>());
       norm2_kernel<<<nb, 256, 0, h.stream>>>(n, r.as<cd>(), nrm.as<double>());
@@ -2174,7 +2193,7 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
               q[0] / q[nb], q[nb - 1] / q[2 * nb - 1]);
     }
     for (int it = 0; it < (use_krylov ? 0 : maxit); ++it) {
-      residual_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, h.dc_ptr.as<int64_t>(), h.dc_idx.as<int64_t>(), nullptr,
+      residual_kernel<<<dim3(vb, spmv_blocks(nb)), 256, 0, h.stream>>>(n, nb, h.dc_ptr.as<int64_t>(), h.dc_idx.as<int64_t>(), nullptr,
                                                           a.Kc, a.Mc, a.Dc, dom.as<double>(), h.beta, b.as<cd>(),
                                                           x.as<cd>(), r.as<cd>());
       rc = sw.solve_graphed(1, nb, r.as<cd>(), dx.as<cd>());
@@ -2213,7 +2232,7 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
         for (int f = 0; f < nb; ++f) hit[f] += kits[f], aconv[f] = kconv[f];
       } else {
         // one FP64 refinement step, as for the primal solution
-        residual_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, opT.rp, opT.ci, opT.vp, a.Kc, a.Mc, a.Dc,
+        residual_kernel<<<dim3(vb, spmv_blocks(nb)), 256, 0, h.stream>>>(n, nb, opT.rp, opT.ci, opT.vp, a.Kc, a.Mc, a.Dc,
                                                             dom.as<double>(), h.beta, cvec.as<cd>(), mu.as<cd>(),
                                                             r.as<cd>());
         rc = sw.solve_graphed(2, nb, r.as<cd>(), dx.as<cd>());
@@ -2223,7 +2242,7 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
       if (correct) {
         // dual-weighted correction: Q = c^T x + mu^T (b - A' x) is exact up to
         // (mu_exact - mu)^T (b - A' x), the product of the two solves' errors
-        residual_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, h.dc_ptr.as<int64_t>(), h.dc_idx.as<int64_t>(),
+        residual_kernel<<<dim3(vb, spmv_blocks(nb)), 256, 0, h.stream>>>(n, nb, h.dc_ptr.as<int64_t>(), h.dc_idx.as<int64_t>(),
                                                             nullptr, a.Kc, a.Mc, a.Dc, dom.as<double>(), h.beta,
                                                             b.as<cd>(), x.as<cd>(), r.as<cd>());
         dotu_kernel<<<nb, 256, 0, h.stream>>>(n, mu.as<cd>(), r.as<cd>(), dQ.as<cd>() + B);

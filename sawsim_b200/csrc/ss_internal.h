@@ -33,6 +33,11 @@ struct KrylovWork {
   void release() { V.release(); Z.release(); w.release(); h.release(); hn.release(); y.release(); kf.release(); sc.release(); }
 };
 
+// frequencies per thread in the sparse products (residual, Krylov SpMV): the
+// matrix row is read once per block of this many frequencies
+constexpr int kSpmvFreqs = 8;
+inline unsigned spmv_blocks(int nb) { return (unsigned)((nb + kSpmvFreqs - 1) / kSpmvFreqs); }
+
 // Allocate (or grow) a device buffer; returns cudaError_t.
 cudaError_t dalloc(DBuf &b, size_t bytes);
 template <class T>
