@@ -648,12 +648,15 @@ static inline int tile_bn(int s) { return s == kSquare ? 64 : s == kSkinny ? 32 
 // One BMxBN complex tile of C -= A B per CTA, TMxTN outputs per thread; K in
 // chunks of 8 with the next chunk prefetched into registers.
 template <class T, int S>
-__global__ void __launch_bounds__(256) front_gemm_kernel(FrontArgs<T> a, const GemmTask *__restrict__ tasks) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) front_gemm_kernel(FrontArgs<T> a,
+                                                                                const GemmTask *__restrict__ tasks) {
   constexpr int BM = Tile<S>::BM, BN = Tile<S>::BN, TM = Tile<S>::TM, TN = Tile<S>::TN, BK = kGemmBK;
   constexpr int TX = BN / TN, TY = BM / TM;
   static_assert(TX * TY == 256, "256 threads");
   constexpr int NA = BM * BK / 256, NBt = BN * BK / 256;
-  __shared__ cplx<T> As[BK][BM];
+  // A rows padded by 4: the transposing stores (8 k values x 4 rows per warp) hit
+  // 32 distinct slots
+  __shared__ cplx<T> As[BK][BM + 4];
   __shared__ cplx<T> Bs[BK][BN];
   const GemmTask tk = tasks[blockIdx.x];
   const int fq = blockIdx.y;
