@@ -204,7 +204,8 @@ def schur_kernel_name(s, used):
     """The Schur-update kernels the plan's autotuner picked, with their level counts."""
     if used == 'mixed':
         names = ['tc::front_tc_gemm_kernel (tcgen05 3xTF32, one CTA per tile)',
-                 'tc::front_tc_gemm_persistent (tcgen05 3xTF32, warp-specialised)']
+                 'tc::front_tc_gemm_persistent (tcgen05 3xTF32, warp-specialised)',
+                 'front_gemm_kernel<float> (SIMT FP32 128x64)']
     else:
         names = ['front_gemm_kernel<double> SIMT 128x64', 'front_gemm_kernel<double> SIMT 64x64',
                  'front_dmma_kernel<2,2> (FP64 DMMA 64x64)']

@@ -189,8 +189,9 @@ int ss_adjoint_gradient(ss_handle *h, int n_f, const double *omega, double V, in
  *  16 Schur GEMM launches, 17 device time of the last ss_sweep (ms, CUDA events),
  *  18 refinement / Krylov steps of the last ss_sweep (sum over points),
  *  19 precision the last ss_sweep ran in (SS_PREC_FP64 or SS_PREC_MIXED),
- *  20-22 levels whose Schur update uses the autotuner's candidate 0 (SIMT
- *  128x64), 1 (SIMT 64x64), 2 (FP64 tensor-core DMMA 64x64),
+ *  20-22 levels whose Schur update uses the autotuner's candidate 0, 1, 2
+ *  (FP64 sweep: SIMT 128x64, SIMT 64x64, FP64 tensor-core DMMA 64x64; mixed
+ *  sweep: tcgen05 one CTA per tile, tcgen05 persistent, SIMT FP32 128x64),
  *  23 1 if the panel-step GEMMs use DMMA tiles (128x32 / 32x128), else 0,
  *  24-25 autotuner time of all panel-step GEMMs with SIMT / DMMA tiles (ms),
  *  26 fronts factored whole in shared memory, 27 autotuner time of all

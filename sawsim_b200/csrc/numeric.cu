@@ -1740,8 +1740,13 @@ struct Sweeper {
   void schur_launch(const FrontArgs<T> &b, int l, int c, int nb) {
     const GemmTask *tasks = P.d_tasks.template as<GemmTask>();
     if constexpr (sizeof(T) == 4) {
-      // complex64: candidate 0 one CTA per tile, 1 persistent warp-specialised CTAs
+      // complex64: candidate 0 tcgen05 one CTA per tile, 1 tcgen05 persistent
+      // warp-specialised CTAs, 2 SIMT FP32 tiles of the same 128x64 shape
       const int64_t t0 = P.schur_ptr[l], t1 = P.schur_ptr[l + 1];
+      if (c == 2) {
+        front_gemm_kernel<T, kSquare><<<dim3((unsigned)(t1 - t0), nb), 256, 0, h.stream>>>(b, tasks + t0);
+        return;
+      }
       if (c == 0) {
         tc::front_tc_gemm_kernel<<<dim3((unsigned)(t1 - t0), nb), tc::THREADS, tc::SMEM_BYTES, h.stream>>>(
             reinterpret_cast<cf *>(b.arena), b.stride, b.off, b.ld, tasks + t0, tc_err);
@@ -1767,12 +1772,13 @@ struct Sweeper {
 
   // Autotuner: time every candidate on every level with Schur work, on the chunk's
   // arena before its first factorisation (GEMM time does not depend on the
-  // values), and keep the fastest per level.  SS_SCHUR_TILE=0|1|2 forces one.
+  // values), and keep the fastest per level.  SS_SCHUR_TILE=0|1|2 (FP64) and
+  // SS_SCHUR_TILE_C64=0|1|2 (complex64) force one.
   int tune(int nb) {
     if (P.tuned) return SS_OK;
     const Symbolic &S = h.sym;
     const char *force = getenv(sizeof(T) == 8 ? "SS_SCHUR_TILE" : "SS_SCHUR_TILE_C64");
-    constexpr int NC = sizeof(T) == 8 ? 3 : 2;
+    constexpr int NC = 3;
     P.tune_ms.assign((size_t)NC * S.nlevel, 0.f);
     if (!force) {
       std::vector<cudaEvent_t> e(2 * NC * S.nlevel);
