@@ -299,7 +299,8 @@ def b200_arm(a, rank, world, local):
     if used == 'mixed':
         peak = pk.get('bf16_tflops', 1590.0) / 2
         peak_note = (f'TF32 dense = half the {pk_kind} cuBLAS bf16 burst; achieved counts the algorithmic '
-                     f'complex flops, the 3xTF32 split issues three times as many MMA flops')
+                     f'complex flops over the per-level mix of tcgen05 3xTF32 tiles (which issue three times '
+                     f'as many MMA flops) and SIMT FP32 tiles (nominal FP32 peak about 75 TFLOP/s)')
     else:
         peak = 37.0
         peak_note = 'FP64 nominal 37 TFLOP/s (fallback: MEASURED_PEAKS.json has no FP64 figure)'
