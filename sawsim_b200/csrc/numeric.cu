@@ -324,6 +324,14 @@ constexpr int kPanel = 32;      // panel width of the blocked partial LU
 // 32 rows, a whole front when it is that small (narrow fronts would otherwise
 // make hundreds of thousands of near-empty CTAs)
 static inline int asm_rows(int maxm) { return std::max(32, std::min(maxm, 16384 / std::max(1, maxm))); }
+// Which assembly kernel: the row-owned one for complex64 fronts, the row-chunk one
+// for complex128 (measured: 94.7 vs 92.1 points/s on the Hex27 slab's mixed sweep,
+// 72.4 vs 74.6 on the ME1 cell's FP64 sweep); SS_ASM_BY_ROWS=0|1 overrides.
+template <class T>
+static inline bool asm_by_rows() {
+  if (const char *e = getenv("SS_ASM_BY_ROWS")) return atoi(e) != 0;
+  return sizeof(T) == 4;
+}
 
 // Large fronts, assembly in global memory: CTA (front, frequency, row chunk)
 // zeroes its rows, drops in the arrowhead entries of those rows, then adds the
@@ -398,6 +406,73 @@ __global__ void __launch_bounds__(256) front_assemble_large_kernel(FrontArgs<T> 
         if (dp[u]) *dp[u] = dv[u] + cv[u];
     }
     __syncthreads();
+  }
+}
+
+// The same assembly organised by parent row: a warp owns one row at a time and
+// takes it through zero, arrowhead entries and every child's update row that maps
+// into it (children in order, found by binary search in the child's sorted row
+// map), with only warp-level ordering between the steps.  Each element sees the
+// same operations in the same order as in front_assemble_large_kernel, and a
+// row's zeroes are still in cache when its children's adds arrive.
+constexpr int kAsmRowsPerCta = 32;
+template <class T>
+__global__ void __launch_bounds__(256) front_assemble_rows_kernel(FrontArgs<T> a) {
+  const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
+  const int m = a.m[f], ld = a.ld[f];
+  const int r0 = blockIdx.z * kAsmRowsPerCta;
+  if (r0 >= m) return;
+  const int r1 = min(m, r0 + kAsmRowsPerCta);
+  const double w = a.omega[fq];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  cplx<T> *arena = a.arena + (int64_t)fq * a.stride;
+  cplx<T> *F = arena + a.off[f];
+  const int64_t alo = a.arrow_ptr[f], ahi = a.arrow_ptr[f + 1];
+  for (int r = r0 + wid; r < r1; r += nw) {
+    cplx<T> *row = F + (int64_t)r * ld;
+    for (int c = lane; c < m; c += 32) row[c] = cplx<T>{0, 0};
+    __syncwarp();
+    {
+      // arrow entries are sorted by position: those of row r are one range
+      int64_t b = alo, e = ahi;
+      while (b < e) {
+        const int64_t mid = (b + e) / 2;
+        if (a.arrow_pos[mid] < r * ld) b = mid + 1; else e = mid;
+      }
+      for (int64_t q = b + lane; q < ahi && a.arrow_pos[q] < (r + 1) * ld; q += 32)
+        F[a.arrow_pos[q]] = to_t<T>(a_entry(a.Kc, a.Mc, a.Dc, a.arrow_slot[q], w, a.beta));
+    }
+    __syncwarp();
+    for (int64_t cc = a.child_ptr[f]; cc < a.child_ptr[f + 1]; ++cc) {
+      const int ch = a.child[cc];
+      const int kc = a.k[ch], nn = a.m[ch] - kc, ldc = a.ld[ch];
+      const int *rel = a.relpos + a.relpos_ptr[ch];
+      int b = 0, e = nn;
+      while (b < e) {
+        const int mid = (b + e) / 2;
+        if (rel[mid] < r) b = mid + 1; else e = mid;
+      }
+      if (b == nn || rel[b] != r) continue;
+      const cplx<T> *src = arena + a.off[ch] + (int64_t)(kc + b) * ldc + kc;
+      constexpr int U = 4;
+      for (int j0 = lane; j0 < nn; j0 += 32 * U) {
+        int cj[U];
+        cplx<T> cv[U], dv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int j = j0 + 32 * u;
+          cj[u] = j < nn ? rel[j] : -1;
+          if (cj[u] >= 0) cv[u] = src[j];
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+          if (cj[u] >= 0) dv[u] = row[cj[u]];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+          if (cj[u] >= 0) row[cj[u]] = dv[u] + cv[u];
+      }
+      __syncwarp();
+    }
   }
 }
 
@@ -1862,8 +1937,13 @@ struct Sweeper {
       FrontArgs<T> b = a;
       b.fronts = P.d_large.as<int>() + P.large_ptr[l];
       const int ml = P.maxm_large[l];
-      const int ar = asm_rows(ml);
-      front_assemble_large_kernel<T><<<dim3(nl, nb, (ml + ar - 1) / ar), 256, 0, h.stream>>>(b, ar);
+      if (asm_by_rows<T>()) {
+        front_assemble_rows_kernel<T><<<dim3(nl, nb, (ml + kAsmRowsPerCta - 1) / kAsmRowsPerCta), 256, 0,
+                                        h.stream>>>(b);
+      } else {
+        const int ar = asm_rows(ml);
+        front_assemble_large_kernel<T><<<dim3(nl, nb, (ml + ar - 1) / ar), 256, 0, h.stream>>>(b, ar);
+      }
       ++launches;
       const GemmTask *tasks = P.d_tasks.as<GemmTask>();
       // row/column-parallel panel kernels: CTAs no wider than the level's fronts
