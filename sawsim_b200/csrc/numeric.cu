@@ -2043,8 +2043,9 @@ struct Sweeper {
       front_tfwd_kernel<T><<<dim3(nf, nb), solve_threads(l), sm + kDiagBytes, h.stream>>>(c, cvec, mu, wv, wstride);
       ++launches;
       if (P.lvl_maxu[l] > 0) {
-        const unsigned z = (unsigned)((P.lvl_maxu[l] + 255) / 256);
-        front_tfwd_u12_kernel<T><<<dim3(nf, nb, z), 256, smk, h.stream>>>(c, mu, wv, wstride);
+        const int bs = solve_threads(l);
+        const unsigned z = (unsigned)((P.lvl_maxu[l] + bs - 1) / bs);
+        front_tfwd_u12_kernel<T><<<dim3(nf, nb, z), bs, smk, h.stream>>>(c, mu, wv, wstride);
         ++launches;
       }
     }
@@ -2053,8 +2054,10 @@ struct Sweeper {
       c.fronts = h.d_level_fronts.as<int>() + S.level_ptr[l];
       const int nf = (int)(S.level_ptr[l + 1] - S.level_ptr[l]);
       if (P.lvl_maxu[l] > 0) {
-        const unsigned z = (unsigned)((P.lvl_maxk[l] + 255) / 256);
-        front_tbwd_l21_kernel<T><<<dim3(nf, nb, z), 256, (size_t)P.lvl_maxu[l] * sizeof(cplx<T>), h.stream>>>(c, mu);
+        const int bs = solve_threads(l);
+        const unsigned z = (unsigned)((P.lvl_maxk[l] + bs - 1) / bs);
+        front_tbwd_l21_kernel<T><<<dim3(nf, nb, z), bs, (size_t)P.lvl_maxu[l] * sizeof(cplx<T>), h.stream>>>(c,
+                                                                                                          mu);
         ++launches;
       }
       front_tbwd_kernel<T><<<dim3(nf, nb), solve_threads(l), smk + kDiagBytes + pivb, h.stream>>>(c, mu);

@@ -105,3 +105,22 @@ def test_every_complex64_schur_candidate_converges(mid, tile, monkeypatch):
         e.close()
     assert (st == 0).all()
     assert np.max(np.abs(Q - Q64) / np.abs(Q64)) < 1e-6
+
+
+@pytest.mark.parametrize('precision', ['fp64', 'mixed'])
+def test_assembly_kernels_agree_bit_for_bit(mid, precision, monkeypatch):
+    """The row-chunk and the row-owned front assembly perform the same additions in
+    the same order, so sweeps through either give identical charges."""
+    case, _, _ = mid
+    w = 2 * np.pi * np.linspace(case.freqs[0], case.freqs[-1], 4)
+    Q = []
+    for by_rows in ('0', '1'):
+        monkeypatch.setenv('SS_ASM_BY_ROWS', by_rows)
+        e = cases.engine_for(case)
+        try:
+            q, st, _ = e.charges(w, 1.0, precision)
+        finally:
+            e.close()
+        assert (st == 0).all()
+        Q.append(q)
+    assert np.array_equal(Q[0], Q[1])
