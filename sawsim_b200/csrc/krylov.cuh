@@ -111,8 +111,8 @@ __global__ void norm2_kernel(int64_t n, const cd *__restrict__ w, double *__rest
 }
 
 // out_f = w_f * s[f]
-__global__ void scale_vec_kernel(int64_t n, int nb, const cd *__restrict__ w, const double *__restrict__ s,
-                                 cd *__restrict__ out) {
+// out may be w (in-place scaling): each element is read and written by one thread
+__global__ void scale_vec_kernel(int64_t n, int nb, const cd *w, const double *__restrict__ s, cd *out) {
   const int64_t R = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int f = blockIdx.y;
   if (R >= n) return;

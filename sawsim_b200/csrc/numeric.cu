@@ -1874,9 +1874,8 @@ struct Sweeper {
           cudaEventElapsedTime(&P.tune_ms[c * S.nlevel + l], e[2 * (c * S.nlevel + l)], e[2 * (c * S.nlevel + l) + 1]);
         }
       for (auto &x : e) cudaEventDestroy(x);
-      if constexpr (sizeof(T) == 4) goto picks;
-      {
-      // panel-step GEMMs: all of them once with SIMT tiles, once with DMMA tiles
+      if constexpr (sizeof(T) == 8) {
+      // panel-step GEMMs (FP64): all of them once with SIMT tiles, once with DMMA tiles
       cudaEvent_t pe[4];
       for (auto &x : pe) SS_CK(cudaEventCreate(&x));
       float pt[2] = {0, 0};
@@ -1905,7 +1904,6 @@ struct Sweeper {
     } else {
       P.panel_dmma = sizeof(T) == 8 && atoi(force) == 2;
     }
-  picks:
     for (int l = 0; l < S.nlevel; ++l) {
       int best = 0;
       if (force) {
