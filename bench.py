@@ -290,7 +290,7 @@ def b200_arm(a, rank, world, local):
     pk, pk_kind = peaks()
     schur_flops_launch = s['schur_gemm_flops'] / max(1.0, s['schur_launches'])
     # DRAM bytes of the Schur update per frequency point, from an ncu capture of the
-    # same kernels (profiles/schur_fp64_me1_64x256_traffic.md; 1 and 2 points: the
+    # same kernels (an ncu capture of 1 and 2 points of this cell: the
     # bytes grow in proportion to the points), scaled to the launches of this run
     traffic = None
     if used == 'fp64' and a.case in SCHUR_DRAM_BYTES_PER_POINT:

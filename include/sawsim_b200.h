@@ -140,8 +140,10 @@ int ss_set_damping(ss_handle *h, double beta);
 int ss_sweep(ss_handle *h, int n_f, const double *omega, double V, int precision,
              double *Q, int *status, int *iters);
 
-/* Full DOF vector at one frequency (fields.npz, solver.py:131-140): gdof x 2. */
-int ss_solve_fields(ss_handle *h, double omega, double V, double *disp);
+/* Full DOF vector at one frequency (fields.npz, solver.py:131-140): gdof x 2,
+ * and the charge of the same solve in Q (2 doubles; may be NULL), as
+ * FrequencySolver.solve returns both (sweep.py:335-364). */
+int ss_solve_fields(ss_handle *h, double omega, double V, double *disp, double *Q);
 
 /*
  * Adjoint of the charge at one frequency: lambda (n_active x 2, the reference's
@@ -195,15 +197,41 @@ int ss_adjoint_gradient(ss_handle *h, int n_f, const double *omega, double V, in
  *  23 1 if the panel-step GEMMs use DMMA tiles (128x32 / 32x128), else 0,
  *  24-25 autotuner time of all panel-step GEMMs with SIMT / DMMA tiles (ms),
  *  26 fronts factored whole in shared memory, 27 autotuner time of all
- *  Schur candidates (ms, sum over candidates and levels).
+ *  Schur candidates (ms, sum over candidates and levels),
+ *  28 device time of the last SS_PREC_AUTO probe (ms), 29 points of the last
+ *  mixed sweep re-solved in FP64 (option fp64_fallback), 30 / 31 Krylov steps of
+ *  the primal / adjoint solves of the last sweep (sums over points), 32 points
+ *  whose mixed refinement did not converge (before any FP64 re-solve), 33 device
+ *  time of the FP64 re-solves (ms, included in 17).  Slots past 35 read 0.
  */
 int ss_stats(const ss_handle *h, double *out, int n);
 
 /*
- * Q9 assembly that allocates nothing (no counterpart in the reference: it
- * serves callers of this library that cannot allocate device memory, e.g.
- * code running while a stream is captured into a CUDA graph, or a host
- * framework that owns all device memory through its own pool).
+ * Solver options, by name (the reference's PARDISO / SuperLU calls,
+ * sweep.py:346-353, take none; these tune the replacement's refinement):
+ *   krylov_restart    FGMRES restart length of the mixed sweep (default 30)
+ *   krylov_cycles     FGMRES restarts (default 4)
+ *   krylov_tol        relative residual target of the primal and adjoint
+ *                     Krylov solves (default 1e-10)
+ *   pivot_tiny_c128   static pivot perturbation of complex128 fronts: a pivot
+ *                     of modulus below it is replaced by it (default 1e-13; the
+ *                     system is equilibrated to unit row and column maxima)
+ *   pivot_tiny_c64    the same for complex64 fronts (default 1e-6)
+ *   fp64_fallback     1: points of a mixed sweep whose refinement does not
+ *                     converge are re-solved in FP64 in the same call (default)
+ *   auto_probe_steps  Krylov steps of SS_PREC_AUTO's probe (default 12)
+ * Options persist in the handle; changing one drops a kept SS_PREC_AUTO
+ * decision.  SS_EINVAL for an unknown name or a value out of range.
+ */
+int ss_set_option(ss_handle *h, const char *name, double value);
+
+/*
+ * Q9 assembly that allocates nothing (no counterpart in the reference).  It is
+ * for callers of this library that may not allocate device memory: a host
+ * framework that hands out all device memory from its own pool (a caching
+ * allocator, a serving runtime with a fixed memory budget) and forbids
+ * allocations behind its back.  Such a caller still owns every input and
+ * output buffer; only the scratch is fixed.
  *
  * Every pointer is a device pointer the caller owns: the mesh and materials as
  * for ss_set_mesh / ss_set_materials (materials already zero-lifted for
@@ -211,16 +239,23 @@ int ss_stats(const ss_handle *h, double *out, int n);
  * clamps the ratio), and the global pattern: indptr (ndisp+1)*n_nodes+1 row
  * pointers of the component-major K layout and the node adjacency nadj_ptr /
  * nadj (sorted neighbours, self included).  K and M (nnz complex values each)
- * are zeroed and then filled.  Element matrices go through a fixed internal
- * scratch of 512 elements (11.3 MB, allocated with the library image on every
- * GPU that loads it); larger meshes are processed in 512-element batches.
- * Shared slots are summed with atomic adds, so results equal ss_assemble's to
- * rounding, not bit for bit.  The first call on a device resolves the scratch
- * address (make it before any stream capture).  All calls share the scratch:
- * calls that overlap on the GPU (other streams, other threads) race.  The call
- * synchronises `stream` (a cudaStream_t, NULL for the legacy default stream)
- * and returns SS_EINVAL when the pattern does not contain an element's node
- * pair.
+ * are zeroed and then filled.
+ *
+ * Scratch: element matrices go through one fixed file-scope device array of
+ * 512 elements (11.3 MB), which every GPU that loads the library holds until
+ * the process exits; larger meshes are processed in 512-element batches.  All
+ * calls share that array and it keeps the last call's contents, so calls that
+ * overlap on the GPU (other streams, other host threads) race.  Shared slots are
+ * summed with atomic adds, so results equal ss_assemble's to rounding, not bit
+ * for bit.  The first call on a device, with that device current, resolves the
+ * array's device address and keeps it for the life of the process: make that
+ * first call before any stream capture, and do not call this entry point on a
+ * device after cudaDeviceReset of that device.
+ *
+ * The call synchronises `stream` (a cudaStream_t, NULL for the legacy default
+ * stream) to read back its pattern check, and returns SS_EINVAL when the
+ * pattern does not contain an element's node pair (the skipped entries are
+ * then missing from K and M).
  */
 int ss_assemble_q9_noalloc(int ndisp, int64_t n_nodes, const double *pos, int64_t n_elem,
                            const int64_t *conn, const int32_t *elem_mat, const double *rho,

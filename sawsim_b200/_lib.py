@@ -43,11 +43,12 @@ SIGNATURES = [
     ('ss_analyze', C.c_int, [_P]),
     ('ss_set_damping', C.c_int, [_P, C.c_double]),
     ('ss_sweep', C.c_int, [_P, C.c_int, _DP, C.c_double, C.c_int, _DP, _IP, _IP]),
-    ('ss_solve_fields', C.c_int, [_P, C.c_double, C.c_double, _DP]),
+    ('ss_solve_fields', C.c_int, [_P, C.c_double, C.c_double, _DP, _DP]),
     ('ss_solve_adjoint', C.c_int, [_P, C.c_double, C.c_int, _DP]),
     ('ss_adjoint_gradient', C.c_int, [_P, C.c_int, _DP, C.c_double, C.c_int, C.c_int, _DP, _DP, _DP, _DP, _DP, _DP,
                                       _DP, _DP, _DP, _IP]),
     ('ss_stats', C.c_int, [_P, _DP, C.c_int]),
+    ('ss_set_option', C.c_int, [_P, C.c_char_p, C.c_double]),
     ('ss_assemble_q9_noalloc', C.c_int, [C.c_int, C.c_int64, _P, C.c_int64, _P, _P, _P, _P, _P, _P, C.c_int, _P, _P,
                                          _P, _P, _P, _P, C.c_double, _P, _P, _P, C.c_int64, _P, _P, _P]),
 ]

@@ -1,13 +1,11 @@
 // Allocation-free Q9 assembly entry point.
 //
-// Some callers cannot call cudaMalloc: code running while a CUDA stream is
-// being captured into a graph, code inside a framework that owns all device
-// memory through its own pool (a caching allocator, a serving runtime with a
-// fixed memory budget), or real-time loops where an allocation's implicit
-// synchronisation is not allowed.  ss_assemble_q9_noalloc gives them the GPU
-// Q9 assembly with no allocation at all: inputs and outputs are device buffers
-// the caller already owns, and the element-matrix scratch lives in a fixed
-// file-scope __device__ array below.
+// Some callers of this library may not call cudaMalloc: a host framework that
+// hands out all device memory from its own pool (a caching allocator, a serving
+// runtime with a fixed memory budget) and forbids allocations behind its back.
+// ss_assemble_q9_noalloc gives them the GPU Q9 assembly with no allocation at
+// all: inputs and outputs are device buffers the caller already owns, and the
+// element-matrix scratch lives in a fixed file-scope __device__ array below.
 #include "ss_internal.h"
 #include "dev_complex.cuh"
 #include "q9_element.cuh"
@@ -38,7 +36,9 @@ NoAllocPtrs g_ptrs[kMaxDevices];
 std::mutex g_mu;
 
 // Host code must not use the arrays' names as device addresses: resolve them
-// once per device, with that device current.
+// once per device, with that device current, on the first call there.  The
+// addresses are kept for the life of the process (a cudaDeviceReset of the
+// device would make them stale; the header tells callers not to do that).
 int noalloc_setup(int dev, NoAllocPtrs &out) {
   std::lock_guard<std::mutex> lk(g_mu);
   NoAllocPtrs &p = g_ptrs[dev];

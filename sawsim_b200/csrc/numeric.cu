@@ -1604,16 +1604,14 @@ int launch_condense(Handle &h) {
 
 namespace ss {
 
-constexpr int kKrylovM = 30;            // FGMRES restart length (mixed precision)
-constexpr int kKrylovRestarts = 4;
-// relative residual target of the primal and adjoint Krylov solves: with the
-// dual-weighted correction the charge error is the product of the two
-// residuals' effects, ~1e-12 relative at this target
-constexpr double kKrylovTol = 1e-10;
+// Krylov settings of one sweep: FGMRES restart length, restarts and the relative
+// residual target of the primal and adjoint solves (the handle's options; with
+// the dual-weighted correction the charge error is the product of the two
+// residuals' effects, ~1e-12 relative at the default target 1e-10)
 struct SweepOpts {
-  int krylov_m = kKrylovM;
-  int restarts = kKrylovRestarts;
-  double tol = kKrylovTol;
+  int krylov_m = 30;
+  int restarts = 4;
+  double tol = 1e-10;
 };
 
 // Fronts with m up to this are factored whole in shared memory (one CTA each);
@@ -2214,7 +2212,7 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
   a.stride = S.arena;
   a.piv = piv.as<int>();
   a.n = n;
-  a.tiny = sizeof(T) == 8 ? (T)1e-13 : (T)1e-6;
+  a.tiny = sizeof(T) == 8 ? (T)h.opt.tiny_c128 : (T)h.opt.tiny_c64;
   a.nperturb = npert.as<int>();
   sw.wstride = W;
   const int maxit = sizeof(T) == 8 ? 1 : 40;   // FP64: one refinement step
@@ -2233,7 +2231,8 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
   cudaEventCreate(&eall0);
   cudaEventCreate(&eall1);
   cudaEventRecord(eall0, h.stream);
-  int perturbed = 0;
+  int perturbed = 0, nfail = 0;
+  int64_t steps_p = 0, steps_a = 0;
   for (int c0 = 0; c0 < n_f; c0 += B) {
     const int nb = std::min(B, n_f - c0);
     SS_CK(cudaMemcpyAsync(dom.p, omega + c0, nb * sizeof(double), cudaMemcpyHostToDevice, h.stream));
@@ -2267,7 +2266,7 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
       rc = fgmres(h, kw, opA, nb, krylov_m, krylov_restarts, tol_p, a.Kc, a.Mc, a.Dc, dom.as<double>(), b.as<cd>(),
                   x.as<cd>(), pre, kits, kconv);
       if (rc) return rc;
-      for (int f = 0; f < nb; ++f) hit[f] = kits[f], conv[f] = kconv[f];
+      for (int f = 0; f < nb; ++f) hit[f] = kits[f], conv[f] = kconv[f], steps_p += kits[f];
     }
     if (getenv("SS_DEBUG_IR")) {
       // backward error of the direct solve: |b - A x| / |b|, and the solution size
@@ -2319,7 +2318,7 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
         rc = fgmres(h, kw, opT, nb, krylov_m, krylov_restarts, tol_a, a.Kc, a.Mc, a.Dc, dom.as<double>(),
                     cvec.as<cd>(), mu.as<cd>(), pre, kits, kconv);
         if (rc) return rc;
-        for (int f = 0; f < nb; ++f) hit[f] += kits[f], aconv[f] = kconv[f];
+        for (int f = 0; f < nb; ++f) hit[f] += kits[f], aconv[f] = kconv[f], steps_a += kits[f];
       } else {
         // one FP64 refinement step, as for the primal solution
         residual_kernel<<<dim3(vb, spmv_blocks(nb)), 256, 0, h.stream>>>(n, nb, opT.rp, opT.ci, opT.vp, a.Kc, a.Mc, a.Dc,
@@ -2355,7 +2354,9 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
         Qout[2 * (int64_t)(c0 + f)] += corr[f].x;
         Qout[2 * (int64_t)(c0 + f) + 1] += corr[f].y;
       }
-      if (status) status[c0 + f] = (sizeof(T) == 4 && !(conv[f] && aconv[f])) ? SS_ENOCONV : SS_OK;
+      const bool ok = !(sizeof(T) == 4 && !(conv[f] && aconv[f]));
+      nfail += !ok;
+      if (status) status[c0 + f] = ok ? SS_OK : SS_ENOCONV;
       if (iters) iters[c0 + f] = hit[f];
     }
     if (disp) {
@@ -2403,6 +2404,9 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
   h.st[17] = total_ms;
   h.st[14] = perturbed;
   h.st[15] = sw.launches;
+  h.st[30] = (double)steps_p;
+  h.st[31] = (double)steps_a;
+  h.st[32] = nfail;
   h.st[20] = h.st[21] = h.st[22] = 0;
   h.st[23] = P.panel_dmma ? 1.0 : 0.0;
   h.st[24] = P.panel_ms[0];
@@ -2422,14 +2426,31 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
 }
 
 // SS_PREC_AUTO: a probe of the mixed sweep on the band's two end points with a
-// short Krylov budget (12 steps each for the primal and the adjoint); if both
-// converge the whole sweep runs mixed, otherwise FP64 (the complex64 factors of a
-// cell whose conditioning defeats FP32 would need many Krylov steps per point).
-// The decision is kept for the band's end points until the system changes, so a
-// repeated sweep of the same band probes once.
+// short Krylov budget (the handle's auto_probe_steps, 12 by default, for the
+// primal and the adjoint); if both converge the whole sweep runs mixed, otherwise
+// FP64 (the complex64 factors of a cell whose conditioning defeats FP32 would
+// need many Krylov steps per point).  The decision is kept for the band's end
+// points until the system or an option changes, so a repeated sweep of the same
+// band probes once; the probe's device time is kept in stats slot 28.
+//
+// A mixed sweep whose refinement leaves points unconverged re-solves those points
+// with the FP64 path in the same call (option fp64_fallback, on by default), so
+// every point returned has SS_OK unless FP64 fails too.
 int run_sweep(Handle &h, int n_f, const double *omega, double V, int precision, double *Q, int *status,
               int *iters, double *disp_out, const SweepExtra *ex) {
   SweepOpts opt;
+  opt.krylov_m = h.opt.krylov_m;
+  opt.restarts = h.opt.krylov_cycles;
+  opt.tol = h.opt.krylov_tol;
+  std::vector<int> st_local, it_local;
+  if (!status) {
+    st_local.assign(std::max(0, n_f), 0);
+    status = st_local.data();
+  }
+  if (!iters) {
+    it_local.assign(std::max(0, n_f), 0);
+    iters = it_local.data();
+  }
   int rc;
   double probe_ms = 0, probe_launches = 0;
   if (precision == SS_PREC_AUTO && n_f > 0 && h.auto_prec >= 0 && h.auto_w0 == omega[0] &&
@@ -2439,9 +2460,9 @@ int run_sweep(Handle &h, int n_f, const double *omega, double V, int precision, 
     const double ends[2] = {omega[0], omega[n_f - 1]};
     double q[4];
     int st[2] = {0, 0}, it[2] = {0, 0};
-    SweepOpts probe;
+    SweepOpts probe = opt;
     probe.restarts = 1;
-    probe.krylov_m = 12;
+    probe.krylov_m = h.opt.auto_probe_m;
     rc = sweep_impl<float>(h, n_f > 1 ? 2 : 1, ends, V, q, st, it, nullptr, nullptr, probe);
     if (rc) return rc;
     precision = (st[0] == SS_OK && st[1] == SS_OK) ? SS_PREC_MIXED : SS_PREC_FP64;
@@ -2450,15 +2471,65 @@ int run_sweep(Handle &h, int n_f, const double *omega, double V, int precision, 
     h.auto_prec = precision;
     probe_ms = h.st[17];
     probe_launches = h.st[15];
+    h.st[28] = probe_ms;
   }
   if (precision == SS_PREC_MIXED)
     rc = sweep_impl<float>(h, n_f, omega, V, Q, status, iters, disp_out, ex, opt);
   else
     rc = sweep_impl<double>(h, n_f, omega, V, Q, status, iters, disp_out, ex, opt);
+  if (rc) return rc;
   h.st[19] = precision;
+  h.st[29] = 0;
+  h.st[33] = 0;
+  if (precision == SS_PREC_MIXED && h.opt.fp64_fallback) {
+    // maximal runs of consecutive unconverged points, each re-solved in FP64
+    std::vector<std::pair<int, int>> runs;
+    for (int i = 0; i < n_f;) {
+      if (status[i] != SS_ENOCONV) {
+        ++i;
+        continue;
+      }
+      int j = i;
+      while (j < n_f && status[j] == SS_ENOCONV) ++j;
+      runs.emplace_back(i, j);
+      i = j;
+    }
+    if (!runs.empty()) {
+      double keep[Handle::kStats];
+      std::copy(h.st, h.st + Handle::kStats, keep);
+      double fb_ms = 0, fb_launches = 0;
+      int resolved = 0;
+      for (const auto &r : runs) {
+        const int i0 = r.first, len = r.second - r.first;
+        SweepExtra exr;
+        if (ex && ex->per_chunk)
+          exr.per_chunk = [ex, i0](int c0, int nb, const cplx<double> *x, const cplx<double> *mu) {
+            return ex->per_chunk(c0 + i0, nb, x, mu);
+          };
+        std::vector<int> it2(len, 0);
+        rc = sweep_impl<double>(h, len, omega + i0, V, Q + 2 * (int64_t)i0, status + i0, it2.data(),
+                                disp_out, ex ? &exr : nullptr, opt);
+        if (rc) return rc;
+        for (int f = 0; f < len; ++f) iters[i0 + f] += it2[f];
+        fb_ms += h.st[17];
+        fb_launches += h.st[15];
+        resolved += len;
+      }
+      std::copy(keep, keep + Handle::kStats, h.st);
+      h.st[17] += fb_ms;
+      h.st[15] += fb_launches;
+      h.st[29] = resolved;
+      h.st[33] = fb_ms;
+    }
+  }
   h.st[17] += probe_ms;        // the probe is part of an AUTO sweep's device time
   h.st[15] += probe_launches;
-  return rc;
+  {
+    double tot = 0;
+    for (int i = 0; i < n_f; ++i) tot += iters[i];
+    h.st[18] = tot;
+  }
+  return SS_OK;
 }
 
 }  // namespace ss

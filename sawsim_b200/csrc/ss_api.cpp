@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <cstring>
 #include <new>
 
@@ -297,18 +298,53 @@ extern "C" int ss_sweep(ss_handle *hp, int n_f, const double *omega, double V, i
   return run_sweep(h, n_f, omega, V, precision, Q, status, iters, nullptr);
 }
 
-extern "C" int ss_solve_fields(ss_handle *hp, double omega, double V, double *disp) {
+extern "C" int ss_solve_fields(ss_handle *hp, double omega, double V, double *disp, double *Q) {
   H_CHECK(hp);
   if (!h.analyzed) return fail(h, SS_ESTATE, "fields: analyze first");
   if (!disp || !(omega > 0.0) || V == 0.0) return fail(h, SS_EINVAL, "fields: bad arguments");
-  double Q[2];
+  double q[2];
   int st = 0, it = 0;
-  return run_sweep(h, 1, &omega, V, SS_PREC_FP64, Q, &st, &it, disp);
+  const int rc = run_sweep(h, 1, &omega, V, SS_PREC_FP64, q, &st, &it, disp);
+  if (rc == SS_OK && Q) Q[0] = q[0], Q[1] = q[1];
+  return rc;
 }
 
 extern "C" int ss_stats(const ss_handle *hp, double *out, int n) {
   if (!hp || !out || n < 0) return SS_EINVAL;
-  for (int i = 0; i < n && i < 28; ++i) out[i] = hp->h.st[i];
+  for (int i = 0; i < n && i < Handle::kStats; ++i) out[i] = hp->h.st[i];
+  for (int i = Handle::kStats; i < n; ++i) out[i] = 0.0;
+  return SS_OK;
+}
+
+extern "C" int ss_set_option(ss_handle *hp, const char *name, double value) {
+  H_CHECK(hp);
+  if (!name) return fail(h, SS_EINVAL, "option: null name");
+  const std::string k(name);
+  Handle::Options &o = h.opt;
+  auto whole = [&](double lo, double hi) { return value == std::floor(value) && value >= lo && value <= hi; };
+  if (k == "krylov_restart") {
+    if (!whole(1, 200)) return fail(h, SS_EINVAL, "option krylov_restart: integer in [1, 200]");
+    o.krylov_m = (int)value;
+  } else if (k == "krylov_cycles") {
+    if (!whole(1, 100)) return fail(h, SS_EINVAL, "option krylov_cycles: integer in [1, 100]");
+    o.krylov_cycles = (int)value;
+  } else if (k == "krylov_tol") {
+    if (!(value > 0.0 && value < 1.0)) return fail(h, SS_EINVAL, "option krylov_tol: in (0, 1)");
+    o.krylov_tol = value;
+  } else if (k == "pivot_tiny_c128" || k == "pivot_tiny_c64") {
+    if (!(value >= 0.0 && value < 1.0)) return fail(h, SS_EINVAL, "option pivot_tiny: in [0, 1)");
+    (k == "pivot_tiny_c128" ? o.tiny_c128 : o.tiny_c64) = value;
+    free_plans(h);   // the captured factorisation graphs bake the threshold in
+  } else if (k == "fp64_fallback") {
+    if (!whole(0, 1)) return fail(h, SS_EINVAL, "option fp64_fallback: 0 or 1");
+    o.fp64_fallback = (int)value;
+  } else if (k == "auto_probe_steps") {
+    if (!whole(1, 200)) return fail(h, SS_EINVAL, "option auto_probe_steps: integer in [1, 200]");
+    o.auto_probe_m = (int)value;
+  } else {
+    return fail(h, SS_EINVAL, "option: unknown name '" + k + "'");
+  }
+  h.auto_prec = -1;   // a kept SS_PREC_AUTO decision was taken under the old options
   return SS_OK;
 }
 

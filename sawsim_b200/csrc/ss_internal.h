@@ -144,8 +144,19 @@ struct Handle {
   int auto_prec = -1;
   DBuf dKs, dMs, dDs;                    // equilibrated condensed values
   double scale_w = -1;                   // frequency the scaling was computed at
+  // solver options (ss_set_option); kept until changed
+  struct Options {
+    int krylov_m = 30;                   // FGMRES restart length of the mixed sweep
+    int krylov_cycles = 4;               // FGMRES restarts
+    double krylov_tol = 1e-10;           // relative residual target (primal and adjoint)
+    double tiny_c128 = 1e-13;            // static pivot perturbation, complex128 fronts
+    double tiny_c64 = 1e-6;              // static pivot perturbation, complex64 fronts
+    int fp64_fallback = 1;               // re-solve unconverged mixed points in FP64
+    int auto_probe_m = 12;               // Krylov steps of SS_PREC_AUTO's probe
+  } opt;
   // stats
-  double st[28] = {0};
+  static constexpr int kStats = 36;
+  double st[kStats] = {0};
 };
 
 // ---------------------------------------------------------------- kernels

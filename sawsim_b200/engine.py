@@ -154,16 +154,24 @@ class FrequencySolver:
         self._h('ss_analyze')
 
     # ------------------------------------------------------------------ queries
+    STAT_KEYS = ['n_active', 'n_fronts', 'max_front', 'factor_flops_per_point', 'nnz_lu', 'analyze_s',
+                 'assemble_ms', 'sweep_ms', 'factor_ms', 'solve_ms', 'chunk', 'schur_gemm_ms',
+                 'schur_gemm_flops', 'levels', 'perturbed_pivots', 'launches', 'schur_launches',
+                 'sweep_device_ms', 'refine_solves', 'precision_used', 'schur_tile_simt128', 'schur_tile_simt64',
+                 'schur_tile_dmma', 'panel_gemm_dmma', 'panel_tune_simt_ms', 'panel_tune_dmma_ms', 'small_fronts',
+                 'schur_tune_ms', 'auto_probe_ms', 'fp64_resolved', 'krylov_steps_primal', 'krylov_steps_adjoint',
+                 'mixed_not_converged', 'fp64_resolve_ms']
+
     def stats(self) -> dict:
-        out = np.zeros(28)
-        self._h('ss_stats', L.ptr(out, C.c_double), 28)
-        keys = ['n_active', 'n_fronts', 'max_front', 'factor_flops_per_point', 'nnz_lu', 'analyze_s',
-                'assemble_ms', 'sweep_ms', 'factor_ms', 'solve_ms', 'chunk', 'schur_gemm_ms',
-                'schur_gemm_flops', 'levels', 'perturbed_pivots', 'launches', 'schur_launches',
-                'sweep_device_ms', 'refine_solves', 'precision_used', 'schur_tile_simt128', 'schur_tile_simt64',
-                'schur_tile_dmma', 'panel_gemm_dmma', 'panel_tune_simt_ms', 'panel_tune_dmma_ms', 'small_fronts',
-                'schur_tune_ms']
-        return dict(zip(keys, out.tolist()))
+        n = len(self.STAT_KEYS)
+        out = np.zeros(n)
+        self._h('ss_stats', L.ptr(out, C.c_double), n)
+        return dict(zip(self.STAT_KEYS, out.tolist()))
+
+    def set_option(self, name: str, value: float):
+        """Solver option by name (``ss_set_option``): krylov_restart, krylov_cycles,
+        krylov_tol, pivot_tiny_c128, pivot_tiny_c64, fp64_fallback, auto_probe_steps."""
+        self._h('ss_set_option', name.encode(), float(value))
 
     @property
     def n_active(self) -> int:
@@ -200,9 +208,10 @@ class FrequencySolver:
     def solve(self, omega: float, V: float = 1.0):
         """One point: ``(disp, Q, |Y|)`` like ``FrequencySolver.solve`` (sweep.py:335-364)."""
         disp = np.zeros(2 * self.gdof)
-        self._h('ss_solve_fields', float(omega), float(V), L.ptr(disp, C.c_double))
-        Q, _, _ = self.charges([omega], V, 'fp64')
-        return disp.view(np.complex128), Q[0], abs(1j * omega * Q[0] / V)
+        q = np.zeros(2)
+        self._h('ss_solve_fields', float(omega), float(V), L.ptr(disp, C.c_double), L.ptr(q, C.c_double))
+        Q = complex(q[0], q[1])
+        return disp.view(np.complex128), Q, abs(1j * omega * Q / V)
 
     def solve_adjoint(self, omega: float, precision: str = 'fp64'):
         """lambda (complex, n_active, active-DOF order) with A_aa^T lambda = kq, the

@@ -23,6 +23,7 @@ from __future__ import annotations
 
 import hashlib
 import json
+import os
 import sys
 from pathlib import Path
 
@@ -30,7 +31,8 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parents[1]
-REF = Path('/root/reference')
+# the reference checkout: SAWSIM_REFERENCE, else where the build container mounts it
+REF = Path(os.environ.get('SAWSIM_REFERENCE', '/root/reference'))
 sys.path.insert(0, str(REPO))
 sys.path.insert(0, str(REF / 'src'))
 

@@ -17,6 +17,7 @@ stands in for it (no Gmsh call is made on this path).  The GPU box never reads
 """
 from __future__ import annotations
 
+import os
 import sys
 import types
 from pathlib import Path
@@ -26,7 +27,8 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parents[1]
 sys.path.insert(0, str(REPO))
-sys.path.insert(0, '/root/reference/src')
+# the reference checkout: SAWSIM_REFERENCE, else where the build container mounts it
+sys.path.insert(0, str(Path(os.environ.get('SAWSIM_REFERENCE', '/root/reference')) / 'src'))
 sys.modules.setdefault('gmsh', types.ModuleType('gmsh'))
 
 from sawsim.saw2d.saw3d.assembly import form_stiffness_mass_3d          # noqa: E402

@@ -19,13 +19,15 @@ codes.  The GPU box never reads /root/reference.
 from __future__ import annotations
 
 import json
+import os
 import sys
 from pathlib import Path
 
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REF = Path('/root/reference')
+# the reference checkout: SAWSIM_REFERENCE, else where the build container mounts it
+REF = Path(os.environ.get('SAWSIM_REFERENCE', '/root/reference'))
 sys.path.insert(0, str(REF / 'src'))
 
 from sawsim.metrics import resonances  # noqa: E402
