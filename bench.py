@@ -51,6 +51,7 @@ def parse():
     p.add_argument('--case', default='me1_64x256')
     p.add_argument('--points', type=int, default=None)
     p.add_argument('--no-cpu-baseline', action='store_true')
+    p.add_argument('--no-modes', action='store_true', help='skip the untimed FP64-vs-mixed comparison')
     return p.parse_args()
 
 
@@ -214,6 +215,105 @@ def schur_kernel_name(s, used):
     return 'Schur update F22 -= F21 F12: ' + ', '.join(parts)
 
 
+def _sweep_stats(eng, w, precision, reps):
+    """Device time of `reps` sweeps after one untimed sweep (plan, tuner, graphs)."""
+    eng.charges(w, 1.0, precision)
+    ms, out = [], None
+    for _ in range(reps):
+        Q, st, it = eng.charges(w, 1.0, precision)
+        s = eng.stats()
+        ms.append(s['sweep_device_ms'])
+        out = (Q, st, it, s)
+    return float(np.median(ms)), out
+
+
+def mode_comparison(eng, f, w, reps):
+    """FP64 and mixed sweeps of the same points: rates, refinement and the mixed
+    sweep's Y11 / fr / fa error against FP64 (the metric's comparison)."""
+    from sawsim_b200.metrics import compare, resonances
+    res = {}
+    Ys = {}
+    for prec in ('fp64', 'mixed'):
+        ms, (Q, st, it, s) = _sweep_stats(eng, w, prec, reps)
+        Ys[prec] = -1j * w * Q
+        res[prec] = dict(points_per_s=w.size / (ms * 1e-3), ms_per_sweep=ms, chunk=int(s['chunk']),
+                         points_not_ok=int(np.sum(st != 0)))
+        if prec == 'mixed':
+            res[prec].update(krylov_steps_per_point=(s['krylov_steps_primal'] + s['krylov_steps_adjoint']) / w.size,
+                             refinement_not_converged=int(s['mixed_not_converged']),
+                             points_resolved_in_fp64=int(s['fp64_resolved']),
+                             fp64_resolve_ms=s['fp64_resolve_ms'])
+    d = compare(resonances(f, Ys['fp64']), resonances(f, Ys['mixed']))
+    res['mixed'].update(
+        y11_max_rel_err_vs_fp64=float(np.max(np.abs(Ys['mixed'] - Ys['fp64']) / np.abs(Ys['fp64']))),
+        fr_diff_khz_vs_fp64=None if d['fr_diff_mhz'] is None else d['fr_diff_mhz'] * 1e3,
+        fa_diff_khz_vs_fp64=None if d['fa_diff_mhz'] is None else d['fa_diff_mhz'] * 1e3)
+    res['ratio_mixed_over_fp64'] = res['mixed']['points_per_s'] / res['fp64']['points_per_s']
+    return res
+
+
+def rooflines(eng, c, s, st0, used, schur_ms, nf, pk, pk_kind, ceilings):
+    """Roofline entries: the Schur update (tensor), the triangular solves and the
+    assembly (HBM), each from this run's CUDA-event times and the algorithmic work
+    of the project's symbolic analysis."""
+    out = []
+    launches = max(1.0, s['schur_launches'])
+    flops_launch = s['schur_gemm_flops'] / launches
+    ms_launch = float(np.mean(schur_ms)) / launches
+    achieved = flops_launch / (ms_launch * 1e-3) / 1e12 if ms_launch > 0 else None
+    traffic, traffic_note = None, None
+    if used == 'fp64' and c.name in SCHUR_DRAM_BYTES_PER_POINT:
+        traffic = SCHUR_DRAM_BYTES_PER_POINT[c.name] * nf / launches
+        traffic_note = ('dram__bytes_read.sum + dram__bytes_write.sum of the Schur launches in an ncu capture of '
+                        '1 and 2 points of this cell (bytes grow in proportion to the points), scaled to this '
+                        "run's points per launch; not measured in this run")
+    if used == 'mixed':
+        peak = pk.get('bf16_tflops', 1590.0) / 2
+        peak_note = (f'TF32 dense = half the {pk_kind} cuBLAS bf16 burst; achieved counts the algorithmic complex '
+                     f'flops over the per-level mix of tcgen05 3xTF32 tiles (three MMA passes each) and SIMT FP32 '
+                     f'tiles; own-kernel ceilings on dense 2560-row fronts: {ceilings}')
+    else:
+        peak = ceilings.get('fp64_dmma')
+        peak_note = ('measured ceiling of this library\'s FP64 DMMA Schur tile on 8 dense fronts of 2560 rows with '
+                     '512 pivots (ss_measure_gemm_ceiling, median of 5 launches); nominal FP64 tensor peak 37-40 '
+                     'TFLOP/s for context')
+    out.append(dict(kernel=schur_kernel_name(s, used), bound='tensor', achieved=achieved, peak=peak, unit='TFLOP/s',
+                    frac=(achieved / peak) if achieved and peak else None, traffic=traffic,
+                    traffic_unit='bytes per launch', traffic_note=traffic_note, peak_note=peak_note,
+                    flops_per_launch=flops_launch))
+    hbm = pk.get('hbm_gbs', 6650.0)
+    # triangular solves: the first solve of every chunk (forward + backward over all
+    # fronts), algorithmic bytes nnz(L+U) x scalar + 2 n x 16 per point
+    scal = 8 if used == 'mixed' else 16
+    n = st0['n_active']
+    sb = nf * (st0['nnz_lu'] * scal + 2 * n * 16)
+    if s['solve_ms'] > 0:
+        ach = sb / (s['solve_ms'] * 1e-3) / 1e9
+        out.append(dict(kernel='front_fwd* / front_bwd* (batched forward + backward triangular solves, first solve '
+                               'of every chunk)', bound='hbm', achieved=ach, peak=hbm, unit='GB/s', frac=ach / hbm,
+                        traffic=None, bytes_per_point=sb / nf,
+                        peak_note=f'{pk_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)'))
+    # assembly: K and M written on the CSR pattern + coordinates + connectivity +
+    # gather map, element kernel + scatter kernel times of the setup's ss_assemble
+    t_asm = st0['element_kernel_ms'] + st0['scatter_kernel_ms']
+    if t_asm > 0:
+        K = eng.export(0)
+        Mx = eng.export(1)
+        npe = 27 if c.name.startswith('hex') else 9
+        ne = c.hexas.shape[0] if c.name.startswith('hex') else c.mesh.ne
+        N = c.N if c.name.startswith('hex') else c.mesh.N
+        dim = 3 if c.name.startswith('hex') else 2
+        ab = 16 * (K.nnz + Mx.nnz) + 8 * dim * N + 8 * npe * ne + 8 * npe * npe * ne
+        ach = ab / (t_asm * 1e-3) / 1e9
+        out.append(dict(kernel='q9/hex27 element kernel + gather_pairs_kernel (GPU assembly of K and M, once per '
+                               'engine)', bound='hbm', achieved=ach, peak=hbm, unit='GB/s', frac=ach / hbm, traffic=None,
+                        bytes=ab, ms=t_asm,
+                        bytes_note='16 (nnz K + nnz M) written + coordinates + connectivity + 8-byte gather map '
+                                   'entries; the element-matrix scratch round trip is not algorithmic',
+                        peak_note=f'{pk_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)'))
+    return out
+
+
 def b200_arm(a, rank, world, local):
     import torch
     import torch.distributed as dist
@@ -232,8 +332,12 @@ def b200_arm(a, rank, world, local):
     mine = shard(n_total, rank, world)
     w = 2 * np.pi * f_all[mine]
     nf = w.size
-    for _ in range(a.warmup):
+    first_sweep_ms = None
+    for i in range(a.warmup):
         Q, status, iters = eng.charges(w, 1.0, a.precision)
+        if i == 0:
+            first_sweep_ms = eng.stats()['sweep_device_ms']
+    probe_ms = eng.stats()['auto_probe_ms'] if a.precision == 'auto' else None
 
     def barrier():
         if world > 1:
@@ -257,10 +361,9 @@ def b200_arm(a, rank, world, local):
         barrier()
     dev = float(np.sum(dev_ms)) / 1e3
     wall = float(np.sum(wall_s))
-    used = 'mixed' if int(eng.stats()['precision_used']) == 1 else 'fp64'
-    # accuracy of the timed sweep: fr/fa of Y11 = -i w Q / V (solver.py:128), and for a
-    # mixed sweep its Y11 error against an FP64 sweep of the same points (untimed)
-    from sawsim_b200.metrics import compare, resonances
+    used = 'mixed' if int(s_timed['precision_used']) == 1 else 'fp64'
+    # accuracy of the timed sweep: fr/fa of Y11 = -i w Q / V (solver.py:128)
+    from sawsim_b200.metrics import resonances
     if world > 1:
         Q_all = gather_charges(Q, n_total, rank, world)
     else:
@@ -269,42 +372,19 @@ def b200_arm(a, rank, world, local):
     Y = -1j * w_all * Q_all
     res = resonances(f_all, Y)
     acc = dict(fr_ghz=res['fr_ghz'], fa_ghz=res['fa_ghz'], k2eff=res['k2eff'])
-    any_mixed = used == 'mixed'
-    if world > 1:      # every rank takes the same collective steps
-        t = torch.tensor([1.0 if any_mixed else 0.0], device='cuda')
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        any_mixed = bool(t.item() > 0)
-    if any_mixed:
-        Q64, _, _ = eng.charges(w, 1.0, 'fp64')
-        Q64 = gather_charges(Q64, n_total, rank, world) if world > 1 else Q64
-        Y64 = -1j * w_all * Q64
-        d = compare(resonances(f_all, Y64), res)
-        acc.update(y11_max_rel_err_vs_fp64=float(np.max(np.abs(Y - Y64) / np.abs(Y64))),
-                   fr_diff_khz_vs_fp64=None if d['fr_diff_mhz'] is None else d['fr_diff_mhz'] * 1e3,
-                   fa_diff_khz_vs_fp64=None if d['fa_diff_mhz'] is None else d['fa_diff_mhz'] * 1e3)
     if world > 1:
         t = torch.tensor([dev, wall], device='cuda', dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dev, wall = t.tolist()
-    s = s_timed           # counters of the last timed sweep (not of the FP64 accuracy check)
-    pk, pk_kind = peaks()
-    schur_flops_launch = s['schur_gemm_flops'] / max(1.0, s['schur_launches'])
-    # DRAM bytes of the Schur update per frequency point, from an ncu capture of the
-    # same kernels (an ncu capture of 1 and 2 points of this cell: the
-    # bytes grow in proportion to the points), scaled to the launches of this run
-    traffic = None
-    if used == 'fp64' and a.case in SCHUR_DRAM_BYTES_PER_POINT:
-        traffic = SCHUR_DRAM_BYTES_PER_POINT[a.case] * nf / max(1.0, s['schur_launches'])
-    schur_ms_launch = float(np.mean(schur_ms)) / max(1.0, s['schur_launches'])
+    s = s_timed           # counters of the last timed sweep
+    # untimed: both precision modes on this rank's points, and the measured ceilings
+    modes = None if a.no_modes else mode_comparison(eng, f_all[mine], w, 2)
+    ceilings = {'fp64_dmma': eng.gemm_ceiling(0)}
     if used == 'mixed':
-        peak = pk.get('bf16_tflops', 1590.0) / 2
-        peak_note = (f'TF32 dense = half the {pk_kind} cuBLAS bf16 burst; achieved counts the algorithmic '
-                     f'complex flops over the per-level mix of tcgen05 3xTF32 tiles (which issue three times '
-                     f'as many MMA flops) and SIMT FP32 tiles (nominal FP32 peak about 75 TFLOP/s)')
-    else:
-        peak = 37.0
-        peak_note = 'FP64 nominal 37 TFLOP/s (fallback: MEASURED_PEAKS.json has no FP64 figure)'
-    achieved = schur_flops_launch / (schur_ms_launch * 1e-3) / 1e12 if schur_ms_launch > 0 else None
+        ceilings.update(c64_tcgen05=eng.gemm_ceiling(2), c64_tcgen05_persistent=eng.gemm_ceiling(3),
+                        c64_simt=eng.gemm_ceiling(4))
+    pk, pk_kind = peaks()
+    roof = rooflines(eng, c, s, st0, used, schur_ms, nf, pk, pk_kind, ceilings)
     line = None
     if rank == 0:
         cpu = None
@@ -312,6 +392,7 @@ def b200_arm(a, rank, world, local):
             workers = min(8, os.cpu_count() or 1)
             v, sample = cpu_sweep_sample(a.case, 2 * workers, workers)
             cpu = dict(value=v, unit='points/s', cores=workers, kind='port', sample=sample)
+            acc.update(oracle_check(c, eng, a.case))
         bad = int(np.sum(status != 0))
         line = dict(metric=METRIC, value=world * nf * a.steps / dev, unit='points/s', n_gpus=world,
                     steps=a.steps, warmup=a.warmup, ms_per_step=dev * 1e3 / a.steps, higher_is_better=True,
@@ -319,25 +400,45 @@ def b200_arm(a, rank, world, local):
                     data='synthetic',
                     config=dict(workload=workload_name(c),
                                 precision=a.precision, precision_used=used, accuracy=acc,
-                                auto_probe=('probed on the first (warm-up) sweep of the band; the repeated sweeps '
-                                            'keep the decision' if a.precision == 'auto' else None),
+                                auto_probe_ms=probe_ms, first_sweep_ms=first_sweep_ms,
+                                auto_note=('SS_PREC_AUTO probes the mixed path on the band ends in the first sweep '
+                                           '(first_sweep_ms includes it, auto_probe_ms is its share); the timed '
+                                           'sweeps keep the decision' if a.precision == 'auto' else None),
+                                modes=modes,
                                 n_active=int(st0['n_active']), fronts=int(st0['n_fronts']),
                                 factor_gflop_per_point=st0['factor_flops_per_point'] / 1e9,
                                 setup_s=setup_s, analyze_s=st0['analyze_s'], assemble_ms=st0['assemble_ms'],
                                 l2='inputs larger than L2 (front arena of GBs per chunk)',
                                 chunk=int(s['chunk']), points_not_converged=bad,
-                                mean_refinement_steps=float(np.mean(iters)), parallelism=f'interleaved frequency shards x{world}' if world > 1 else 'one GPU'),
+                                mean_refinement_steps=float(np.mean(iters)),
+                                parallelism=f'interleaved frequency shards x{world}' if world > 1 else 'one GPU'),
                     e2e=dict(value=world * nf * a.steps / wall, unit='points/s', h2d_bytes_per_step=8 * nf,
                              d2h_bytes_per_step=16 * nf + 8 * nf),
                     gpu_launches=launches,
-                    roofline=dict(kernel=schur_kernel_name(s, used),
-                                  bound='tensor',
-                                  achieved=achieved, peak=peak, unit='TFLOP/s',
-                                  frac=(achieved / peak) if achieved else None, traffic=traffic, traffic_unit='bytes per launch',
-                                  peak_note=peak_note,
-                                  flops_per_launch=schur_flops_launch),
+                    roofline=roof[0], rooflines=roof, gemm_ceilings_tflops=ceilings,
                     clocks=clk.summary(), cpu_baseline=cpu)
     return line
+
+
+def oracle_check(c, eng, case_name):
+    """Part of the CPU-baseline leg: the oracle (the CPU restatement of the
+    reference) assembles and condenses the same cell, and the GPU FP64 solutions
+    at two sampled points are checked in the oracle's own system (normwise
+    backward error)."""
+    sys.path.insert(0, str(REPO / 'oracle'))
+    from helpers_cpu import oracle_solver_for
+    o = oracle_solver_for(case_name)
+    out = []
+    for fi in c.freqs[[len(c.freqs) // 3, 2 * len(c.freqs) // 3]]:
+        wi = 2 * np.pi * fi
+        A, rhs = o.system(wi)
+        disp, _, _ = eng.solve(wi)
+        x = disp[o.active]
+        r = A @ x - rhs
+        eta = np.linalg.norm(r, np.inf) / (abs(A).sum(axis=1).max() * np.linalg.norm(x, np.inf) +
+                                           np.linalg.norm(rhs, np.inf))
+        out.append(dict(f_ghz=fi / 1e9, backward_error=float(eta)))
+    return dict(fp64_backward_error_in_oracle_system=out)
 
 
 def main():

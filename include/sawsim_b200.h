@@ -50,7 +50,7 @@ typedef struct ss_handle ss_handle;
                               decision is kept for the same two end
                               frequencies until the system changes               */
 
-/* matrix selectors for ss_set_csr / ss_export_csr */
+/* matrix selectors for ss_export_csr */
 #define SS_MAT_K    0      /* global stiffness                                   */
 #define SS_MAT_M    1      /* global mass                                        */
 #define SS_MAT_D    2      /* global damping (Rayleigh beta*D part)              */
@@ -108,11 +108,6 @@ int ss_set_bc(ss_handle *h, int64_t gdof, int64_t n_fix, const int64_t *fix,
               int64_t n_zheng, const int64_t *zheng, int64_t n_fu, const int64_t *fu,
               int64_t n_groups, const int64_t *group_ptr, const int64_t *group_dofs,
               int64_t two_stage);
-
-/* Drop-in input: an already assembled global matrix (what FrequencySolver
- * receives, sweep.py:283).  Complex interleaved values. */
-int ss_set_csr(ss_handle *h, int which, int64_t n, const int64_t *indptr,
-               const int64_t *indices, const double *vals);
 
 /* GPU assembly of K and M (and D when damping materials were set). */
 int ss_assemble(ss_handle *h);
@@ -202,7 +197,9 @@ int ss_adjoint_gradient(ss_handle *h, int n_f, const double *omega, double V, in
  *  mixed sweep re-solved in FP64 (option fp64_fallback), 30 / 31 Krylov steps of
  *  the primal / adjoint solves of the last sweep (sums over points), 32 points
  *  whose mixed refinement did not converge (before any FP64 re-solve), 33 device
- *  time of the FP64 re-solves (ms, included in 17).  Slots past 35 read 0.
+ *  time of the FP64 re-solves (ms, included in 17), 34 / 35 device time of the
+ *  element kernel / of the scatter into the CSR pattern of the last
+ *  ss_assemble (ms, CUDA events).  Slots past 35 read 0.
  */
 int ss_stats(const ss_handle *h, double *out, int n);
 
@@ -224,6 +221,19 @@ int ss_stats(const ss_handle *h, double *out, int n);
  * decision.  SS_EINVAL for an unknown name or a value out of range.
  */
 int ss_set_option(ss_handle *h, const char *name, double value);
+
+/*
+ * Roofline denominator of the Schur update (no counterpart in the reference):
+ * the median algorithmic rate in TFLOP/s (8 real flops per complex
+ * multiply-add) of one Schur-update kernel of this library on n_fronts dense
+ * synthetic fronts of m rows with k pivots (update block (m-k)^2, K = k), one
+ * launch covering all fronts, timed by CUDA events over `reps` launches after a
+ * warm-up.  kernel: 0 FP64 DMMA 64x64 tiles, 1 FP64 SIMT 128x64, 2 complex64
+ * tcgen05 one CTA per tile, 3 complex64 tcgen05 persistent, 4 complex64 SIMT
+ * FP32 128x64.  Allocates and frees its fronts (at most 64 GB).
+ */
+int ss_measure_gemm_ceiling(ss_handle *h, int kernel, int m, int k, int n_fronts, int reps,
+                            double *tflops);
 
 /*
  * Q9 assembly that allocates nothing (no counterpart in the reference).  It is

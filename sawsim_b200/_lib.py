@@ -37,7 +37,6 @@ SIGNATURES = [
     ('ss_set_pml', C.c_int, [_P, C.c_int, _I32P, _DP, _I32P, _DP, _DP, C.c_int, _I32P, C.c_double]),
     ('ss_set_bc', C.c_int, [_P, C.c_int64, C.c_int64, _I64P, C.c_int64, _I64P, C.c_int64, _I64P, C.c_int64,
                             _I64P, _I64P, C.c_int64]),
-    ('ss_set_csr', C.c_int, [_P, C.c_int, C.c_int64, _I64P, _I64P, _DP]),
     ('ss_assemble', C.c_int, [_P]),
     ('ss_export_csr', C.c_int, [_P, C.c_int, _I64P, _I64P, _I64P, _I64P, _DP]),
     ('ss_analyze', C.c_int, [_P]),
@@ -49,6 +48,7 @@ SIGNATURES = [
                                       _DP, _DP, _DP, _IP]),
     ('ss_stats', C.c_int, [_P, _DP, C.c_int]),
     ('ss_set_option', C.c_int, [_P, C.c_char_p, C.c_double]),
+    ('ss_measure_gemm_ceiling', C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _DP]),
     ('ss_assemble_q9_noalloc', C.c_int, [C.c_int, C.c_int64, _P, C.c_int64, _P, _P, _P, _P, _P, _P, C.c_int, _P, _P,
                                          _P, _P, _P, _P, C.c_double, _P, _P, _P, C.c_int64, _P, _P, _P]),
 ]

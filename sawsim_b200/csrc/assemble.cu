@@ -305,6 +305,14 @@ int launch_assemble(Handle &h, int which) {
   }
   SS_TRY(dalloc(dKel, (size_t)ne * nc * nc * npe2 * sizeof(cd)));
   SS_TRY(dalloc(dMel, (size_t)ne * npe2 * sizeof(cd)));
+  // the element and scatter kernels are timed by events (stats slots 34 and 35)
+  cudaEvent_t ev[3];
+  for (auto &x : ev) SS_TRY(cudaEventCreate(&x));
+  struct EvFree {
+    cudaEvent_t *e;
+    ~EvFree() { for (int i = 0; i < 3; ++i) cudaEventDestroy(e[i]); }
+  } ev_free{ev};
+  SS_TRY(cudaEventRecord(ev[0], h.stream));
   if (h.kind == SS_HEX27) {
     int rc = launch_hex27_elements(h, which, pml, dKel.as<cd>(), dMel.as<cd>(), dpos.as<double>(),
                                    dconn.as<int64_t>(), demat.as<int32_t>(), drho.as<double>(), dC.as<double>(),
@@ -316,6 +324,7 @@ int launch_assemble(Handle &h, int which) {
         de.as<double>(), deps.as<double>(), pml, dKel.as<cd>(), dMel.as<cd>());
     SS_TRY(cudaGetLastError());
   }
+  SS_TRY(cudaEventRecord(ev[1], h.stream));
   SS_TRY(dupload(dprow, prow));
   SS_TRY(dupload(dnadj, h.nadj_ptr));
   SS_TRY(dupload(dindptr, h.indptr));
@@ -332,11 +341,23 @@ int launch_assemble(Handle &h, int which) {
   }
   const int ndisp = h.kind == SS_Q9_ME0 ? 2 : 3;
   const int64_t nt = npairs * nc * nc;
+  cudaEvent_t g0;
+  SS_TRY(cudaEventCreate(&g0));
+  SS_TRY(cudaEventRecord(g0, h.stream));
   gather_pairs_kernel<<<(unsigned)((nt + 255) / 256), 256, 0, h.stream>>>(
       npairs, nc, npe2, h.kind == SS_HEX27, ndisp, N, dprow.as<int32_t>(), dnadj.as<int64_t>(),
       dindptr.as<int64_t>(), dgp.as<int64_t>(), dgs.as<int64_t>(), dKel.as<cd>(), dMel.as<cd>(), dst.as<cd>(), dM);
   SS_TRY(cudaGetLastError());
+  SS_TRY(cudaEventRecord(ev[2], h.stream));
   SS_TRY(cudaStreamSynchronize(h.stream));
+  if (!which) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev[0], ev[1]);
+    h.st[34] = ms;
+    cudaEventElapsedTime(&ms, g0, ev[2]);
+    h.st[35] = ms;
+  }
+  cudaEventDestroy(g0);
   if (which) h.have_D = true;
   else h.have_K = h.have_M = true;
   return SS_OK;

@@ -2356,7 +2356,12 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
       }
       const bool ok = !(sizeof(T) == 4 && !(conv[f] && aconv[f]));
       nfail += !ok;
-      if (status) status[c0 + f] = ok ? SS_OK : SS_ENOCONV;
+      // singular: a non-finite charge, or (FP64 direct solve) statically
+      // perturbed pivots whose refinement step still moves the solution by more
+      // than 1e-6 of its size
+      const bool finite = std::isfinite(Qout[2 * (int64_t)(c0 + f)]) && std::isfinite(Qout[2 * (int64_t)(c0 + f) + 1]);
+      const bool moved = !use_krylov && hp[f] > 0 && !(hn[2 * f] <= 1e-6 * hn[2 * f + 1]);
+      if (status) status[c0 + f] = (!finite || moved) ? SS_ESINGULAR : ok ? SS_OK : SS_ENOCONV;
       if (iters) iters[c0 + f] = hit[f];
     }
     if (disp) {
@@ -2530,6 +2535,117 @@ int run_sweep(Handle &h, int n_f, const double *omega, double V, int precision, 
     h.st[18] = tot;
   }
   return SS_OK;
+}
+
+}  // namespace ss
+
+namespace ss {
+
+// deterministic pseudo-random fill of a complex buffer (values in [-1, 1))
+template <class T>
+__global__ void fill_hash_kernel(int64_t n, cplx<T> *x) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint64_t z = (uint64_t)i * 0x9e3779b97f4a7c15ull + 0x632be59bd9b4e019ull;
+  z ^= z >> 29;
+  z *= 0xbf58476d1ce4e5b9ull;
+  z ^= z >> 32;
+  const T re = (T)((double)(z & 0xffffff) / 8388608.0 - 1.0);
+  const T im = (T)((double)((z >> 24) & 0xffffff) / 8388608.0 - 1.0);
+  x[i] = cplx<T>{re, im};
+}
+
+// Measured ceiling of one Schur-update kernel: n_fronts dense fronts of m rows
+// with k pivots (C -= A B over the (m-k) x (m-k) update block, K = k), every
+// front a separate "frequency" of one launch, timed by CUDA events over `reps`
+// launches after one warm-up; returns the median algorithmic rate (8 real flops
+// per complex multiply-add).  kernel: 0 FP64 DMMA 64x64, 1 FP64 SIMT 128x64,
+// 2 complex64 tcgen05 one CTA per tile, 3 complex64 tcgen05 persistent,
+// 4 complex64 SIMT FP32 128x64.
+template <class T>
+static int measure_ceiling_impl(Handle &h, int kernel, int m, int k, int nb, int reps, double *tflops) {
+  const int ld = (m + 3) / 4 * 4;
+  DBuf arena, dld, doff, dtasks, derr;
+  const size_t stride = (size_t)m * ld;
+  SS_CK(dalloc(arena, (size_t)nb * stride * sizeof(cplx<T>)));
+  std::vector<int> vld(1, ld);
+  std::vector<int64_t> voff(1, 0);
+  std::vector<GemmTask> tasks;
+  if (kernel == 0)
+    add_tiles(tasks, kSquare64, 0, k, m, k, m, 0, k);
+  else if (kernel == 2 || kernel == 3)
+    add_tiles(tasks, tc::BM, tc::BN, 0, k, m, k, m, 0, k);
+  else
+    add_tiles(tasks, kSquare, 0, k, m, k, m, 0, k);
+  SS_CK(dupload(dld, vld));
+  SS_CK(dupload(doff, voff));
+  SS_CK(dupload(dtasks, tasks));
+  SS_CK(dalloc(derr, sizeof(int)));
+  SS_CK(cudaMemsetAsync(derr.p, 0, sizeof(int), h.stream));
+  const int64_t ne = (int64_t)nb * stride;
+  fill_hash_kernel<T><<<(unsigned)((ne + 255) / 256), 256, 0, h.stream>>>(ne, arena.as<cplx<T>>());
+  FrontArgs<T> a{};
+  a.ld = dld.as<int>();
+  a.off = doff.as<int64_t>();
+  a.arena = arena.as<cplx<T>>();
+  a.stride = (int64_t)stride;
+  const GemmTask *tk = dtasks.as<GemmTask>();
+  const unsigned nt = (unsigned)tasks.size();
+  if (sizeof(T) == 4) {
+    SS_CK(cudaFuncSetAttribute(tc::front_tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
+    SS_CK(cudaFuncSetAttribute(tc::front_tc_gemm_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               tc::SMEM_BYTES));
+  }
+  auto launch = [&]() {
+    if constexpr (sizeof(T) == 8) {
+      if (kernel == 0)
+        front_dmma_kernel<2, 2><<<dim3(nt, nb), 128, 0, h.stream>>>(a, tk);
+      else
+        front_gemm_kernel<T, kSquare><<<dim3(nt, nb), 256, 0, h.stream>>>(a, tk);
+    } else {
+      cf *ar = reinterpret_cast<cf *>(a.arena);
+      if (kernel == 2)
+        tc::front_tc_gemm_kernel<<<dim3(nt, nb), tc::THREADS, tc::SMEM_BYTES, h.stream>>>(ar, a.stride, a.off, a.ld, tk,
+                                                                                         derr.as<int>());
+      else if (kernel == 3)
+        tc::front_tc_gemm_persistent<<<(unsigned)std::min<int64_t>((int64_t)nt * nb, h.num_sms), tc::P_THREADS,
+                                       tc::SMEM_BYTES, h.stream>>>(ar, a.stride, a.off, a.ld, tk, (int)nt, nb,
+                                                                   derr.as<int>());
+      else
+        front_gemm_kernel<T, kSquare><<<dim3(nt, nb), 256, 0, h.stream>>>(a, tk);
+    }
+  };
+  launch();
+  SS_CK(cudaGetLastError());
+  std::vector<cudaEvent_t> ev(2 * reps);
+  for (auto &e : ev) SS_CK(cudaEventCreate(&e));
+  for (int r = 0; r < reps; ++r) {
+    cudaEventRecord(ev[2 * r], h.stream);
+    launch();
+    cudaEventRecord(ev[2 * r + 1], h.stream);
+  }
+  SS_CK(cudaGetLastError());
+  SS_CK(cudaStreamSynchronize(h.stream));
+  std::vector<double> ms(reps);
+  for (int r = 0; r < reps; ++r) {
+    float t = 0;
+    cudaEventElapsedTime(&t, ev[2 * r], ev[2 * r + 1]);
+    ms[r] = t;
+  }
+  for (auto &e : ev) cudaEventDestroy(e);
+  int e = 0;
+  SS_CK(cudaMemcpy(&e, derr.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) return fail(h, SS_ETIMEOUT, "ceiling: a tensor-core tile timed out waiting for its MMAs");
+  std::sort(ms.begin(), ms.end());
+  const double med = ms[reps / 2];
+  const double flops = 8.0 * k * (double)(m - k) * (m - k) * nb;
+  *tflops = flops / (med * 1e-3) / 1e12;
+  return SS_OK;
+}
+
+int measure_ceiling(Handle &h, int kernel, int m, int k, int nb, int reps, double *tflops) {
+  if (kernel <= 1) return measure_ceiling_impl<double>(h, kernel, m, k, nb, reps, tflops);
+  return measure_ceiling_impl<float>(h, kernel, m, k, nb, reps, tflops);
 }
 
 }  // namespace ss

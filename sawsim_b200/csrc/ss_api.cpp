@@ -31,6 +31,12 @@ using namespace ss;
 
 static const char *kNoHandle = "null handle";
 
+static bool all_finite(const double *p, int64_t n) {
+  for (int64_t i = 0; i < n; ++i)
+    if (!std::isfinite(p[i])) return false;
+  return true;
+}
+
 extern "C" int ss_create(ss_handle **out, int device) {
   if (!out) return SS_EINVAL;
   *out = nullptr;
@@ -71,6 +77,7 @@ extern "C" int ss_set_mesh(ss_handle *hp, int kind, int64_t n_nodes, const doubl
   H_CHECK(hp);
   if (kind < SS_Q9_ME0 || kind > SS_HEX27) return fail(h, SS_EINVAL, "unknown element kind");
   if (n_nodes <= 0 || n_elem <= 0 || !pos || !conn || !emat) return fail(h, SS_EINVAL, "empty mesh or null array");
+  if (!all_finite(pos, n_nodes * (kind == SS_HEX27 ? 3 : 2))) return fail(h, SS_EINVAL, "non-finite coordinate");
   h.kind = kind;
   h.npe = kind == SS_HEX27 ? 27 : 9;
   h.dim = kind == SS_HEX27 ? 3 : 2;
@@ -95,6 +102,9 @@ extern "C" int ss_set_materials(ss_handle *hp, int which, int n_mat, const doubl
   H_CHECK(hp);
   if (which != SS_MAT_K && which != SS_MAT_D) return fail(h, SS_EINVAL, "materials: which must be K or D");
   if (n_mat <= 0 || !rho || !C || !e || !eps) return fail(h, SS_EINVAL, "materials: empty or null");
+  if (!all_finite(rho, n_mat) || !all_finite(C, n_mat * 72) || !all_finite(e, n_mat * 36) ||
+      !all_finite(eps, n_mat * 18))
+    return fail(h, SS_EINVAL, "materials: non-finite value");
   const int w = which == SS_MAT_D;
   h.nmat[w] = n_mat;
   h.rho[w].assign(rho, rho + n_mat);
@@ -108,9 +118,12 @@ extern "C" int ss_set_pml(ss_handle *hp, int n_regions, const int32_t *axis, con
                           const double *inner, const double *outer, int clip, const int32_t *elem_region,
                           double omega_top) {
   H_CHECK(hp);
-  if (omega_top <= 0) return fail(h, SS_EINVAL, "omega_top must be positive");
+  if (!(omega_top > 0) || !std::isfinite(omega_top)) return fail(h, SS_EINVAL, "omega_top must be positive and finite");
   if (n_regions < 0 || (n_regions > 0 && (!axis || !dmax || !npow || !inner || !outer || !elem_region)))
     return fail(h, SS_EINVAL, "pml: null array");
+  if (n_regions > 0 && (!all_finite(dmax, n_regions) || !all_finite(inner, 3 * n_regions) ||
+                        !all_finite(outer, 3 * n_regions)))
+    return fail(h, SS_EINVAL, "pml: non-finite value");
   h.omega_top = omega_top;
   h.npml = n_regions;
   h.pml_clip = clip;
@@ -244,13 +257,6 @@ extern "C" int ss_export_csr(ss_handle *hp, int which, int64_t *n_out, int64_t *
   return fail(h, SS_EINVAL, "export: unknown matrix");
 }
 
-extern "C" int ss_set_csr(ss_handle *hp, int which, int64_t n, const int64_t *indptr, const int64_t *indices,
-                          const double *vals) {
-  H_CHECK(hp);
-  (void)which; (void)n; (void)indptr; (void)indices; (void)vals;
-  return fail(h, SS_EINVAL, "ss_set_csr: assembled-matrix input needs a mesh-free ordering (not built)");
-}
-
 extern "C" int ss_analyze(ss_handle *hp) {
   H_CHECK(hp);
   if (!h.have_K || !h.have_M) return fail(h, SS_ESTATE, "analyze: assemble (or set) K and M first");
@@ -276,6 +282,7 @@ extern "C" int ss_analyze(ss_handle *hp) {
 
 extern "C" int ss_set_damping(ss_handle *hp, double beta) {
   H_CHECK(hp);
+  if (!std::isfinite(beta)) return fail(h, SS_EINVAL, "damping: beta must be finite");
   if (beta != 0.0 && !h.have_D) return fail(h, SS_ESTATE, "damping: assemble D first (damping materials)");
   if (beta < 0.0) return fail(h, SS_EINVAL, "damping: beta must be >= 0");
   h.beta = beta;
@@ -291,9 +298,9 @@ extern "C" int ss_sweep(ss_handle *hp, int n_f, const double *omega, double V, i
   if (n_f < 0 || (n_f > 0 && (!omega || !Q))) return fail(h, SS_EINVAL, "sweep: bad frequency arrays");
   if (precision != SS_PREC_FP64 && precision != SS_PREC_MIXED && precision != SS_PREC_AUTO)
     return fail(h, SS_EINVAL, "sweep: bad precision");
-  if (V == 0.0) return fail(h, SS_EINVAL, "sweep: V must be nonzero");
+  if (V == 0.0 || !std::isfinite(V)) return fail(h, SS_EINVAL, "sweep: V must be nonzero and finite");
   for (int i = 0; i < n_f; ++i)
-    if (!(omega[i] > 0.0)) return fail(h, SS_EINVAL, "sweep: omega must be positive");
+    if (!(omega[i] > 0.0) || !std::isfinite(omega[i])) return fail(h, SS_EINVAL, "sweep: omega must be positive and finite");
   if (n_f == 0) return SS_OK;
   return run_sweep(h, n_f, omega, V, precision, Q, status, iters, nullptr);
 }
@@ -391,4 +398,13 @@ extern "C" int ss_adjoint_gradient(ss_handle *hp, int n_f, const double *omega, 
     if (!(omega[i] > 0.0)) return fail(h, SS_EINVAL, "gradient: omega must be positive");
   return run_adjoint_gradient(h, n_f, omega, V, precision, n_params, dpos, dC, de, deps, drho, dinner, douter, Q,
                               dQ, status);
+}
+
+extern "C" int ss_measure_gemm_ceiling(ss_handle *hp, int kernel, int m, int k, int n_fronts, int reps,
+                                       double *tflops) {
+  H_CHECK(hp);
+  if (!tflops || kernel < 0 || kernel > 4 || k <= 0 || m <= k || n_fronts <= 0 || reps <= 0 || reps > 1000)
+    return fail(h, SS_EINVAL, "ceiling: bad arguments");
+  if ((double)n_fronts * m * m * 16.0 > 64e9) return fail(h, SS_EINVAL, "ceiling: more than 64 GB of fronts");
+  return measure_ceiling(h, kernel, m, k, n_fronts, reps, tflops);
 }

@@ -172,6 +172,8 @@ struct SweepExtra {
 };
 int run_sweep(Handle &h, int n_f, const double *omega, double V, int precision,
               double *Q, int *status, int *iters, double *disp_out, const SweepExtra *ex = nullptr);
+// Median algorithmic TFLOP/s of one Schur-update kernel on dense synthetic fronts
+int measure_ceiling(Handle &h, int kernel, int m, int k, int nb, int reps, double *tflops);
 // adjoint.cu: Q (n_f x 2) and dQ (n_f x n_params x 2) with the seeds of ss_adjoint_gradient
 int run_adjoint_gradient(Handle &h, int n_f, const double *omega, double V, int precision, int n_params,
                          const double *dpos, const double *dC, const double *de, const double *deps,

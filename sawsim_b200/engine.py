@@ -160,13 +160,21 @@ class FrequencySolver:
                  'sweep_device_ms', 'refine_solves', 'precision_used', 'schur_tile_simt128', 'schur_tile_simt64',
                  'schur_tile_dmma', 'panel_gemm_dmma', 'panel_tune_simt_ms', 'panel_tune_dmma_ms', 'small_fronts',
                  'schur_tune_ms', 'auto_probe_ms', 'fp64_resolved', 'krylov_steps_primal', 'krylov_steps_adjoint',
-                 'mixed_not_converged', 'fp64_resolve_ms']
+                 'mixed_not_converged', 'fp64_resolve_ms', 'element_kernel_ms', 'scatter_kernel_ms']
 
     def stats(self) -> dict:
         n = len(self.STAT_KEYS)
         out = np.zeros(n)
         self._h('ss_stats', L.ptr(out, C.c_double), n)
         return dict(zip(self.STAT_KEYS, out.tolist()))
+
+    def gemm_ceiling(self, kernel: int, m: int = 2560, k: int = 512, n_fronts: int = 8, reps: int = 5) -> float:
+        """Measured algorithmic TFLOP/s of a Schur-update kernel on dense fronts
+        (``ss_measure_gemm_ceiling``; kernel 0 FP64 DMMA, 1 FP64 SIMT, 2 / 3
+        complex64 tcgen05 per tile / persistent, 4 complex64 SIMT FP32)."""
+        out = C.c_double()
+        self._h('ss_measure_gemm_ceiling', int(kernel), int(m), int(k), int(n_fronts), int(reps), C.byref(out))
+        return out.value
 
     def set_option(self, name: str, value: float):
         """Solver option by name (``ss_set_option``): krylov_restart, krylov_cycles,
