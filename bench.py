@@ -204,8 +204,8 @@ def workload_name(c):
 def schur_kernel_name(s, used):
     """The Schur-update kernels the plan's autotuner picked, with their level counts."""
     if used == 'mixed':
-        names = ['tc::front_tc_gemm_kernel (tcgen05 3xTF32, one CTA per tile)',
-                 'tc::front_tc_gemm_persistent (tcgen05 3xTF32, warp-specialised)',
+        names = ['tc::pack_kernel + tc::tma_gemm_kernel<128,2> (TMA + tcgen05 3xTF32, 128x128 complex tiles)',
+                 'tc::pack_kernel + tc::tma_gemm_kernel<64,3> (TMA + tcgen05 3xTF32, 128x64 complex tiles)',
                  'front_gemm_kernel<float> (SIMT FP32 128x64)']
     else:
         names = ['front_gemm_kernel<double> SIMT 128x64', 'front_gemm_kernel<double> SIMT 64x64',
@@ -380,8 +380,8 @@ def b200_arm(a, rank, world, local):
     # untimed: both precision modes on this rank's points, and the measured ceilings
     modes = None if a.no_modes else mode_comparison(eng, f_all[mine], w, 2)
     ceilings = {'fp64_dmma': eng.gemm_ceiling(0)}
-    if used == 'mixed':
-        ceilings.update(c64_tcgen05=eng.gemm_ceiling(2), c64_tcgen05_persistent=eng.gemm_ceiling(3),
+    if used == 'mixed' or modes is not None:
+        ceilings.update(c64_tma_tcgen05_128=eng.gemm_ceiling(2), c64_tma_tcgen05_64=eng.gemm_ceiling(3),
                         c64_simt=eng.gemm_ceiling(4))
     pk, pk_kind = peaks()
     roof = rooflines(eng, c, s, st0, used, schur_ms, nf, pk, pk_kind, ceilings)

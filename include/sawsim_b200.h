@@ -42,7 +42,8 @@ typedef struct ss_handle ss_handle;
 
 /* precision modes for ss_sweep */
 #define SS_PREC_FP64   0   /* complex128 fronts, FP64 throughout (the drop-in)   */
-#define SS_PREC_MIXED  1   /* complex64 fronts, 3xTF32 tensor-core Schur updates,
+#define SS_PREC_MIXED  1   /* complex64 fronts, 3xTF32 tensor-core Schur updates
+                              (or SIMT FP32 where the autotuner finds it faster),
                               FP64 residual, FP64 flexible GMRES on the primal and
                               the adjoint, dual-weighted charge correction       */
 #define SS_PREC_AUTO   2   /* probe MIXED on the two band ends with 12 Krylov
@@ -109,7 +110,12 @@ int ss_set_bc(ss_handle *h, int64_t gdof, int64_t n_fix, const int64_t *fix,
               int64_t n_groups, const int64_t *group_ptr, const int64_t *group_dofs,
               int64_t two_stage);
 
-/* GPU assembly of K and M (and D when damping materials were set). */
+/* GPU assembly of K and M (and D when damping materials were set).  On an
+ * analysed handle whose mesh and boundary sets are unchanged (new materials,
+ * PML or freeze frequency only) the analysis, the factorisation plans and their
+ * autotuner picks are kept and only the condensed values are gathered again;
+ * the reference rebuilds its engine for every sweep (agent.py:406-477 runs 2-9
+ * of them per locate). */
 int ss_assemble(ss_handle *h);
 
 /*
@@ -188,7 +194,8 @@ int ss_adjoint_gradient(ss_handle *h, int n_f, const double *omega, double V, in
  *  19 precision the last ss_sweep ran in (SS_PREC_FP64 or SS_PREC_MIXED),
  *  20-22 levels whose Schur update uses the autotuner's candidate 0, 1, 2
  *  (FP64 sweep: SIMT 128x64, SIMT 64x64, FP64 tensor-core DMMA 64x64; mixed
- *  sweep: tcgen05 one CTA per tile, tcgen05 persistent, SIMT FP32 128x64),
+ *  sweep: packed operands + TMA + tcgen05 3xTF32 with 128 / 64 complex columns
+ *  per tile, SIMT FP32 128x64),
  *  23 1 if the panel-step GEMMs use DMMA tiles (128x32 / 32x128), else 0,
  *  24-25 autotuner time of all panel-step GEMMs with SIMT / DMMA tiles (ms),
  *  26 fronts factored whole in shared memory, 27 autotuner time of all
@@ -229,8 +236,9 @@ int ss_set_option(ss_handle *h, const char *name, double value);
  * synthetic fronts of m rows with k pivots (update block (m-k)^2, K = k), one
  * launch covering all fronts, timed by CUDA events over `reps` launches after a
  * warm-up.  kernel: 0 FP64 DMMA 64x64 tiles, 1 FP64 SIMT 128x64, 2 complex64
- * tcgen05 one CTA per tile, 3 complex64 tcgen05 persistent, 4 complex64 SIMT
- * FP32 128x64.  Allocates and frees its fronts (at most 64 GB).
+ * TMA + tcgen05 3xTF32 with 128-column tiles, 3 the same with 64-column tiles
+ * (operands packed once before the timed launches), 4 complex64 SIMT FP32
+ * 128x64.  Allocates and frees its fronts (at most 64 GB).
  */
 int ss_measure_gemm_ceiling(ss_handle *h, int kernel, int m, int k, int n_fronts, int reps,
                             double *tflops);

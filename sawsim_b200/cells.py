@@ -206,6 +206,20 @@ def sp_double_layer_cell() -> Q9Cell:
                    Band(TAG_ELECTRODE, 0.17, 1))
 
 
+def sp_quad_layer_cell() -> Q9Cell:
+    """The reference's ``sp_quad_layer`` template at its defaults, rebuilt without Gmsh.
+
+    Geometry of ``src/sawsim/sp_meshes/quad.py:26-160`` with pitch 1.085 um,
+    MR 0.5, Al 0.17 um (1 row), LT 0.6 um (3 rows, tag 16), SiO2 0.5 um (2 rows,
+    tag 22), poly-Si 1.0 um (4 rows, tag 23), Si 7.83 um (29 rows, tag 24), PML
+    2.17 um (8 rows, tag 25, the Si material), 8 columns of p/4: 372 elements,
+    1601 nodes.  Material order: 0 piezo, 1 Al, 2 SiO2, 3 poly-Si, 4 Si.
+    """
+    p = 1.085
+    return q9_cell(p, 8, [Band(TAG_PIEZO, 0.6, 3), Band(22, 0.5, 2), Band(23, 1.0, 4), Band(24, 7.83, 29),
+                          Band(25, 2.17, 8)], Band(TAG_ELECTRODE, 0.17, 1))
+
+
 def me0_cell(columns: int = 16, rows: int = 64, pitch_um: float = 1.085) -> Q9Cell:
     """Plane-strain single-crystal cell: 3p piezo substrate over a 1p PML.
 

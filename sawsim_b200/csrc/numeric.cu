@@ -1403,6 +1403,16 @@ struct Plan {
   std::vector<char> pick;                  // per level candidate
   std::vector<float> tune_ms;              // [candidate][level] measured times
   bool tuned = true;
+  // complex64 TMA Schur candidates: per level the packed fronts, the pack items
+  // (packed front, K chunk) and the output tiles of 128 and 64 complex columns
+  std::vector<int64_t> pk_ptr, pi_ptr, tt_ptr[2];
+  std::vector<tc::PackFront> pk;
+  std::vector<int2> pitems;
+  std::vector<tc::TmaTask> tt[2];
+  int64_t stage_rows = 0;                  // packed rows of the widest level, per frequency
+  bool tma_ok = false;                     // staging buffer and tensor map ready for this sweep
+  DBuf d_pk, d_pitems, d_tt[2];
+  CUtensorMap tmap{};                      // 2D map over the staging buffer (128-byte rows)
   ~Plan() {
     for (auto &g : graphs)
       if (g.exec) cudaGraphExecDestroy(g.exec);
@@ -1484,12 +1494,7 @@ Plan *build_plan(Handle &h, int small_m, bool tensor_schur) {
   for (int l = 0; l < S.nlevel; ++l) {
     for (int q = P->large_ptr[l]; q < P->large_ptr[l + 1]; ++q) {
       const int f = P->fronts_large[q], k = S.k[f], m = S.m[f];
-      if (m > k) {
-        if (tensor_schur)   // complex64 Schur updates on tcgen05 tiles
-          add_tiles(P->tasks, tc::BM, tc::BN, f, k, m, k, m, 0, k);
-        else
-          add_tiles(P->tasks, kSquare, f, k, m, k, m, 0, k);
-      }
+      if (m > k) add_tiles(P->tasks, kSquare, f, k, m, k, m, 0, k);
       P->schur_flops += 8.0 * k * (double)(m - k) * (m - k);
     }
     sp.push_back((int64_t)P->tasks.size());
@@ -1497,6 +1502,37 @@ Plan *build_plan(Handle &h, int small_m, bool tensor_schur) {
   P->schur_ptr = sp;
   P->pick.assign(S.nlevel, 0);
   P->tuned = false;
+  if (tensor_schur) {
+    // packed operands of every front with an update block, level by level (the
+    // staging buffer is reused per level), and the TMA kernels' tiles
+    P->pk_ptr.assign(1, 0);
+    P->pi_ptr.assign(1, 0);
+    P->tt_ptr[0].assign(1, 0);
+    P->tt_ptr[1].assign(1, 0);
+    for (int l = 0; l < S.nlevel; ++l) {
+      int64_t base = 0;
+      for (int q = P->large_ptr[l]; q < P->large_ptr[l + 1]; ++q) {
+        const int f = P->fronts_large[q], k = S.k[f], m = S.m[f], u = m - k;
+        if (u <= 0 || k <= 0) continue;
+        const int kc = (k + tc::KCH - 1) / tc::KCH, au = (u + tc::PADC - 1) / tc::PADC * tc::PADC;
+        const int pf = (int)P->pk.size();
+        P->pk.push_back(tc::PackFront{base, f, kc, au, au});
+        for (int c = 0; c < kc; ++c) P->pitems.push_back(make_int2(pf, c));
+        for (int v = 0; v < 2; ++v) {
+          const int bnc = v == 0 ? 128 : 64;
+          for (int r0 = k; r0 < m; r0 += tc::BM)
+            for (int c0 = k; c0 < m; c0 += bnc)
+              P->tt[v].push_back(tc::TmaTask{base, f, r0, c0, m, m, kc, au, au, r0 - k, 2 * (c0 - k)});
+        }
+        base += tc::pack_rows(kc, au, au);
+      }
+      P->stage_rows = std::max(P->stage_rows, base);
+      P->pk_ptr.push_back((int64_t)P->pk.size());
+      P->pi_ptr.push_back((int64_t)P->pitems.size());
+      P->tt_ptr[0].push_back((int64_t)P->tt[0].size());
+      P->tt_ptr[1].push_back((int64_t)P->tt[1].size());
+    }
+  }
   if (!tensor_schur) {
     std::vector<int64_t> sb(1, (int64_t)P->tasks.size());
     for (int l = 0; l < S.nlevel; ++l) {
@@ -1533,6 +1569,37 @@ Plan *build_plan(Handle &h, int small_m, bool tensor_schur) {
   return P;
 }
 
+// Condensed values from the global K, M (and D) through the fixed-order gather
+// lists: the condensed matrices (new order), ks | kq, ms (and ds), Qz.  Run after
+// the analysis and again after a value-only reassembly (same mesh and pattern).
+int gather_values(Handle &h) {
+  const int64_t n = h.sym.n;
+  const size_t cb = (size_t)h.c_nnz * sizeof(cd);
+  SS_CK(dalloc(h.dKc, cb));
+  SS_CK(dalloc(h.dMc, cb));
+  SS_CK(dalloc(h.dks, 2 * n * sizeof(cd)));   // ks | kq
+  SS_CK(dalloc(h.dms, n * sizeof(cd)));
+  SS_CK(dalloc(h.dQz, sizeof(cd)));
+  const unsigned gb = (unsigned)((h.c_nnz + 255) / 256), vb = (unsigned)((n + 255) / 256);
+  const int64_t *gp = h.dg_ptr.as<int64_t>(), *gs = h.dg_src.as<int64_t>();
+  const int64_t *vp = h.dv_ptr.as<int64_t>(), *vs = h.dv_src.as<int64_t>();
+  gather_sum_kernel<<<gb, 256, 0, h.stream>>>(h.c_nnz, gp, gs, h.dK.as<cd>(), h.dKc.as<cd>());
+  gather_sum_kernel<<<gb, 256, 0, h.stream>>>(h.c_nnz, gp, gs, h.dM.as<cd>(), h.dMc.as<cd>());
+  gather_sum_kernel<<<(unsigned)((2 * n + 255) / 256), 256, 0, h.stream>>>(2 * n, vp, vs, h.dK.as<cd>(), h.dks.as<cd>());
+  gather_sum_kernel<<<vb, 256, 0, h.stream>>>(n, vp, vs, h.dM.as<cd>(), h.dms.as<cd>());
+  gather_sum_kernel<<<1, 256, 0, h.stream>>>(1, h.dq_ptr.as<int64_t>(), h.dq_src.as<int64_t>(), h.dK.as<cd>(),
+                                             h.dQz.as<cd>());
+  if (h.have_D) {
+    SS_CK(dalloc(h.dDc, cb));
+    SS_CK(dalloc(h.dds, n * sizeof(cd)));
+    gather_sum_kernel<<<gb, 256, 0, h.stream>>>(h.c_nnz, gp, gs, h.dD.as<cd>(), h.dDc.as<cd>());
+    gather_sum_kernel<<<vb, 256, 0, h.stream>>>(n, vp, vs, h.dD.as<cd>(), h.dds.as<cd>());
+  }
+  SS_CK(cudaGetLastError());
+  SS_CK(cudaStreamSynchronize(h.stream));
+  return SS_OK;
+}
+
 int launch_condense(Handle &h) {
   Symbolic &S = h.sym;
   const int64_t n = S.n;
@@ -1552,35 +1619,18 @@ int launch_condense(Handle &h) {
       vp[w * n + R + 1] = (int64_t)vs.size();
     }
   std::vector<int64_t> qp = {0, (int64_t)h.qz_src.size()};
-  DBuf dvp, dvs, dqp, dqs;
   SS_CK(dupload(h.dc_ptr, h.c_ptr));
   SS_CK(dupload(h.dc_idx, h.c_idx));
   SS_CK(dupload(h.dg_ptr, gp));
   SS_CK(dupload(h.dg_src, gs));
-  SS_CK(dupload(dvp, vp));
-  SS_CK(dupload(dvs, vs));
-  SS_CK(dupload(dqp, qp));
-  SS_CK(dupload(dqs, h.qz_src));
-  const size_t cb = (size_t)h.c_nnz * sizeof(cd);
-  SS_CK(dalloc(h.dKc, cb));
-  SS_CK(dalloc(h.dMc, cb));
-  SS_CK(dalloc(h.dks, 2 * n * sizeof(cd)));   // ks | kq
-  SS_CK(dalloc(h.dms, n * sizeof(cd)));
-  SS_CK(dalloc(h.dQz, sizeof(cd)));
-  const unsigned gb = (unsigned)((h.c_nnz + 255) / 256), vb = (unsigned)((n + 255) / 256);
-  gather_sum_kernel<<<gb, 256, 0, h.stream>>>(h.c_nnz, h.dg_ptr.as<int64_t>(), h.dg_src.as<int64_t>(), h.dK.as<cd>(), h.dKc.as<cd>());
-  gather_sum_kernel<<<gb, 256, 0, h.stream>>>(h.c_nnz, h.dg_ptr.as<int64_t>(), h.dg_src.as<int64_t>(), h.dM.as<cd>(), h.dMc.as<cd>());
-  gather_sum_kernel<<<(unsigned)((2 * n + 255) / 256), 256, 0, h.stream>>>(2 * n, dvp.as<int64_t>(), dvs.as<int64_t>(), h.dK.as<cd>(), h.dks.as<cd>());
-  gather_sum_kernel<<<vb, 256, 0, h.stream>>>(n, dvp.as<int64_t>(), dvs.as<int64_t>(), h.dM.as<cd>(), h.dms.as<cd>());
-  gather_sum_kernel<<<1, 256, 0, h.stream>>>(1, dqp.as<int64_t>(), dqs.as<int64_t>(), h.dK.as<cd>(), h.dQz.as<cd>());
-  if (h.have_D) {
-    SS_CK(dalloc(h.dDc, cb));
-    SS_CK(dalloc(h.dds, n * sizeof(cd)));
-    gather_sum_kernel<<<gb, 256, 0, h.stream>>>(h.c_nnz, h.dg_ptr.as<int64_t>(), h.dg_src.as<int64_t>(), h.dD.as<cd>(), h.dDc.as<cd>());
-    gather_sum_kernel<<<vb, 256, 0, h.stream>>>(n, dvp.as<int64_t>(), dvs.as<int64_t>(), h.dD.as<cd>(), h.dds.as<cd>());
+  SS_CK(dupload(h.dv_ptr, vp));
+  SS_CK(dupload(h.dv_src, vs));
+  SS_CK(dupload(h.dq_ptr, qp));
+  SS_CK(dupload(h.dq_src, h.qz_src));
+  {
+    const int rc = gather_values(h);
+    if (rc) return rc;
   }
-  SS_CK(cudaGetLastError());
-  SS_CK(cudaStreamSynchronize(h.stream));
   // symbolic arrays
   SS_CK(dupload(h.d_k, S.k));
   SS_CK(dupload(h.d_m, S.m));
@@ -1626,6 +1676,34 @@ static int small_limit() {
   int v = sizeof(T) == 8 ? 96 : 128;
   if (const char *e = getenv("SS_SMALL_FRONT_M")) v = atoi(e);
   return std::max(0, std::min(cap, v));
+}
+
+// 2D tensor map over a staging buffer of `rows` rows of 32 fp32 (128 bytes):
+// boxes of 32 x 128 with the 128-byte swizzle the MMA operand descriptors use.
+// The encoder is the driver's cuTensorMapEncodeTiled, reached through the
+// runtime's entry-point query (no link against the driver library).
+static int encode_stage_map(Handle &h, CUtensorMap &map, void *base, int64_t rows) {
+  using Encode = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                              const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static Encode fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !p)
+      return fail(h, SS_ECUDA, "tensor map: cuTensorMapEncodeTiled not available");
+    fn = reinterpret_cast<Encode>(p);
+  }
+  const cuuint64_t dim[2] = {32, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)tc::ROWB};
+  const cuuint32_t box[2] = {32, 128};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = fn(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dim, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(h, SS_ECUDA, "tensor map: cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  return SS_OK;
 }
 
 // equilibration at angular frequency w (Ruiz, 3 sweeps)
@@ -1813,22 +1891,29 @@ struct Sweeper {
   void schur_launch(const FrontArgs<T> &b, int l, int c, int nb) {
     const GemmTask *tasks = P.d_tasks.template as<GemmTask>();
     if constexpr (sizeof(T) == 4) {
-      // complex64: candidate 0 tcgen05 one CTA per tile, 1 tcgen05 persistent
-      // warp-specialised CTAs, 2 SIMT FP32 tiles of the same 128x64 shape
+      // complex64: candidates 0 / 1 pack the level's operands and run the TMA +
+      // tcgen05 kernel with 128 / 64 complex columns per tile; 2 SIMT FP32 128x64
       const int64_t t0 = P.schur_ptr[l], t1 = P.schur_ptr[l + 1];
-      if (c == 2) {
+      if (c == 2 || !P.tma_ok) {
         front_gemm_kernel<T, kSquare><<<dim3((unsigned)(t1 - t0), nb), 256, 0, h.stream>>>(b, tasks + t0);
         return;
       }
-      if (c == 0) {
-        tc::front_tc_gemm_kernel<<<dim3((unsigned)(t1 - t0), nb), tc::THREADS, tc::SMEM_BYTES, h.stream>>>(
-            reinterpret_cast<cf *>(b.arena), b.stride, b.off, b.ld, tasks + t0, tc_err);
-      } else {
-        const int64_t items = (t1 - t0) * nb;
-        const unsigned grid = (unsigned)std::min<int64_t>(items, h.num_sms);
-        tc::front_tc_gemm_persistent<<<grid, tc::P_THREADS, tc::SMEM_BYTES, h.stream>>>(
-            reinterpret_cast<cf *>(b.arena), b.stride, b.off, b.ld, tasks + t0, (int)(t1 - t0), nb, tc_err);
-      }
+      const int v = c;   // tile variant
+      const int64_t i0 = P.pi_ptr[l], i1 = P.pi_ptr[l + 1], q0 = P.tt_ptr[v][l], q1 = P.tt_ptr[v][l + 1];
+      if (i1 == i0 || q1 == q0) return;
+      cf *ar = reinterpret_cast<cf *>(b.arena);
+      tc::pack_kernel<<<dim3((unsigned)(i1 - i0), nb), tc::PACK_THREADS, 0, h.stream>>>(
+          ar, b.stride, b.off, b.ld, b.k, b.m, P.d_pk.template as<tc::PackFront>(), P.d_pitems.template as<int2>() + i0,
+          h.tc_stage.template as<float>(), P.stage_rows);
+      const int64_t items = (q1 - q0) * nb;
+      const unsigned grid = (unsigned)std::min<int64_t>(items, h.num_sms);
+      const tc::TmaTask *tt = P.d_tt[v].template as<tc::TmaTask>() + q0;
+      if (v == 0)
+        tc::tma_gemm_kernel<128, 2><<<grid, 192, tc::TmaCfg<128, 2>::SMEM, h.stream>>>(
+            P.tmap, ar, b.stride, b.off, b.ld, tt, (int)(q1 - q0), nb, P.stage_rows, tc_err);
+      else
+        tc::tma_gemm_kernel<64, 3><<<grid, 192, tc::TmaCfg<64, 3>::SMEM, h.stream>>>(
+            P.tmap, ar, b.stride, b.off, b.ld, tt, (int)(q1 - q0), nb, P.stage_rows, tc_err);
       return;
     }
     if (c == 0) {
@@ -2105,10 +2190,16 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
                                small_limit<T>() * small_limit<T>() * (int)sizeof(cplx<T>)));
     SS_CK(cudaFuncSetAttribute(front_panel_smem_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                kPanelSmemMax));
-    SS_CK(cudaFuncSetAttribute(tc::front_tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               tc::SMEM_BYTES));
-    SS_CK(cudaFuncSetAttribute(tc::front_tc_gemm_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               tc::SMEM_BYTES));
+    SS_CK(cudaFuncSetAttribute(tc::tma_gemm_kernel<128, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               tc::TmaCfg<128, 2>::SMEM));
+    SS_CK(cudaFuncSetAttribute(tc::tma_gemm_kernel<64, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               tc::TmaCfg<64, 3>::SMEM));
+    if (sizeof(T) == 4) {
+      SS_CK(dupload(P->d_pk, P->pk));
+      SS_CK(dupload(P->d_pitems, P->pitems));
+      SS_CK(dupload(P->d_tt[0], P->tt[0]));
+      SS_CK(dupload(P->d_tt[1], P->tt[1]));
+    }
     // solve kernels stage a whole front vector in shared memory
     // (the four triangular kernels also hold one staged 32x32 diagonal block)
     const int vec = (int)std::min<int64_t>(227 * 1024, (int64_t)S.max_m * (int64_t)sizeof(cplx<T>));
@@ -2143,11 +2234,13 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
   const bool correct = sizeof(T) == 4;
   const bool need_adjoint = correct || (ex && ex->per_chunk);
   const double per = (double)S.arena * sizeof(cplx<T>) + n * 4.0 + W * (double)sizeof(cplx<T>) + n * 64.0 + krylov +
-                     (need_adjoint ? 32.0 * n : 0.0) + 32.0 * n + 256;
+                     (need_adjoint ? 32.0 * n : 0.0) + 32.0 * n + 256 +
+                     (sizeof(T) == 4 ? (double)P.stage_rows * tc::ROWB : 0.0);
   // the Krylov workspace persists in the handle; a sweep without Krylov steps
   // gives its memory back to the fronts
   KrylovWork &kw = h.kw;
   if (!(sizeof(T) == 4 || getenv("SS_FP64_KRYLOV") != nullptr)) kw.release();
+  if (sizeof(T) == 8) h.tc_stage.release();   // packed tensor-core operands: mixed sweeps only
   size_t fr = 0, tot = 0;
   SS_CK(cudaMemGetInfo(&fr, &tot));
   fr += kw.bytes();
@@ -2156,10 +2249,24 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
        &dom = h.wk[7], &npert = h.wk[8], &nrm = h.wk[9], &dQ = h.wk[10], &mu = h.wk[11], &cvec = h.wk[12];
   // the chunk size counts only memory not already held by these buffers
   for (int i = 0; i < 16; ++i) fr += h.wk[i].bytes;
+  fr += h.tc_stage.bytes;
   int B = (int)std::max(1.0, std::min((double)n_f, std::min(256.0, (0.85 * (double)fr - 512e6) / per)));
   // a buffer that must grow is released first so that old and new never coexist
   if ((size_t)B * S.arena * sizeof(cplx<T>) > arena.bytes) arena.release();
   SS_CK(dalloc(arena, (size_t)B * S.arena * sizeof(cplx<T>)));
+  if (sizeof(T) == 4) {
+    // staging buffer of the packed Schur operands (one level at a time) and the
+    // 2D tensor map over it: rows of 32 fp32, boxes of 128 rows, 128-byte swizzle
+    P.tma_ok = false;
+    const int64_t rows = (int64_t)B * P.stage_rows;
+    if (P.stage_rows > 0 && rows < ((int64_t)1 << 31)) {
+      if ((size_t)rows * tc::ROWB > h.tc_stage.bytes) h.tc_stage.release();
+      SS_CK(dalloc(h.tc_stage, (size_t)rows * tc::ROWB));
+      const int rc = encode_stage_map(h, P.tmap, h.tc_stage.p, rows);
+      if (rc) return rc;
+      P.tma_ok = true;
+    }
+  }
   SS_CK(dalloc(piv, (size_t)B * n * sizeof(int)));
   SS_CK(dalloc(wv, (size_t)B * std::max<int64_t>(W, 1) * sizeof(cplx<T>)));
   SS_CK(dalloc(b, (size_t)B * n * sizeof(cd)));
@@ -2560,7 +2667,8 @@ __global__ void fill_hash_kernel(int64_t n, cplx<T> *x) {
 // front a separate "frequency" of one launch, timed by CUDA events over `reps`
 // launches after one warm-up; returns the median algorithmic rate (8 real flops
 // per complex multiply-add).  kernel: 0 FP64 DMMA 64x64, 1 FP64 SIMT 128x64,
-// 2 complex64 tcgen05 one CTA per tile, 3 complex64 tcgen05 persistent,
+// 2 / 3 complex64 TMA + tcgen05 3xTF32 with 128 / 64-column tiles (operands
+// packed once before the timed launches),
 // 4 complex64 SIMT FP32 128x64.
 template <class T>
 static int measure_ceiling_impl(Handle &h, int kernel, int m, int k, int nb, int reps, double *tflops) {
@@ -2573,10 +2681,32 @@ static int measure_ceiling_impl(Handle &h, int kernel, int m, int k, int nb, int
   std::vector<GemmTask> tasks;
   if (kernel == 0)
     add_tiles(tasks, kSquare64, 0, k, m, k, m, 0, k);
-  else if (kernel == 2 || kernel == 3)
-    add_tiles(tasks, tc::BM, tc::BN, 0, k, m, k, m, 0, k);
   else
     add_tiles(tasks, kSquare, 0, k, m, k, m, 0, k);
+  // TMA kernels: the front's packed operands and the tiles of 128 / 64 columns
+  const int kc = (k + tc::KCH - 1) / tc::KCH, u = m - k, au = (u + tc::PADC - 1) / tc::PADC * tc::PADC;
+  const int bnc = kernel == 2 ? 128 : 64;
+  std::vector<tc::PackFront> pk(1, tc::PackFront{0, 0, kc, au, au});
+  std::vector<int2> pitems;
+  for (int c = 0; c < kc; ++c) pitems.push_back(make_int2(0, c));
+  std::vector<tc::TmaTask> tt;
+  for (int r0 = k; r0 < m; r0 += tc::BM)
+    for (int c0 = k; c0 < m; c0 += bnc) tt.push_back(tc::TmaTask{0, 0, r0, c0, m, m, kc, au, au, r0 - k, 2 * (c0 - k)});
+  const int64_t srows = tc::pack_rows(kc, au, au);
+  DBuf dpk, dpi, dtt, dk, dm, dstage;
+  CUtensorMap map{};
+  const bool tma = kernel == 2 || kernel == 3;
+  if (tma) {
+    if ((int64_t)nb * srows >= ((int64_t)1 << 31)) return fail(h, SS_EINVAL, "ceiling: staging rows exceed 2^31");
+    SS_CK(dupload(dpk, pk));
+    SS_CK(dupload(dpi, pitems));
+    SS_CK(dupload(dtt, tt));
+    SS_CK(dupload(dk, std::vector<int>(1, k)));
+    SS_CK(dupload(dm, std::vector<int>(1, m)));
+    SS_CK(dalloc(dstage, (size_t)nb * srows * tc::ROWB));
+    const int rc = encode_stage_map(h, map, dstage.p, (int64_t)nb * srows);
+    if (rc) return rc;
+  }
   SS_CK(dupload(dld, vld));
   SS_CK(dupload(doff, voff));
   SS_CK(dupload(dtasks, tasks));
@@ -2591,10 +2721,15 @@ static int measure_ceiling_impl(Handle &h, int kernel, int m, int k, int nb, int
   a.stride = (int64_t)stride;
   const GemmTask *tk = dtasks.as<GemmTask>();
   const unsigned nt = (unsigned)tasks.size();
-  if (sizeof(T) == 4) {
-    SS_CK(cudaFuncSetAttribute(tc::front_tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
-    SS_CK(cudaFuncSetAttribute(tc::front_tc_gemm_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               tc::SMEM_BYTES));
+  if (tma) {
+    SS_CK(cudaFuncSetAttribute(tc::tma_gemm_kernel<128, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               tc::TmaCfg<128, 2>::SMEM));
+    SS_CK(cudaFuncSetAttribute(tc::tma_gemm_kernel<64, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               tc::TmaCfg<64, 3>::SMEM));
+    // operands packed once; the timed launches are the GEMM alone
+    tc::pack_kernel<<<dim3((unsigned)pitems.size(), nb), tc::PACK_THREADS, 0, h.stream>>>(
+        reinterpret_cast<const cf *>(a.arena), a.stride, a.off, a.ld, dk.as<int>(), dm.as<int>(),
+        dpk.as<tc::PackFront>(), dpi.as<int2>(), dstage.as<float>(), srows);
   }
   auto launch = [&]() {
     if constexpr (sizeof(T) == 8) {
@@ -2604,13 +2739,13 @@ static int measure_ceiling_impl(Handle &h, int kernel, int m, int k, int nb, int
         front_gemm_kernel<T, kSquare><<<dim3(nt, nb), 256, 0, h.stream>>>(a, tk);
     } else {
       cf *ar = reinterpret_cast<cf *>(a.arena);
+      const unsigned grid = (unsigned)std::min<int64_t>((int64_t)tt.size() * nb, h.num_sms);
       if (kernel == 2)
-        tc::front_tc_gemm_kernel<<<dim3(nt, nb), tc::THREADS, tc::SMEM_BYTES, h.stream>>>(ar, a.stride, a.off, a.ld, tk,
-                                                                                         derr.as<int>());
+        tc::tma_gemm_kernel<128, 2><<<grid, 192, tc::TmaCfg<128, 2>::SMEM, h.stream>>>(
+            map, ar, a.stride, a.off, a.ld, dtt.as<tc::TmaTask>(), (int)tt.size(), nb, srows, derr.as<int>());
       else if (kernel == 3)
-        tc::front_tc_gemm_persistent<<<(unsigned)std::min<int64_t>((int64_t)nt * nb, h.num_sms), tc::P_THREADS,
-                                       tc::SMEM_BYTES, h.stream>>>(ar, a.stride, a.off, a.ld, tk, (int)nt, nb,
-                                                                   derr.as<int>());
+        tc::tma_gemm_kernel<64, 3><<<grid, 192, tc::TmaCfg<64, 3>::SMEM, h.stream>>>(
+            map, ar, a.stride, a.off, a.ld, dtt.as<tc::TmaTask>(), (int)tt.size(), nb, srows, derr.as<int>());
       else
         front_gemm_kernel<T, kSquare><<<dim3(nt, nb), 256, 0, h.stream>>>(a, tk);
     }

@@ -179,15 +179,31 @@ extern "C" int ss_assemble(ss_handle *hp) {
   if (mx >= h.nmat[0]) return fail(h, SS_EINVAL, "element material index >= number of materials");
   if (h.omega_top <= 0 && h.npml > 0) return fail(h, SS_ESTATE, "assemble: set the PML first");
   auto t0 = std::chrono::steady_clock::now();
+  // a reassembly of an analysed system with the same mesh and boundary sets (new
+  // materials, PML or freeze frequency) keeps the analysis, the factorisation
+  // plans, their autotuner picks and launch graphs: only the values change
+  const bool keep = h.analyzed;
+  const bool had_D = h.have_D;
+  if (h.nmat[1] > 0 && mx >= h.nmat[1]) return fail(h, SS_EINVAL, "damping materials fewer than element materials");
   int rc = launch_assemble(h, 0);
   if (rc) return rc;
   if (h.nmat[1] > 0) {
-    if (mx >= h.nmat[1]) return fail(h, SS_EINVAL, "damping materials fewer than element materials");
     rc = launch_assemble(h, 1);
     if (rc) return rc;
   }
   h.st[6] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-  reset_derived(h);
+  if (keep) {
+    if (h.have_D != had_D) free_plans(h);   // the launch graphs bake the damping matrix in
+    rc = gather_values(h);
+    if (rc) {
+      reset_derived(h);
+      return rc;
+    }
+    h.scale_w = -1;      // equilibrate again at the next sweep
+    h.auto_prec = -1;    // a kept SS_PREC_AUTO decision was for the old values
+  } else {
+    reset_derived(h);
+  }
   return SS_OK;
 }
 

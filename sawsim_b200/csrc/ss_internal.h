@@ -120,7 +120,8 @@ struct Handle {
   DBuf dc_ptr, dc_idx, dKc, dMc, dDc;    // device condensed CSR
   DBuf dg_ptr, dg_src;                   // gather lists: condensed slot <- global slots
   DBuf dks, dms, dds, dkq;               // rhs/charge vectors (new order)
-  DBuf dv_ptr, dv_src;                   // gather lists for the 4 vectors
+  DBuf dv_ptr, dv_src;                   // gather lists of ks | kq (and ms, ds)
+  DBuf dq_ptr, dq_src;                   // gather list of Qz
   std::vector<int64_t> v_ptr;            // host copy (sizes)
   double Qz_dummy = 0;
   DBuf dQz;                              // complex: sum over zheng rows/cols of K
@@ -143,6 +144,7 @@ struct Handle {
   double auto_w0 = 0, auto_w1 = 0;
   int auto_prec = -1;
   DBuf dKs, dMs, dDs;                    // equilibrated condensed values
+  DBuf tc_stage;                         // packed tensor-core Schur operands (mixed sweeps)
   double scale_w = -1;                   // frequency the scaling was computed at
   // solver options (ss_set_option); kept until changed
   struct Options {
@@ -164,6 +166,7 @@ struct Handle {
 int launch_assemble(Handle &h, int which);  // which 0: K+M, 1: D
 // numeric.cu
 int launch_condense(Handle &h);
+int gather_values(Handle &h);   // condensed values again after a value-only reassembly
 // Optional work of a sweep beyond the charges: per_chunk(c0, nb, x, mu) is called
 // for every chunk of frequencies with the scaled primal solutions x' and adjoint
 // solutions mu' (A'^T mu' = cs * kq) of that chunk on the device (nb x n each).

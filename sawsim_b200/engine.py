@@ -115,6 +115,8 @@ class FrequencySolver:
           L.ptr(inner, C.c_double), L.ptr(outer, C.c_double), 1, L.ptr(region, C.c_int32), float(omega_top))
         h('ss_assemble')
         eng = cls(h, (ndisp + 1) * pos.shape[0], ndisp, kind, bc[1], bc[2])
+        eng._pml = (nreg, axis, dmax, npow, inner, outer, 1, region)
+        eng.omega_top = float(omega_top)
         eng._set_bc(bc, two_stage=0)
         if damping_materials is not None and beta:
             h('ss_set_damping', float(beta))
@@ -143,6 +145,8 @@ class FrequencySolver:
         h('ss_assemble')
         fix, zheng, fu, groups, two_stage = bc
         eng = cls(h, 4 * pos.shape[0], 3, L.SS_HEX27, zheng, fu)
+        eng._pml = (nreg, axis, dmax, npow, inner, outer, 0, region)
+        eng.omega_top = float(omega_top)
         eng._set_bc((fix, zheng, fu, groups), two_stage=two_stage)
         return eng
 
@@ -152,6 +156,20 @@ class FrequencySolver:
                 fu.size, L.ptr(fu, C.c_int64), gptr.size - 1, L.ptr(gptr, C.c_int64), L.ptr(gd, C.c_int64),
                 int(two_stage))
         self._h('ss_analyze')
+
+    def set_freeze_frequency(self, omega_top: float):
+        """Reassemble K and M with the PML stretch frozen at ``omega_top`` (the
+        reference assembles at each sweep's top frequency, solver.py:106-107).
+        The mesh and the boundary sets are unchanged, so the analysis, the
+        factorisation plans and their autotuner picks are kept."""
+        if float(omega_top) == self.omega_top:
+            return
+        nreg, axis, dmax, npow, inner, outer, clip, region = self._pml
+        self._h('ss_set_pml', nreg, L.ptr(axis, C.c_int32), L.ptr(dmax, C.c_double), L.ptr(npow, C.c_int32),
+                L.ptr(inner, C.c_double), L.ptr(outer, C.c_double), clip, L.ptr(region, C.c_int32),
+                float(omega_top))
+        self._h('ss_assemble')
+        self.omega_top = float(omega_top)
 
     # ------------------------------------------------------------------ queries
     STAT_KEYS = ['n_active', 'n_fronts', 'max_front', 'factor_flops_per_point', 'nnz_lu', 'analyze_s',
@@ -171,7 +189,8 @@ class FrequencySolver:
     def gemm_ceiling(self, kernel: int, m: int = 2560, k: int = 512, n_fronts: int = 8, reps: int = 5) -> float:
         """Measured algorithmic TFLOP/s of a Schur-update kernel on dense fronts
         (``ss_measure_gemm_ceiling``; kernel 0 FP64 DMMA, 1 FP64 SIMT, 2 / 3
-        complex64 tcgen05 per tile / persistent, 4 complex64 SIMT FP32)."""
+        complex64 TMA + tcgen05 3xTF32 with 128 / 64-column tiles, 4 complex64
+        SIMT FP32)."""
         out = C.c_double()
         self._h('ss_measure_gemm_ceiling', int(kernel), int(m), int(k), int(n_fronts), int(reps), C.byref(out))
         return out.value

@@ -9,9 +9,10 @@ It imports the reference's own modules (``sawsim.saw2d.piezo_fem``,
 ``sawsim.saw2d.sweep``, the material library) and records, for meshes built by
 ``sawsim_b200.cells`` without Gmsh:
 
-* ``sp_double_layer.npz`` — the template's published curve at its 5 test
-  frequencies (``tests/data/sp_double_layer.npz['sawsim_magnitude']``), the
-  resolved material tensors of the template, and the reference's own |Y| there;
+* ``sp_double_layer.npz``, ``sp_quad_layer.npz`` — each template's published
+  curve at its 5 test frequencies (``tests/data/<name>.npz['sawsim_magnitude']``),
+  the resolved material tensors of the template, and the reference's own |Y|
+  there on the rebuilt mesh;
 * ``ref_<case>.npz`` — for small seeded synthetic cells (ME0 and ME1): a hash of
   the reference's global K pattern, K @ v and M @ v for a seeded v, the condensed
   Km_aa @ w, Mm_aa @ w, the active DOF list and the reference's Q at a few
@@ -55,18 +56,19 @@ def pattern_hash(A) -> str:
     return h.hexdigest()
 
 
-def double_layer():
-    meta = json.loads((REF / 'tests/data/sp_double_layer.json').read_text())
-    d = np.load(REF / 'tests/data/sp_double_layer.npz')
+def template(name, cell):
+    """A structured template's published curve at its test frequencies, its
+    resolved materials and the reference's own run on the rebuilt mesh."""
+    meta = json.loads((REF / f'tests/data/{name}.json').read_text())
+    d = np.load(REF / f'tests/data/{name}.npz')
     idx = np.array(meta['test_indices'])
     cfg = meta['config']
     sub = from_record(get_record(cfg['substrate_material']))
     el = from_record(get_record(cfg['electrode_material']))
-    lay = from_record(get_record(cfg['layers'][0]['material_id']))
+    lays = [from_record(get_record(layer['material_id'])) for layer in cfg['layers']]
     C, e, eps = oula_transfer([cfg['euler_phi_deg'], cfg['euler_theta_deg'], cfg['euler_psi_deg']],
                               sub.C, sub.e, sub.eps)
-    mats = [Material(sub.rho, C, e, eps), el, lay]
-    cell = cells.sp_double_layer_cell()
+    mats = [Material(sub.rho, C, e, eps), el] + lays
     model = piezo_fem.build_model(type('M', (), cell.msh())())
     tag_map = cell.tag_map
     mi = piezo_fem.material_index(model, tag_map)
@@ -78,13 +80,13 @@ def double_layer():
     eng = sweep.FrequencySolver(K, M, *sweep.bc_periodic(model, cell.LINES3, ndisp=3))
     Q = np.array([eng.solve(2 * np.pi * x, 1.0)[1] for x in fre])
     Y = -1j * 2 * np.pi * fre * Q
-    np.savez_compressed(HERE / 'sp_double_layer.npz', frequency_hz=fre, published_magnitude=d['sawsim_magnitude'][idx],
+    np.savez_compressed(HERE / f'{name}.npz', frequency_hz=fre, published_magnitude=d['sawsim_magnitude'][idx],
                         reference_fem_magnitude=d['reference_magnitude'][idx], reference_run_admittance=Y,
                         rho=np.array([m.rho for m in mats]), C=np.stack([m.C for m in mats]),
                         e=np.stack([m.e for m in mats]), eps=np.stack([m.eps for m in mats]),
                         pitch_um=cfg['pitch_um'])
     err = np.max(np.abs(np.abs(Y) - d['sawsim_magnitude'][idx]) / d['sawsim_magnitude'][idx])
-    print('sp_double_layer: reference run vs published curve', err)
+    print(name, ': reference run vs published curve', err)
 
 
 def small(name, cols, rows, nf):
@@ -110,6 +112,7 @@ def small(name, cols, rows, nf):
 
 
 if __name__ == '__main__':
-    double_layer()
+    template('sp_double_layer', cells.sp_double_layer_cell())
+    template('sp_quad_layer', cells.sp_quad_layer_cell())
     for args in SMALL:
         small(*args)

@@ -29,8 +29,8 @@ def test_fp64_kernel_name_lists_the_picked_tiles(bench):
 def test_mixed_kernel_name_lists_the_picked_tiles(bench):
     s = dict(schur_tile_simt128=5.0, schur_tile_simt64=1.0, schur_tile_dmma=7.0)
     name = bench.schur_kernel_name(s, 'mixed')
-    assert 'tc::front_tc_gemm_kernel' in name and 'on 5 levels' in name
-    assert 'tc::front_tc_gemm_persistent' in name and 'on 1 levels' in name
+    assert 'tc::tma_gemm_kernel<128,2>' in name and 'on 5 levels' in name
+    assert 'tc::tma_gemm_kernel<64,3>' in name and 'on 1 levels' in name
     assert 'SIMT FP32 128x64) on 7 levels' in name
 
 

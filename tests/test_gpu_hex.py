@@ -89,4 +89,5 @@ def test_hex_mixed_matches_fp64(hexpair):
     Q64, _, _ = g.charges(w, 1.0, 'fp64')
     Q32, st, _ = g.charges(w, 1.0, 'mixed')
     assert (st == 0).all(), st
+    assert g.stats()['fp64_resolved'] == 0
     assert np.max(np.abs(Q32 - Q64) / np.abs(Q64)) < 1e-6

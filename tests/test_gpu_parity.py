@@ -103,13 +103,14 @@ def test_adjoint_solves_transposed_system(pair, precision, tol):
     assert np.max(np.abs(lam - ref)) <= tol * np.max(np.abs(ref))
 
 
-def test_double_layer_published_curve(built_lib):
-    """The rebuilt sp_double_layer template reproduces the reference's published
-    curve at its 5 test frequencies on the GPU FP64 path."""
-    gl = np.load(GOLDEN / 'sp_double_layer.npz')
-    cell = cells.sp_double_layer_cell()
+@pytest.mark.parametrize('name', ['sp_double_layer', 'sp_quad_layer'])
+def test_template_published_curve(built_lib, name):
+    """The rebuilt sp_double_layer and sp_quad_layer templates reproduce the
+    reference's published curves at their 5 test frequencies on the GPU FP64 path."""
+    gl = np.load(GOLDEN / f'{name}.npz')
+    cell = {'sp_double_layer': cells.sp_double_layer_cell, 'sp_quad_layer': cells.sp_quad_layer_cell}[name]()
     mesh = cases.mesh_from_msh(cell.msh())
-    mats = [Material(gl['rho'][i], gl['C'][i], gl['e'][i], gl['eps'][i]) for i in range(3)]
+    mats = [Material(gl['rho'][i], gl['C'][i], gl['e'][i], gl['eps'][i]) for i in range(len(gl['rho']))]
     idx = np.array([cell.tag_map[t] for t in mesh.elem_tag])
     bottom = mesh.pos_m[:, 1].min()
     pml = [cases.PML(tag=cell.pml_tag, kind='y', yp=bottom, ya=bottom + 2 * float(gl['pitch_um']) * 1e-6)]

@@ -60,6 +60,7 @@ def test_mixed_matches_fp64(mid):
     Q64, st64, _ = g.charges(2 * np.pi * f, 1.0, 'fp64')
     Q32, st32, it = g.charges(2 * np.pi * f, 1.0, 'mixed')
     assert (st64 == 0).all() and (st32 == 0).all(), st32
+    assert g.stats()['fp64_resolved'] == 0
     assert np.max(np.abs(Q32 - Q64) / np.abs(Q64)) < 1e-6
     Y64, Y32 = -1j * 2 * np.pi * f * Q64, -1j * 2 * np.pi * f * Q32
     d = compare(resonances(f, Y64), resonances(f, Y32))
@@ -91,8 +92,9 @@ def test_every_schur_tile_candidate_is_exact(mid, tile, monkeypatch):
 
 @pytest.mark.parametrize('tile', [0, 1, 2])
 def test_every_complex64_schur_candidate_converges(mid, tile, monkeypatch):
-    """Every complex64 Schur kernel (tcgen05 one CTA per tile; tcgen05 persistent
-    warp-specialised CTAs with double-buffered TMEM accumulators; SIMT FP32 tiles),
+    """Every complex64 Schur kernel (packed operands loaded by TMA into persistent
+    warp-specialised tcgen05 CTAs with double-buffered TMEM accumulators, 128- and
+    64-column tiles; SIMT FP32 tiles),
     each forced on every level, gives a mixed sweep within 1e-6 of FP64."""
     case, _, g = mid
     f = np.linspace(case.freqs[0], case.freqs[-1], 5)
@@ -101,9 +103,12 @@ def test_every_complex64_schur_candidate_converges(mid, tile, monkeypatch):
     e = cases.engine_for(case)
     try:
         Q, st, _ = e.charges(2 * np.pi * f, 1.0, 'mixed')
+        s = e.stats()
     finally:
         e.close()
-    assert (st == 0).all()
+    assert (st == 0).all() and s['fp64_resolved'] == 0      # converged in mixed precision
+    counts = [s['schur_tile_simt128'], s['schur_tile_simt64'], s['schur_tile_dmma']]
+    assert counts[tile] > 0 and sum(counts) == counts[tile]
     assert np.max(np.abs(Q - Q64) / np.abs(Q64)) < 1e-6
 
 

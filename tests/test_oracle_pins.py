@@ -1,7 +1,8 @@
 """The oracle is pinned before it is trusted (CPU only).
 
-* against the reference's published sp_double_layer curve (tests/data of the
-  reference, copied into tests/golden/sp_double_layer.npz with its materials);
+* against the reference's published sp_double_layer and sp_quad_layer curves
+  (tests/data of the reference, copied into tests/golden/<name>.npz with their
+  materials);
 * against the reference's own matrices and charges on small seeded cells
   (tests/golden/ref_me*.npz, produced by tests/golden/make_golden.py).
 """
@@ -26,11 +27,11 @@ def _hash(A):
     return h.hexdigest()
 
 
-def double_layer_oracle():
-    g = np.load(GOLDEN / 'sp_double_layer.npz')
-    cell = cells.sp_double_layer_cell()
+def template_oracle(name='sp_double_layer'):
+    g = np.load(GOLDEN / f'{name}.npz')
+    cell = {'sp_double_layer': cells.sp_double_layer_cell, 'sp_quad_layer': cells.sp_quad_layer_cell}[name]()
     m = oq9.build_model(cell.msh())
-    mats = [Material(g['rho'][i], g['C'][i], g['e'][i], g['eps'][i]) for i in range(3)]
+    mats = [Material(g['rho'][i], g['C'][i], g['e'][i], g['eps'][i]) for i in range(len(g['rho']))]
     idx = oq9.material_index(m, cell.tag_map)
     bottom = m.pos_m[:, 1].min()
     pml = [oq9.PMLRegion(tag=cell.pml_tag, kind='y', yp=bottom, ya=bottom + 2 * float(g['pitch_um']) * 1e-6)]
@@ -40,8 +41,11 @@ def double_layer_oracle():
     return g, eng
 
 
-def test_double_layer_published_curve():
-    g, eng = double_layer_oracle()
+@pytest.mark.parametrize('name', ['sp_double_layer', 'sp_quad_layer'])
+def test_template_published_curve(name):
+    """Structured templates rebuilt without Gmsh: the oracle reproduces the
+    reference's published curve at its test frequencies."""
+    g, eng = template_oracle(name)
     f = g['frequency_hz']
     Y = osol.admittance_2d(f, eng.sweep(f))
     pub = g['published_magnitude']
@@ -52,7 +56,7 @@ def test_double_layer_published_curve():
 
 
 def test_double_layer_realblock_route():
-    g, eng = double_layer_oracle()
+    g, eng = template_oracle()
     f = g['frequency_hz'][:2]
     Qc = eng.sweep(f, route='complex')
     Qr = eng.sweep(f, route='realblock')
