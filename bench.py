@@ -38,6 +38,7 @@ CPU_SAMPLE = {'me0_16x64': [dict(cols=8, rows=32), dict(cols=16, rows=64)],
               'me1_128x512': [dict(cols=16, rows=64), dict(cols=32, rows=128)],
               'hex_8x4x48': [dict(nx=8, ny=1, nz=12), dict(nx=8, ny=2, nz=24)]}
 SCHUR_DRAM_BYTES_PER_POINT = {'me1_64x256': 6.16e9}
+FULL_POINT_LIMIT_S = 900.0     # the measured full-size CPU point gives up after this
 METRIC = 'Y11 points/s, 1 B200: batched FP32-TC+refine vs FP64 sweep, fr/fa within 1 kHz'
 
 
@@ -52,6 +53,8 @@ def parse():
     p.add_argument('--points', type=int, default=None)
     p.add_argument('--no-cpu-baseline', action='store_true')
     p.add_argument('--no-modes', action='store_true', help='skip the untimed FP64-vs-mixed comparison')
+    p.add_argument('--no-full-point', action='store_true',
+                   help='reference arm: skip the one measured full-size CPU point')
     return p.parse_args()
 
 
@@ -161,23 +164,75 @@ def _cpu_init():
     sys.path.insert(0, str(REPO / 'oracle'))
 
 
+def _full_point(case_name, out):
+    """One frequency point of the reference route at the full size (spawned
+    process, one BLAS thread): build seconds, solve seconds, peak RSS."""
+    os.environ['OMP_NUM_THREADS'] = '1'
+    _cpu_init()
+    import resource
+    from helpers_cpu import oracle_solver_for
+    t = time.perf_counter()
+    eng = oracle_solver_for(case_name)
+    build = time.perf_counter() - t
+    c = make(case_name)
+    f = c.freqs[len(c.freqs) // 2]
+    t = time.perf_counter()
+    if case_name.startswith('hex'):
+        eng.solve(2 * np.pi * f, 1.0)
+    else:
+        eng.solve(2 * np.pi * f, 1.0, route='realblock')
+    out.put(dict(solve_s=time.perf_counter() - t, build_s=build, f_ghz=f / 1e9, n_active=int(eng.n_active),
+                 peak_rss_gb=resource.getrusage(resource.RUSAGE_SELF).ru_maxrss / 1e6))
+
+
+def full_point_start(case_name):
+    import multiprocessing as mp
+    ctx = mp.get_context('spawn')
+    q = ctx.Queue()
+    p = ctx.Process(target=_full_point, args=(case_name, q), daemon=True)
+    p.start()
+    return p, q, time.perf_counter()
+
+
+def full_point_finish(handle, limit_s):
+    """The measured full-size point, waiting at most until `limit_s` after its start."""
+    import queue
+    p, q, t0 = handle
+    try:
+        res = q.get(timeout=max(1.0, limit_s - (time.perf_counter() - t0)))
+    except queue.Empty:
+        res = dict(unfinished_after_s=round(time.perf_counter() - t0, 1))
+    if p.is_alive():
+        p.terminate()
+    p.join(5)
+    return res
+
+
 def reference_arm(a, rank, world):
     """Reference CPU implementation (oracle port) on this host, rank 0 only."""
     if rank != 0:
         return
     workers = min(8, os.cpu_count() or 1)
+    # one full-size point of the same route, measured once on a core beside the
+    # sampling workers (it takes minutes: it overlaps the sampled steps)
+    full = full_point_start(a.case) if not a.no_full_point else None
     res = []
     for i in range(a.warmup + a.steps):
         v, sample = cpu_sweep_sample(a.case, 2 * workers, workers)
         if i >= a.warmup:
             res.append(v)
     value = float(np.mean(res))
+    measured = full_point_finish(full, FULL_POINT_LIMIT_S) if full else None
+    if measured and 'solve_s' in measured:
+        measured['extrapolated_point_s'] = workers / value
+        measured['extrapolated_over_measured'] = (workers / value) / measured['solve_s']
     print(json.dumps(dict(impl='reference', metric=METRIC, value=value, unit='points/s', n_gpus=a.gpus,
                           steps=a.steps, warmup=a.warmup, higher_is_better=True, scaling='weak', vs_baseline=None,
                           dtype='f64', data='synthetic',
                           config=dict(workload=workload_name(make(a.case, a.points)),
                                       route='oracle port of the reference route, bounded sample, extrapolated'),
-                          cpu_baseline=dict(value=value, unit='points/s', cores=workers, kind='port', sample=sample),
+                          cpu_baseline=dict(value=value, unit='points/s', cores=workers, kind='port', sample=sample,
+                                            measured_full_point=measured),
                           e2e=dict(value=value, unit='points/s', h2d_bytes_per_step=0, d2h_bytes_per_step=0))),
           flush=True)
 

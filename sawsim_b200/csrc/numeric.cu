@@ -1909,10 +1909,10 @@ struct Sweeper {
       const unsigned grid = (unsigned)std::min<int64_t>(items, h.num_sms);
       const tc::TmaTask *tt = P.d_tt[v].template as<tc::TmaTask>() + q0;
       if (v == 0)
-        tc::tma_gemm_kernel<128, 2><<<grid, 192, tc::TmaCfg<128, 2>::SMEM, h.stream>>>(
+        tc::tma_gemm_kernel<128, 2><<<grid, tc::TmaCfg<128, 2>::THREADS, tc::TmaCfg<128, 2>::SMEM, h.stream>>>(
             P.tmap, ar, b.stride, b.off, b.ld, tt, (int)(q1 - q0), nb, P.stage_rows, tc_err);
       else
-        tc::tma_gemm_kernel<64, 3><<<grid, 192, tc::TmaCfg<64, 3>::SMEM, h.stream>>>(
+        tc::tma_gemm_kernel<64, 3><<<grid, tc::TmaCfg<64, 3>::THREADS, tc::TmaCfg<64, 3>::SMEM, h.stream>>>(
             P.tmap, ar, b.stride, b.off, b.ld, tt, (int)(q1 - q0), nb, P.stage_rows, tc_err);
       return;
     }
@@ -2741,10 +2741,10 @@ static int measure_ceiling_impl(Handle &h, int kernel, int m, int k, int nb, int
       cf *ar = reinterpret_cast<cf *>(a.arena);
       const unsigned grid = (unsigned)std::min<int64_t>((int64_t)tt.size() * nb, h.num_sms);
       if (kernel == 2)
-        tc::tma_gemm_kernel<128, 2><<<grid, 192, tc::TmaCfg<128, 2>::SMEM, h.stream>>>(
+        tc::tma_gemm_kernel<128, 2><<<grid, tc::TmaCfg<128, 2>::THREADS, tc::TmaCfg<128, 2>::SMEM, h.stream>>>(
             map, ar, a.stride, a.off, a.ld, dtt.as<tc::TmaTask>(), (int)tt.size(), nb, srows, derr.as<int>());
       else if (kernel == 3)
-        tc::tma_gemm_kernel<64, 3><<<grid, 192, tc::TmaCfg<64, 3>::SMEM, h.stream>>>(
+        tc::tma_gemm_kernel<64, 3><<<grid, tc::TmaCfg<64, 3>::THREADS, tc::TmaCfg<64, 3>::SMEM, h.stream>>>(
             map, ar, a.stride, a.off, a.ld, dtt.as<tc::TmaTask>(), (int)tt.size(), nb, srows, derr.as<int>());
       else
         front_gemm_kernel<T, kSquare><<<dim3(nt, nb), 256, 0, h.stream>>>(a, tk);

@@ -26,9 +26,11 @@
 //    streams the packed tiles with TMA into a ring of shared-memory stages (the
 //    tensor map's 128-byte swizzle is the layout the MMA descriptors expect),
 //    warp 1 issues 12 MMAs per K chunk into one of two TMEM accumulators, warps
-//    2-5 drain the other accumulator into C (TMEM -> registers -> a padded
-//    per-warp shared tile -> coalesced read-modify-write rows of C), so one
-//    tile's epilogue overlaps the next tile's loads and MMAs.
+//    2-9 drain the other accumulator into C (two warps per TMEM lane quarter,
+//    each half of the columns: TMEM -> registers -> a padded per-warp shared
+//    tile -> coalesced read-modify-write rows of C with all 32 rows of a column
+//    block loaded before any is stored), so one tile's epilogue overlaps the
+//    next tile's loads and MMAs.
 // Every mbarrier wait is bounded (kWaitNs); on time-out the CTA records the
 // error, every role leaves its loop, the producer waits (bounded) for the
 // copies it issued, the MMA warp waits on one final commit that tracks all of
@@ -257,17 +259,18 @@ struct TmaCfg {
   static constexpr int A_BYTES = BM * ROWB;               // one A operand (hi or lo) of a chunk
   static constexpr int B_BYTES = NR * ROWB;               // one B' operand of a chunk
   static constexpr int STAGE = 2 * A_BYTES + 2 * B_BYTES; // A hi, A lo, B' hi, B' lo
+  static constexpr int EPI_WARPS = 8;                     // two per TMEM lane quarter
   static constexpr int EPI_FLOATS = 32 * 33;              // per epilogue warp: 32 rows x 33 fp32
-  static constexpr int SMEM = STG * STAGE + 4 * EPI_FLOATS * 4 + 1024;   // + alignment slack
+  static constexpr int SMEM = STG * STAGE + EPI_WARPS * EPI_FLOATS * 4;
   static constexpr int TMEM_COLS = 2 * NR;                // two accumulators
-  static constexpr int THREADS = 192;                     // producer, MMA, 4 epilogue warps
+  static constexpr int THREADS = 64 + 32 * EPI_WARPS;     // producer, MMA, epilogue warps
   static constexpr uint32_t IDESC = idesc_tf32(NR);
   static_assert(NR % 128 == 0 && NR <= 256, "B' loads are 128-row boxes; N <= 256");
   static_assert(SMEM <= 227 * 1024, "shared memory");
 };
 
 template <int BNC, int STG>
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(TmaCfg<BNC, STG>::THREADS, 1)
     tma_gemm_kernel(const __grid_constant__ CUtensorMap tmap, cf *__restrict__ arena, int64_t stride,
                     const int64_t *__restrict__ off, const int *__restrict__ ldv, const TmaTask *__restrict__ tasks,
                     int ntasks, int nb, int64_t stage_rows, int *__restrict__ err) {
@@ -277,20 +280,25 @@ __global__ void __launch_bounds__(192, 1)
   __shared__ __align__(8) uint64_t full[STG], empty[STG], acc_full[2], acc_empty[2], drain;
   __shared__ uint32_t tmem_base_s;
   __shared__ volatile int abort_s;
-  unsigned char *smem = reinterpret_cast<unsigned char *>(
-      (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  // the 128-byte-swizzled stages need 1024-byte alignment, which the declaration
+  // gives; a base that lacked it would be reported, not used
+  unsigned char *smem = tc_smem_raw;
   float *epi = reinterpret_cast<float *>(smem + STG * Cfg::STAGE);
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t n_items = (int64_t)ntasks * nb;
   if (threadIdx.x == 0) {
     abort_s = *reinterpret_cast<volatile int *>(err);
+    if (smem_u32(smem) & 1023u) {
+      abort_s = 1;
+      atomicExch(err, 1);
+    }
     for (int s = 0; s < STG; ++s) {
       mbar_init(smem_u32(&full[s]), 1);
       mbar_init(smem_u32(&empty[s]), 1);
     }
     for (int a = 0; a < 2; ++a) {
       mbar_init(smem_u32(&acc_full[a]), 1);
-      mbar_init(smem_u32(&acc_empty[a]), 128);
+      mbar_init(smem_u32(&acc_empty[a]), 32 * Cfg::EPI_WARPS);
     }
     mbar_init(smem_u32(&drain), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -395,8 +403,9 @@ __global__ void __launch_bounds__(192, 1)
     }
     __syncwarp();
   } else {
-    // ---------------- epilogue warps 2-5: TMEM lane quarter q = warp % 4
-    const int q = wid & 3;
+    // ---------------- epilogue warps 2-9: TMEM lane quarter q = warp % 4, column
+    // blocks of 32 fp32 with parity h = (warp - 2) / 4
+    const int q = wid & 3, h = (wid - 2) >> 2;
     float *stg = epi + (wid - 2) * Cfg::EPI_FLOATS;
     int64_t ac = 0;
     for (int64_t it = blockIdx.x; it < n_items; it += gridDim.x) {
@@ -413,22 +422,26 @@ __global__ void __launch_bounds__(192, 1)
       }
       tc_fence_after();
       const int rbase = tk.r0 + 32 * q;
+      const int nrow = min(32, tk.rhi - rbase);                // rows of this quarter inside the tile
 #pragma unroll 1
-      for (int blk = 0; blk < NR / 32; ++blk) {
+      for (int blk = h; blk < NR / 32; blk += 2) {
         float v[32];
         tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(a * NR + 32 * blk), v);
 #pragma unroll
         for (int i = 0; i < 32; ++i) stg[lane * 33 + i] = v[i];
         __syncwarp();
-        // row rr of this warp's 32: 32 consecutive fp32 = 16 complex columns
+        // rows of the block: 32 consecutive fp32 (16 complex columns) each; every
+        // row's load is issued before any store
         const int c = tk.c0 + 16 * blk + (lane >> 1);
-        for (int rr = 0; rr < 32; ++rr) {
-          const int r = rbase + rr;
-          if (r >= tk.rhi) break;
-          if (c < tk.chi) {
-            float *p = F + 2 * ((int64_t)r * ld + tk.c0 + 16 * blk) + lane;
-            *p -= stg[rr * 33 + lane];
-          }
+        if (nrow > 0 && c < tk.chi) {
+          float *p0 = F + 2 * ((int64_t)rbase * ld + tk.c0 + 16 * blk) + lane;
+          const int64_t rs = 2 * (int64_t)ld;
+          float cur[32];
+#pragma unroll
+          for (int rr = 0; rr < 32; ++rr) cur[rr] = rr < nrow ? p0[rr * rs] : 0.f;
+#pragma unroll
+          for (int rr = 0; rr < 32; ++rr)
+            if (rr < nrow) p0[rr * rs] = cur[rr] - stg[rr * 33 + lane];
         }
         __syncwarp();
       }
