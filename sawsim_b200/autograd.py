@@ -33,15 +33,32 @@ def y11_and_jacobian(model, params, freqs, precision='fp64', V=1.0, device=0):
     return Y, dY, st
 
 
+def y11_only(model, params, freqs, precision='fp64', V=1.0, device=0):
+    """(Y[n_f], status) at parameters ``params``: the sweep alone, no adjoint."""
+    p = np.asarray(params, dtype=float)
+    case = model.build(p)
+    eng = model.engine(case, device=device)
+    try:
+        w = 2 * np.pi * np.asarray(freqs, dtype=float)
+        Q, st, _ = eng.charges(w, V, precision)
+    finally:
+        eng.close()
+    return model.y11(w, Q, V, case), st
+
+
 class Y11Sweep(torch.autograd.Function):
     """Forward: Y11 at every frequency; backward: the adjoint Jacobian product."""
 
     @staticmethod
     def forward(ctx, params, model, freqs, precision):
-        Y, dY, st = y11_and_jacobian(model, params.detach().cpu().numpy(), freqs, precision)
+        p = params.detach().cpu().numpy()
+        if ctx.needs_input_grad[0]:
+            Y, dY, st = y11_and_jacobian(model, p, freqs, precision)
+        else:               # no backward can follow: the sweep alone
+            (Y, st), dY = y11_only(model, p, freqs, precision), None
         if (st != 0).any():
             raise RuntimeError(f'sweep did not converge at {int((st != 0).sum())} points')
-        ctx.save_for_backward(torch.from_numpy(dY))
+        ctx.save_for_backward(torch.from_numpy(dY) if dY is not None else torch.empty(0))
         ctx.param_dtype = params.dtype
         return torch.from_numpy(Y)
 

@@ -80,6 +80,22 @@ def bc_periodic(mesh: Mesh, lines, ndisp: int = 3, tag_bottom=21, tag_left=19, t
     return fix, zheng + ndisp * N, fu + ndisp * N, groups
 
 
+def bc_floating(mesh: Mesh, lines, ndisp: int = 3, tag_bottom=7, tag_xfl=3, tag_xfr=4, tag_zheng=5, tag_fu=6):
+    """Finite-device boundary sets with floating electrodes (sweep.py:75-91): the
+    bottom u fixed, the + and - electrode phi prescribed, and the phi DOFs of each
+    floating electrode merged into one equipotential group (its first node the
+    master)."""
+    N = mesh.N
+    bottom = mesh.nodes_with_tag(tag_bottom, lines)
+    xfl = mesh.nodes_with_tag(tag_xfl, lines)
+    xfr = mesh.nodes_with_tag(tag_xfr, lines)
+    zheng = mesh.nodes_with_tag(tag_zheng, lines)
+    fu = mesh.nodes_with_tag(tag_fu, lines)
+    fix = np.concatenate([bottom + a * N for a in range(ndisp)])
+    groups = [xfl + ndisp * N, xfr + ndisp * N]
+    return fix, zheng + ndisp * N, fu + ndisp * N, groups
+
+
 @dataclass
 class Case:
     name: str
