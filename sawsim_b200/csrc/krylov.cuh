@@ -26,11 +26,17 @@ struct MatOp {
 __global__ void spmv_kernel(int64_t n, int nb, const int64_t *__restrict__ rp, const int64_t *__restrict__ ci,
                             const int64_t *__restrict__ vp, const cd *__restrict__ K, const cd *__restrict__ M,
                             const cd *__restrict__ D, const double *__restrict__ omega, double beta,
-                            const cd *__restrict__ x, cd *__restrict__ y) {
+                            const cd *__restrict__ x, cd *__restrict__ y, const int *__restrict__ active = nullptr) {
   const int64_t R = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int f0 = blockIdx.y * kSpmvFreqs;
   if (R >= n || f0 >= nb) return;
-  const int nf = min(kSpmvFreqs, nb - f0);
+  // frequencies [f0, f0 + nf) of this block; trailing ones that stopped iterating
+  // are left out (a block whose frequencies have all stopped returns)
+  int nf = min(kSpmvFreqs, nb - f0);
+  if (active) {
+    while (nf > 0 && !active[f0 + nf - 1]) --nf;
+    if (nf == 0) return;
+  }
   double w2[kSpmvFreqs], wb[kSpmvFreqs];
   cd acc[kSpmvFreqs];
 #pragma unroll
@@ -73,9 +79,10 @@ __device__ inline cd block_reduce_cd(cd v, cd *red) {
 
 // h[f * ldh + i] = V_i,f^H w_f for i < J;  grid (J, nb), 256 threads
 __global__ void multi_dot_kernel(int64_t n, int nb, const cd *__restrict__ V, const cd *__restrict__ w,
-                                 cd *__restrict__ h, int ldh) {
+                                 cd *__restrict__ h, int ldh, const int *__restrict__ active = nullptr) {
   __shared__ cd red[256];
   const int i = blockIdx.x, f = blockIdx.y;
+  if (active && !active[f]) return;
   const cd *v = V + ((int64_t)i * nb + f) * n;
   const cd *x = w + (int64_t)f * n;
   cd acc{0.0, 0.0};
@@ -90,19 +97,21 @@ __global__ void multi_dot_kernel(int64_t n, int nb, const cd *__restrict__ V, co
 
 // w_f -= sum_{i<J} h[f*ldh+i] V_i,f
 __global__ void multi_axpy_kernel(int64_t n, int nb, int J, const cd *__restrict__ V, const cd *__restrict__ h,
-                                  int ldh, cd *__restrict__ w) {
+                                  int ldh, cd *__restrict__ w, const int *__restrict__ active = nullptr) {
   const int64_t R = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int f = blockIdx.y;
-  if (R >= n) return;
+  if (R >= n || (active && !active[f])) return;
   cd acc = w[(int64_t)f * n + R];
   for (int i = 0; i < J; ++i) acc = acc - cmul(h[f * ldh + i], V[((int64_t)i * nb + f) * n + R]);
   w[(int64_t)f * n + R] = acc;
 }
 
 // out[f] = ||w_f||_2
-__global__ void norm2_kernel(int64_t n, const cd *__restrict__ w, double *__restrict__ out) {
+__global__ void norm2_kernel(int64_t n, const cd *__restrict__ w, double *__restrict__ out,
+                             const int *__restrict__ active = nullptr) {
   __shared__ cd red[256];
   const int f = blockIdx.x;
+  if (active && !active[f]) return;
   const cd *x = w + (int64_t)f * n;
   double acc = 0.0;
   for (int64_t R = threadIdx.x; R < n; R += blockDim.x) acc += cabs2(x[R]);
@@ -112,10 +121,11 @@ __global__ void norm2_kernel(int64_t n, const cd *__restrict__ w, double *__rest
 
 // out_f = w_f * s[f]
 // out may be w (in-place scaling): each element is read and written by one thread
-__global__ void scale_vec_kernel(int64_t n, int nb, const cd *w, const double *__restrict__ s, cd *out) {
+__global__ void scale_vec_kernel(int64_t n, int nb, const cd *w, const double *__restrict__ s, cd *out,
+                                 const int *__restrict__ active = nullptr) {
   const int64_t R = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int f = blockIdx.y;
-  if (R >= n) return;
+  if (R >= n || (active && !active[f])) return;
   out[(int64_t)f * n + R] = w[(int64_t)f * n + R] * s[f];
 }
 
@@ -134,10 +144,14 @@ __global__ void combine_kernel(int64_t n, int nb, const int *__restrict__ kf, co
 // FGMRES(m) with up to `restarts` cycles; x holds the initial guess on entry.
 // precond(src, dst) applies M^-1 to nb vectors.  Returns the number of
 // preconditioner applications per frequency in `its`, converged flags in `conv`.
+// d_active (nb ints on the device, may be null) marks the frequencies still
+// iterating: the preconditioner's solve kernels, the sparse products and the
+// orthogonalisation skip the others, so a chunk's cost follows each point's own
+// step count rather than its slowest point's; all ones again on return.
 template <class Precond>
 int fgmres(Handle &h, KrylovWork &kw, const MatOp &op, int nb, int m, int restarts, double tol, const cd *Kc, const cd *Mc,
            const cd *Dc, const double *d_omega, const cd *b, cd *x, Precond precond, std::vector<int> &its,
-           std::vector<char> &conv) {
+           std::vector<char> &conv, int *d_active = nullptr) {
   const int64_t n = h.sym.n;
   const unsigned vb = (unsigned)((n + 255) / 256);
   const size_t vec = (size_t)nb * n * sizeof(cd);
@@ -167,6 +181,19 @@ int fgmres(Handle &h, KrylovWork &kw, const MatOp &op, int nb, int m, int restar
   std::vector<cd> hcol((size_t)nb * ldh * 2);
   std::vector<int> kf(nb);
   std::vector<char> done(nb);
+  std::vector<int> act(nb, 1);
+  // mirror of d_active: upload when a point stops
+  auto push_active = [&]() -> cudaError_t {
+    if (!d_active) return cudaSuccess;
+    for (int f = 0; f < nb; ++f) act[f] = done[f] ? 0 : 1;
+    return cudaMemcpyAsync(d_active, act.data(), nb * sizeof(int), cudaMemcpyHostToDevice, h.stream);
+  };
+  auto all_active = [&]() -> cudaError_t {
+    if (!d_active) return cudaSuccess;
+    std::fill(act.begin(), act.end(), 1);
+    const cudaError_t r = cudaMemcpyAsync(d_active, act.data(), nb * sizeof(int), cudaMemcpyHostToDevice, h.stream);
+    return r == cudaSuccess ? cudaStreamSynchronize(h.stream) : r;
+  };
   for (int cyc = 0; cyc < restarts; ++cyc) {
     // r = b - A x  -> V_0
     spmv_kernel<<<dim3(vb, spmv_blocks(nb)), 256, 0, h.stream>>>(n, nb, op.rp, op.ci, op.vp, Kc, Mc,
@@ -194,25 +221,27 @@ int fgmres(Handle &h, KrylovWork &kw, const MatOp &op, int nb, int m, int restar
       sc[f] = nrm[f] > 0 ? 1.0 / nrm[f] : 0.0;
     }
     if (all) break;
+    KCK(push_active());
     KCK(cudaMemcpyAsync(kw.sc.p, sc.data(), nb * sizeof(double), cudaMemcpyHostToDevice, h.stream));
-    scale_vec_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, V, kw.sc.as<double>(), V);
+    scale_vec_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, V, kw.sc.as<double>(), V, d_active);
     for (int j = 0; j < m; ++j) {
       cd *Vj = V + (size_t)j * nb * n, *Zj = Z + (size_t)j * nb * n;
       int rc = precond(Vj, Zj);
       if (rc) return rc;
       spmv_kernel<<<dim3(vb, spmv_blocks(nb)), 256, 0, h.stream>>>(n, nb, op.rp, op.ci, op.vp, Kc,
-                                                      Mc, Dc, d_omega, h.beta, Zj, w);
+                                                      Mc, Dc, d_omega, h.beta, Zj, w, d_active);
       // classical Gram-Schmidt, twice
       for (int pass = 0; pass < 2; ++pass) {
         cd *hp = hd + (size_t)pass * nb * ldh;
-        multi_dot_kernel<<<dim3(j + 1, nb), 256, 0, h.stream>>>(n, nb, V, w, hp, ldh);
-        multi_axpy_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, j + 1, V, hp, ldh, w);
+        multi_dot_kernel<<<dim3(j + 1, nb), 256, 0, h.stream>>>(n, nb, V, w, hp, ldh, d_active);
+        multi_axpy_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, j + 1, V, hp, ldh, w, d_active);
       }
-      norm2_kernel<<<nb, 256, 0, h.stream>>>(n, w, hn);
+      norm2_kernel<<<nb, 256, 0, h.stream>>>(n, w, hn, d_active);
       KCK(cudaMemcpyAsync(hcol.data(), hd, sizeof(cd) * nb * ldh * 2, cudaMemcpyDeviceToHost, h.stream));
       KCK(cudaMemcpyAsync(nrm.data(), hn, nb * sizeof(double), cudaMemcpyDeviceToHost, h.stream));
       KCK(cudaStreamSynchronize(h.stream));
       all = true;
+      bool stopped = false;
       for (int f = 0; f < nb; ++f) {
         const double hnext = nrm[f];
         sc[f] = hnext > 0 ? 1.0 / hnext : 0.0;
@@ -250,13 +279,16 @@ int fgmres(Handle &h, KrylovWork &kw, const MatOp &op, int nb, int m, int restar
         gf[j] = c * gf[j];
         kf[f] = j + 1;
         ++its[f];
-        if (std::abs(gf[j + 1]) <= tol * bnorm[f] || hnext == 0.0) done[f] = 1;
+        if (std::abs(gf[j + 1]) <= tol * bnorm[f] || hnext == 0.0) done[f] = 1, stopped = true;
         all = all && done[f];
       }
       if (all || j == m - 1) break;
+      if (stopped) KCK(push_active());
       KCK(cudaMemcpyAsync(kw.sc.p, sc.data(), nb * sizeof(double), cudaMemcpyHostToDevice, h.stream));
-      scale_vec_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, w, kw.sc.as<double>(), V + (size_t)(j + 1) * nb * n);
+      scale_vec_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, w, kw.sc.as<double>(), V + (size_t)(j + 1) * nb * n,
+                                                           d_active);
     }
+    KCK(all_active());   // the solution update and the next cycle's residual cover every point
     // least squares: H(0:k,0:k) y = g(0:k), back substitution
     std::vector<cd> yh((size_t)nb * m, cd{0, 0});
     for (int f = 0; f < nb; ++f) {
@@ -274,6 +306,7 @@ int fgmres(Handle &h, KrylovWork &kw, const MatOp &op, int nb, int m, int restar
     combine_kernel<<<dim3(vb, nb), 256, 0, h.stream>>>(n, nb, kw.kf.as<int>(), Z, kw.y.as<cd>(), m, x);
     KCK(cudaGetLastError());
   }
+  KCK(all_active());
   // final true residual check
   spmv_kernel<<<dim3(vb, spmv_blocks(nb)), 256, 0, h.stream>>>(n, nb, op.rp, op.ci, op.vp, Kc, Mc, Dc,
                                                   d_omega, h.beta, x, w);

@@ -167,6 +167,7 @@ struct FrontArgs {
   int64_t n;
   T tiny;                            // static pivot perturbation threshold
   int *nperturb;
+  const int *active;                 // solves: frequencies still iterating (nullptr = all)
 };
 
 template <class T>
@@ -956,6 +957,7 @@ template <class T>
 __global__ void __launch_bounds__(256) front_fwd_kernel(FrontArgs<T> a, const cd *__restrict__ b,
                                                         cd *__restrict__ x, cplx<T> *__restrict__ wv,
                                                         int64_t wstride) {
+  if (a.active && !a.active[blockIdx.y]) return;   // converged in the Krylov loop
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T> *D = reinterpret_cast<cplx<T> *>(smem_raw);
   cplx<T> *v = D + kDiagElems;
@@ -1029,6 +1031,7 @@ constexpr int kSolveRows = 64;   // rows per CTA of the solve GEMV kernels
 template <class T>
 __global__ void __launch_bounds__(256) front_fwd_l21_kernel(FrontArgs<T> a, const cd *__restrict__ x,
                                                             cplx<T> *__restrict__ wv, int64_t wstride) {
+  if (a.active && !a.active[blockIdx.y]) return;   // converged in the Krylov loop
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T> *y = reinterpret_cast<cplx<T> *>(smem_raw);
   const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
@@ -1057,6 +1060,7 @@ __global__ void __launch_bounds__(256) front_fwd_l21_kernel(FrontArgs<T> a, cons
 // frequency, 64 pivot rows); x_U gathered from the ancestors' solution.
 template <class T>
 __global__ void __launch_bounds__(256) front_bwd_u12_kernel(FrontArgs<T> a, cd *__restrict__ x) {
+  if (a.active && !a.active[blockIdx.y]) return;   // converged in the Krylov loop
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T> *xu = reinterpret_cast<cplx<T> *>(smem_raw);
   const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
@@ -1089,6 +1093,7 @@ __global__ void __launch_bounds__(256) front_bwd_u12_kernel(FrontArgs<T> a, cd *
 // then U11 back substitution; x[pivots] <- z.
 template <class T>
 __global__ void __launch_bounds__(256) front_bwd_kernel(FrontArgs<T> a, cd *__restrict__ x) {
+  if (a.active && !a.active[blockIdx.y]) return;   // converged in the Krylov loop
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T> *D = reinterpret_cast<cplx<T> *>(smem_raw);
   cplx<T> *z = D + kDiagElems;
@@ -1147,6 +1152,7 @@ template <class T>
 __global__ void __launch_bounds__(256) front_tfwd_kernel(FrontArgs<T> a, const cd *__restrict__ c,
                                                          cd *__restrict__ x, cplx<T> *__restrict__ wv,
                                                          int64_t wstride) {
+  if (a.active && !a.active[blockIdx.y]) return;   // converged in the Krylov loop
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T> *D = reinterpret_cast<cplx<T> *>(smem_raw);
   cplx<T> *v = D + kDiagElems;
@@ -1199,49 +1205,78 @@ __global__ void __launch_bounds__(256) front_tfwd_kernel(FrontArgs<T> a, const c
 
 // Update rows of the U^T solve: w[r - k] -= sum_i U12[i, r] x_i; CTA per (front,
 // frequency, 256 update rows), one thread per row (coalesced column reads).
+// Update rows of the U^T solve: w[r - k] -= (U12^T w_piv)[r].  CTA per (front,
+// frequency, 32 update rows), lane = row (32 consecutive entries of a U12 row per
+// load); the 8 warps split the pivots and their partial sums are added in warp
+// order (fixed-order, deterministic).
+constexpr int kTColWarps = 8;
 template <class T>
-__global__ void __launch_bounds__(256) front_tfwd_u12_kernel(FrontArgs<T> a, const cd *__restrict__ x,
-                                                             cplx<T> *__restrict__ wv, int64_t wstride) {
+__global__ void __launch_bounds__(32 * kTColWarps) front_tfwd_u12_kernel(FrontArgs<T> a, const cd *__restrict__ x,
+                                                                         cplx<T> *__restrict__ wv, int64_t wstride) {
+  if (a.active && !a.active[blockIdx.y]) return;   // converged in the Krylov loop
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T> *y = reinterpret_cast<cplx<T> *>(smem_raw);
+  __shared__ cplx<T> red[kTColWarps][32];
   const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
   const int k = a.k[f], m = a.m[f], ld = a.ld[f];
-  const int rb = k + blockIdx.z * blockDim.x;
+  const int rb = k + blockIdx.z * 32;
   if (rb >= m) return;
   const cplx<T> *F = a.arena + (int64_t)fq * a.stride + a.off[f];
   const int64_t p0 = a.p0[f];
   for (int i = threadIdx.x; i < k; i += blockDim.x) y[i] = to_t<T>(x[(int64_t)fq * a.n + p0 + i]);
   __syncthreads();
-  const int r = rb + threadIdx.x;
-  if (r >= m) return;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int r = rb + lane;
   cplx<T> acc{0, 0};
-  for (int i = 0; i < k; ++i) acc = acc + cmul(F[(int64_t)i * ld + r], y[i]);
-  cplx<T> *w = wv + (int64_t)fq * wstride + a.relpos_ptr[f] - k;
-  w[r] = w[r] - acc;
+  if (r < m) {
+#pragma unroll 4
+    for (int i = wid; i < k; i += kTColWarps) acc = acc + cmul(F[(int64_t)i * ld + r], y[i]);
+  }
+  red[wid][lane] = acc;
+  __syncthreads();
+  if (wid == 0 && r < m) {
+    cplx<T> s = red[0][lane];
+    for (int q = 1; q < kTColWarps; ++q) s = s + red[q][lane];
+    cplx<T> *w = wv + (int64_t)fq * wstride + a.relpos_ptr[f] - k;
+    w[r] = w[r] - s;
+  }
 }
 
 // First phase of the L^T solve (levels top-down): x[pivots] -= L21^T x_U, with
 // x_U the ancestors' solution at this front's update rows; CTA per (front,
 // frequency, 256 pivots), one thread per pivot (coalesced row reads).
 template <class T>
-__global__ void __launch_bounds__(256) front_tbwd_l21_kernel(FrontArgs<T> a, cd *__restrict__ x) {
+__global__ void __launch_bounds__(32 * kTColWarps) front_tbwd_l21_kernel(FrontArgs<T> a, cd *__restrict__ x) {
+  if (a.active && !a.active[blockIdx.y]) return;   // converged in the Krylov loop
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T> *xu = reinterpret_cast<cplx<T> *>(smem_raw);
+  __shared__ cplx<T> red[kTColWarps][32];
   const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
   const int k = a.k[f], m = a.m[f], ld = a.ld[f];
-  const int ib = blockIdx.z * blockDim.x;
+  const int ib = blockIdx.z * 32;
   if (ib >= k || m == k) return;
   const cplx<T> *F = a.arena + (int64_t)fq * a.stride + a.off[f];
   cd *xf = x + (int64_t)fq * a.n;
   const int64_t *rows = a.rows + a.rows_ptr[f];
   for (int i = threadIdx.x; i < m - k; i += blockDim.x) xu[i] = to_t<T>(xf[rows[k + i]]);
   __syncthreads();
-  const int i = ib + threadIdx.x;
-  if (i >= k) return;
+  // lane = pivot column (32 consecutive entries of an L21 row per load); the 8
+  // warps split the update rows, partial sums added in warp order
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int i = ib + lane;
   cplx<T> acc{0, 0};
-  for (int r = 0; r < m - k; ++r) acc = acc + cmul(F[(int64_t)(k + r) * ld + i], xu[r]);
-  const int64_t p = a.p0[f] + i;
-  xf[p] = cd{xf[p].x - (double)acc.x, xf[p].y - (double)acc.y};
+  if (i < k) {
+#pragma unroll 4
+    for (int r = wid; r < m - k; r += kTColWarps) acc = acc + cmul(F[(int64_t)(k + r) * ld + i], xu[r]);
+  }
+  red[wid][lane] = acc;
+  __syncthreads();
+  if (wid == 0 && i < k) {
+    cplx<T> s = red[0][lane];
+    for (int q = 1; q < kTColWarps; ++q) s = s + red[q][lane];
+    const int64_t p = a.p0[f] + i;
+    xf[p] = cd{xf[p].x - (double)s.x, xf[p].y - (double)s.y};
+  }
 }
 
 // L11^T z = x[pivots] (upper triangular, unit diagonal; entry (i, t) is
@@ -1251,6 +1286,7 @@ __global__ void __launch_bounds__(256) front_tbwd_l21_kernel(FrontArgs<T> a, cd 
 // right after the L11^T solve, before any descendant reads these entries.
 template <class T>
 __global__ void __launch_bounds__(256) front_tbwd_kernel(FrontArgs<T> a, cd *__restrict__ x) {
+  if (a.active && !a.active[blockIdx.y]) return;   // converged in the Krylov loop
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T> *D = reinterpret_cast<cplx<T> *>(smem_raw);
   cplx<T> *z = D + kDiagElems;
@@ -1847,7 +1883,7 @@ struct Sweeper {
   int solve_graphed(int kind, int nb, const cd *b, cd *x) {
     const int64_t n = h.sym.n;
     SS_CK(cudaMemcpyAsync(stage_b, b, (size_t)nb * n * sizeof(cd), cudaMemcpyDeviceToDevice, h.stream));
-    int rc = graphed(kind, nb, {a.arena, a.piv, stage_b, stage_x, stage_wv, a.Kc},
+    int rc = graphed(kind, nb, {a.arena, a.piv, stage_b, stage_x, stage_wv, a.Kc, a.active},
                      [&] { return kind == 1 ? solve(nb, stage_b, stage_x, stage_wv) : solve_t(nb, stage_b, stage_x, stage_wv); });
     if (rc) return rc;
     SS_CK(cudaMemcpyAsync(x, stage_x, (size_t)nb * n * sizeof(cd), cudaMemcpyDeviceToDevice, h.stream));
@@ -2124,9 +2160,8 @@ struct Sweeper {
       front_tfwd_kernel<T><<<dim3(nf, nb), solve_threads(l), sm + kDiagBytes, h.stream>>>(c, cvec, mu, wv, wstride);
       ++launches;
       if (P.lvl_maxu[l] > 0) {
-        const int bs = solve_threads(l);
-        const unsigned z = (unsigned)((P.lvl_maxu[l] + bs - 1) / bs);
-        front_tfwd_u12_kernel<T><<<dim3(nf, nb, z), bs, smk, h.stream>>>(c, mu, wv, wstride);
+        const unsigned z = (unsigned)((P.lvl_maxu[l] + 31) / 32);
+        front_tfwd_u12_kernel<T><<<dim3(nf, nb, z), 32 * kTColWarps, smk, h.stream>>>(c, mu, wv, wstride);
         ++launches;
       }
     }
@@ -2135,10 +2170,9 @@ struct Sweeper {
       c.fronts = h.d_level_fronts.as<int>() + S.level_ptr[l];
       const int nf = (int)(S.level_ptr[l + 1] - S.level_ptr[l]);
       if (P.lvl_maxu[l] > 0) {
-        const int bs = solve_threads(l);
-        const unsigned z = (unsigned)((P.lvl_maxk[l] + bs - 1) / bs);
-        front_tbwd_l21_kernel<T><<<dim3(nf, nb, z), bs, (size_t)P.lvl_maxu[l] * sizeof(cplx<T>), h.stream>>>(c,
-                                                                                                          mu);
+        const unsigned z = (unsigned)((P.lvl_maxk[l] + 31) / 32);
+        front_tbwd_l21_kernel<T><<<dim3(nf, nb, z), 32 * kTColWarps, (size_t)P.lvl_maxu[l] * sizeof(cplx<T>),
+                                   h.stream>>>(c, mu);
         ++launches;
       }
       front_tbwd_kernel<T><<<dim3(nf, nb), solve_threads(l), smk + kDiagBytes + pivb, h.stream>>>(c, mu);
@@ -2213,9 +2247,12 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
     }
     if (vec > 48 * 1024) {
       SS_CK(cudaFuncSetAttribute(front_fwd_l21_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vec));
-      SS_CK(cudaFuncSetAttribute(front_tfwd_u12_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vec));
+      // (these two also hold an 8 x 32 static reduction tile)
+      SS_CK(cudaFuncSetAttribute(front_tfwd_u12_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 std::min(vec, 223 * 1024)));
       SS_CK(cudaFuncSetAttribute(front_bwd_u12_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vec));
-      SS_CK(cudaFuncSetAttribute(front_tbwd_l21_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vec));
+      SS_CK(cudaFuncSetAttribute(front_tbwd_l21_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 std::min(vec, 223 * 1024)));
     }
   }
   Plan &P = *static_cast<Plan *>(h.plan[pi]);
@@ -2286,6 +2323,12 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
   DBuf &stb = h.wk[14], &stx = h.wk[15];
   SS_CK(dalloc(stb, (size_t)B * n * sizeof(cd)));
   SS_CK(dalloc(stx, (size_t)B * n * sizeof(cd)));
+  {
+    // frequencies still iterating in the Krylov loops (read by the solve kernels)
+    SS_CK(dalloc(h.dmask, (size_t)B * sizeof(int)));
+    std::vector<int> ones(B, 1);
+    SS_CK(cudaMemcpy(h.dmask.p, ones.data(), (size_t)B * sizeof(int), cudaMemcpyHostToDevice));
+  }
   DBuf &tcerr = h.wk[13];
   SS_CK(dalloc(tcerr, sizeof(int)));
   SS_CK(cudaMemsetAsync(tcerr.p, 0, sizeof(int), h.stream));
@@ -2321,6 +2364,7 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
   a.n = n;
   a.tiny = sizeof(T) == 8 ? (T)h.opt.tiny_c128 : (T)h.opt.tiny_c64;
   a.nperturb = npert.as<int>();
+  a.active = h.dmask.as<int>();
   sw.wstride = W;
   const int maxit = sizeof(T) == 8 ? 1 : 40;   // FP64: one refinement step
   const double tol = sizeof(T) == 8 ? 1e-15 : 1e-12;
@@ -2371,7 +2415,7 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
       std::vector<char> kconv;
       auto pre = [&](const cd *src, cd *dst) { return sw.solve_graphed(1, nb, src, dst); };
       rc = fgmres(h, kw, opA, nb, krylov_m, krylov_restarts, tol_p, a.Kc, a.Mc, a.Dc, dom.as<double>(), b.as<cd>(),
-                  x.as<cd>(), pre, kits, kconv);
+                  x.as<cd>(), pre, kits, kconv, h.dmask.as<int>());
       if (rc) return rc;
       for (int f = 0; f < nb; ++f) hit[f] = kits[f], conv[f] = kconv[f], steps_p += kits[f];
     }
@@ -2423,7 +2467,7 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
         std::vector<char> kconv;
         auto pre = [&](const cd *src, cd *dst) { return sw.solve_graphed(2, nb, src, dst); };
         rc = fgmres(h, kw, opT, nb, krylov_m, krylov_restarts, tol_a, a.Kc, a.Mc, a.Dc, dom.as<double>(),
-                    cvec.as<cd>(), mu.as<cd>(), pre, kits, kconv);
+                    cvec.as<cd>(), mu.as<cd>(), pre, kits, kconv, h.dmask.as<int>());
         if (rc) return rc;
         for (int f = 0; f < nb; ++f) hit[f] += kits[f], aconv[f] = kconv[f], steps_a += kits[f];
       } else {

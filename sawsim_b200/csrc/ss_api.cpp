@@ -298,9 +298,8 @@ extern "C" int ss_analyze(ss_handle *hp) {
 
 extern "C" int ss_set_damping(ss_handle *hp, double beta) {
   H_CHECK(hp);
-  if (!std::isfinite(beta)) return fail(h, SS_EINVAL, "damping: beta must be finite");
+  if (!std::isfinite(beta) || beta < 0.0) return fail(h, SS_EINVAL, "damping: beta must be finite and >= 0");
   if (beta != 0.0 && !h.have_D) return fail(h, SS_ESTATE, "damping: assemble D first (damping materials)");
-  if (beta < 0.0) return fail(h, SS_EINVAL, "damping: beta must be >= 0");
   h.beta = beta;
   h.scale_w = -1;
   free_plans(h);   // the captured launch graphs bake beta and the damping matrix in

@@ -145,6 +145,7 @@ struct Handle {
   int auto_prec = -1;
   DBuf dKs, dMs, dDs;                    // equilibrated condensed values
   DBuf tc_stage;                         // packed tensor-core Schur operands (mixed sweeps)
+  DBuf dmask;                            // per chunk frequency: still iterating in a Krylov loop
   double scale_w = -1;                   // frequency the scaling was computed at
   // solver options (ss_set_option); kept until changed
   struct Options {

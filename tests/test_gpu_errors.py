@@ -72,6 +72,8 @@ def test_non_finite_inputs_rejected(small):
                L.ptr(em, C.c_double), L.ptr(epsm, C.c_double)) == L.SS_EINVAL
     assert _rc(h, 'ss_set_damping', float('nan')) == L.SS_EINVAL
     assert _rc(h, 'ss_set_damping', -1.0) == L.SS_EINVAL
+    # a positive beta without damping materials is a call out of order
+    assert _rc(h, 'ss_set_damping', 1e-12) == L.SS_ESTATE
 
 
 def test_options_validated(small):
