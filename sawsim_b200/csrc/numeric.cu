@@ -1547,7 +1547,18 @@ Plan *build_plan(Handle &h, int small_m, bool tensor_schur) {
     P->tt_ptr[1].assign(1, 0);
     for (int l = 0; l < S.nlevel; ++l) {
       int64_t base = 0;
+      // levels whose fronts are mostly padding in 128-row tiles stay on the SIMT
+      // candidate (no packed operands, no staging rows)
+      double work = 0, padded = 0;
       for (int q = P->large_ptr[l]; q < P->large_ptr[l + 1]; ++q) {
+        const int f = P->fronts_large[q], k = S.k[f], u = S.m[f] - k;
+        if (u <= 0 || k <= 0) continue;
+        const double au = (u + tc::PADC - 1) / tc::PADC * tc::PADC, kp = (k + tc::KCH - 1) / tc::KCH * tc::KCH;
+        work += (double)u * u * k;
+        padded += au * au * kp;
+      }
+      const bool eligible = work > 0 && padded <= 2.5 * work;
+      for (int q = P->large_ptr[l]; q < P->large_ptr[l + 1] && eligible; ++q) {
         const int f = P->fronts_large[q], k = S.k[f], m = S.m[f], u = m - k;
         if (u <= 0 || k <= 0) continue;
         const int kc = (k + tc::KCH - 1) / tc::KCH, au = (u + tc::PADC - 1) / tc::PADC * tc::PADC;
@@ -1930,13 +1941,15 @@ struct Sweeper {
       // complex64: candidates 0 / 1 pack the level's operands and run the TMA +
       // tcgen05 kernel with 128 / 64 complex columns per tile; 2 SIMT FP32 128x64
       const int64_t t0 = P.schur_ptr[l], t1 = P.schur_ptr[l + 1];
-      if (c == 2 || !P.tma_ok) {
-        front_gemm_kernel<T, kSquare><<<dim3((unsigned)(t1 - t0), nb), 256, 0, h.stream>>>(b, tasks + t0);
+      const int v = c;   // tile variant
+      // SIMT tiles: the third candidate, and the fallback where a level has no
+      // packed operands (mostly padding) or the staging buffer is not available
+      if (c == 2 || !P.tma_ok || P.tt_ptr[v > 1 ? 0 : v][l + 1] == P.tt_ptr[v > 1 ? 0 : v][l]) {
+        if (t1 > t0)
+          front_gemm_kernel<T, kSquare><<<dim3((unsigned)(t1 - t0), nb), 256, 0, h.stream>>>(b, tasks + t0);
         return;
       }
-      const int v = c;   // tile variant
       const int64_t i0 = P.pi_ptr[l], i1 = P.pi_ptr[l + 1], q0 = P.tt_ptr[v][l], q1 = P.tt_ptr[v][l + 1];
-      if (i1 == i0 || q1 == q0) return;
       cf *ar = reinterpret_cast<cf *>(b.arena);
       tc::pack_kernel<<<dim3((unsigned)(i1 - i0), nb), tc::PACK_THREADS, 0, h.stream>>>(
           ar, b.stride, b.off, b.ld, b.k, b.m, P.d_pk.template as<tc::PackFront>(), P.d_pitems.template as<int2>() + i0,
@@ -2025,7 +2038,12 @@ struct Sweeper {
     }
     for (int l = 0; l < S.nlevel; ++l) {
       int best = 0;
-      if (force) {
+      // complex64 levels without packed operands run the SIMT tiles whatever the
+      // candidate: they count as the SIMT candidate
+      const bool no_tma = sizeof(T) == 4 && (!P.tma_ok || P.tt_ptr[0][l + 1] == P.tt_ptr[0][l]);
+      if (no_tma) {
+        best = 2;
+      } else if (force) {
         best = std::max(0, std::min(NC - 1, atoi(force)));
       } else {
         for (int c = 1; c < NC; ++c)
@@ -2288,8 +2306,21 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
   for (int i = 0; i < 16; ++i) fr += h.wk[i].bytes;
   fr += h.tc_stage.bytes;
   int B = (int)std::max(1.0, std::min((double)n_f, std::min(256.0, (0.85 * (double)fr - 512e6) / per)));
-  // a buffer that must grow is released first so that old and new never coexist
-  if ((size_t)B * S.arena * sizeof(cplx<T>) > arena.bytes) arena.release();
+  // The chunk size counted every buffer above as free, so each one is brought to
+  // exactly this sweep's size: larger ones (an earlier sweep's chunk or precision)
+  // are released before anything grows, so old and new never coexist.
+  {
+    const size_t vecb = (size_t)B * n * sizeof(cd);
+    const size_t need[16] = {(size_t)B * S.arena * sizeof(cplx<T>), (size_t)B * n * sizeof(int),
+                             (size_t)B * std::max<int64_t>(W, 1) * sizeof(cplx<T>), vecb, vecb, vecb, vecb,
+                             B * sizeof(double), B * sizeof(int), 2 * B * sizeof(double), 2 * B * sizeof(cd),
+                             need_adjoint ? vecb : 0, need_adjoint ? vecb : 0, sizeof(int), vecb, vecb};
+    for (int i = 0; i < 16; ++i)
+      if (h.wk[i].bytes != need[i]) h.wk[i].release();
+    const size_t stage = sizeof(T) == 4 ? (size_t)B * P.stage_rows * tc::ROWB : 0;
+    if (h.tc_stage.bytes != stage) h.tc_stage.release();
+    if (krylov > 0 && kw.V.bytes != vecb * (size_t)(krylov_m + 1)) kw.release();
+  }
   SS_CK(dalloc(arena, (size_t)B * S.arena * sizeof(cplx<T>)));
   if (sizeof(T) == 4) {
     // staging buffer of the packed Schur operands (one level at a time) and the
@@ -2297,7 +2328,6 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
     P.tma_ok = false;
     const int64_t rows = (int64_t)B * P.stage_rows;
     if (P.stage_rows > 0 && rows < ((int64_t)1 << 31)) {
-      if ((size_t)rows * tc::ROWB > h.tc_stage.bytes) h.tc_stage.release();
       SS_CK(dalloc(h.tc_stage, (size_t)rows * tc::ROWB));
       const int rc = encode_stage_map(h, P.tmap, h.tc_stage.p, rows);
       if (rc) return rc;

@@ -94,8 +94,8 @@ def test_every_schur_tile_candidate_is_exact(mid, tile, monkeypatch):
 def test_every_complex64_schur_candidate_converges(mid, tile, monkeypatch):
     """Every complex64 Schur kernel (packed operands loaded by TMA into persistent
     warp-specialised tcgen05 CTAs with double-buffered TMEM accumulators, 128- and
-    64-column tiles; SIMT FP32 tiles),
-    each forced on every level, gives a mixed sweep within 1e-6 of FP64."""
+    64-column tiles; SIMT FP32 tiles), each forced on every level it serves, gives
+    a mixed sweep within 1e-6 of FP64 without any FP64 re-solve."""
     case, _, g = mid
     f = np.linspace(case.freqs[0], case.freqs[-1], 5)
     Q64, _, _ = g.charges(2 * np.pi * f, 1.0, 'fp64')
@@ -108,7 +108,12 @@ def test_every_complex64_schur_candidate_converges(mid, tile, monkeypatch):
         e.close()
     assert (st == 0).all() and s['fp64_resolved'] == 0      # converged in mixed precision
     counts = [s['schur_tile_simt128'], s['schur_tile_simt64'], s['schur_tile_dmma']]
-    assert counts[tile] > 0 and sum(counts) == counts[tile]
+    # levels whose fronts would be mostly padding in 128-row tensor-core tiles
+    # always run the SIMT tiles
+    if tile < 2:
+        assert counts[tile] > 0 and counts[1 - tile] == 0
+    else:
+        assert counts[0] == counts[1] == 0 and counts[2] > 0
     assert np.max(np.abs(Q - Q64) / np.abs(Q64)) < 1e-6
 
 
