@@ -53,6 +53,8 @@ def parse():
     p.add_argument('--points', type=int, default=None)
     p.add_argument('--no-cpu-baseline', action='store_true')
     p.add_argument('--no-modes', action='store_true', help='skip the untimed FP64-vs-mixed comparison')
+    p.add_argument('--gradient', action='store_true',
+                   help='time Y11 and dY11/dp by the adjoint on a parametrised cell instead of the sweep')
     p.add_argument('--no-full-point', action='store_true',
                    help='reference arm: skip the one measured full-size CPU point')
     return p.parse_args()
@@ -496,8 +498,60 @@ def oracle_check(c, eng, case_name):
     return dict(fp64_backward_error_in_oracle_system=out)
 
 
+def gradient_arm(a):
+    """Y11 and dY11/dp by the adjoint (``autograd.y11_and_jacobian``) at points
+    spanning fr..fa of a parametrised cell, with a central-difference check of
+    two parameters at two points (configs 4 and 5 of the gradient workload)."""
+    from sawsim_b200 import autograd, params
+    from sawsim_b200.metrics import resonances
+    models = {'me1_64x256': lambda: params.Q9Model(64, 256),
+              'me1_128x512': lambda: params.Q9Model(128, 512, stack='four_layer'),
+              'hex_8x4x48': lambda: params.HexModel(8, 4, 48),
+              'hex_12x6x80': lambda: params.HexModel(12, 6, 80, stack='four', f0=1.5e9, f1=2.1e9)}
+    model = models[a.case]()
+    v = model.defaults()
+    # the band around the resonance pair: a coarse FP64 sweep of the model's band
+    case = model.build(v)
+    eng = model.engine(case)
+    try:
+        fc = np.linspace(model.f0, model.f1, 41)
+        Q, _, _ = eng.charges(2 * np.pi * fc, 1.0, 'fp64')
+        r = resonances(fc, model.y11(2 * np.pi * fc, Q, 1.0, case))
+    finally:
+        eng.close()
+    fr, fa = r['fr_ghz'] * 1e9, r['fa_ghz'] * 1e9
+    d = fa - fr
+    f = np.linspace(fr - 0.25 * d, fa + 0.25 * d, a.points or 64)
+    t = time.perf_counter()
+    Y, dY, st = autograd.y11_and_jacobian(model, v, f, a.precision)
+    wall = time.perf_counter() - t
+    # central differences (relative step 1e-5, FP64 sweeps) of two parameters at two points
+    idx = [int(np.argmin(np.abs(f - fr))), int(np.argmin(np.abs(f - fa)))]
+    checks = []
+    for j in (0, 1):
+        hstep = 1e-5 * abs(v[j])
+        vp, vm = v.copy(), v.copy()
+        vp[j] += hstep
+        vm[j] -= hstep
+        yp, _ = autograd.y11_only(model, vp, f[idx], 'fp64')
+        ym, _ = autograd.y11_only(model, vm, f[idx], 'fp64')
+        fd = (yp - ym) / (2 * hstep)
+        checks.append(dict(param=model.names[j], rel_err=[float(abs(dY[i, j] - fd[q]) / abs(fd[q]))
+                                                          for q, i in enumerate(idx)]))
+    return dict(metric='Y11 and dY11/dp points/s (adjoint)', value=f.size / wall, unit='points/s', n_gpus=1,
+                steps=1, warmup=0, higher_is_better=True, scaling='weak', vs_baseline=None,
+                dtype='c64+f64' if a.precision != 'fp64' else 'c128', data='synthetic',
+                config=dict(workload=f'{a.case} parametrised ({type(model).__name__}), {f.size} points spanning fr..fa',
+                            n_params=len(model.names), params=model.names, precision=a.precision,
+                            fr_ghz=r['fr_ghz'], fa_ghz=r['fa_ghz'], points_not_converged=int(np.sum(st != 0)),
+                            wall_s_including_engine_build=wall, fd_checks=checks))
+
+
 def main():
     a = parse()
+    if a.gradient:
+        print(json.dumps(gradient_arm(a)), flush=True)
+        return
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))
     local = int(os.environ.get('LOCAL_RANK', '0'))

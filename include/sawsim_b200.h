@@ -45,7 +45,8 @@ typedef struct ss_handle ss_handle;
 #define SS_PREC_MIXED  1   /* complex64 fronts, 3xTF32 tensor-core Schur updates
                               (or SIMT FP32 where the autotuner finds it faster),
                               FP64 residual, FP64 flexible GMRES on the primal and
-                              the adjoint, dual-weighted charge correction       */
+                              the adjoint, dual-weighted charge correction; points
+                              that do not converge are re-solved in FP64         */
 #define SS_PREC_AUTO   2   /* probe MIXED on the two band ends with 12 Krylov
                               steps; MIXED if both converge, else FP64; the
                               decision is kept for the same two end
@@ -214,9 +215,11 @@ int ss_stats(const ss_handle *h, double *out, int n);
  * Solver options, by name (the reference's PARDISO / SuperLU calls,
  * sweep.py:346-353, take none; these tune the replacement's refinement):
  *   krylov_restart    FGMRES restart length of the mixed sweep (default 30)
- *   krylov_cycles     FGMRES restarts (default 4)
+ *   krylov_cycles     FGMRES restarts (default 1)
  *   krylov_tol        relative residual target of the primal and adjoint
- *                     Krylov solves (default 1e-10)
+ *                     Krylov solves (default 1e-8; with the dual-weighted
+ *                     charge correction the charge error is about the product
+ *                     of the two residuals' effects)
  *   pivot_tiny_c128   static pivot perturbation of complex128 fronts: a pivot
  *                     of modulus below it is replaced by it (default 1e-13; the
  *                     system is equilibrated to unit row and column maxima)

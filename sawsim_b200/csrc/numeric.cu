@@ -991,7 +991,8 @@ __global__ void __launch_bounds__(256) front_fwd_kernel(FrontArgs<T> a, const cd
   }
   __syncthreads();
   // blocked unit-lower solve: warp 0 solves each 32x32 diagonal block with
-  // shuffles, then every warp updates the rows below (coalesced row dots)
+  // shuffles, then one thread per row below it subtracts the block (each thread's
+  // entries are one contiguous run of its row, all of them in flight at once)
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int jb = 0; jb < k; jb += 32) {
     const int je = min(k, jb + 32), bw = je - jb;
@@ -1008,14 +1009,12 @@ __global__ void __launch_bounds__(256) front_fwd_kernel(FrontArgs<T> a, const cd
       if (lane < bw) v[jb + lane] = x;
     }
     __syncthreads();
-    const cplx<T> vt = lane < bw ? v[jb + lane] : cplx<T>{0, 0};
-    for (int r = je + wid; r < k; r += nw) {
-      cplx<T> acc = lane < bw ? cmul(F[(int64_t)r * ld + jb + lane], vt) : cplx<T>{0, 0};
-      for (int o = 16; o > 0; o >>= 1) {
-        acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
-        acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
-      }
-      if (lane == 0) v[r] = v[r] - acc;
+    for (int r = je + threadIdx.x; r < k; r += blockDim.x) {
+      const cplx<T> *Lr = F + (int64_t)r * ld + jb;
+      cplx<T> acc = v[r];
+#pragma unroll 8
+      for (int t = 0; t < bw; ++t) acc = cfms(acc, Lr[t], v[jb + t]);
+      v[r] = acc;
     }
     __syncthreads();
   }
@@ -1106,7 +1105,8 @@ __global__ void __launch_bounds__(256) front_bwd_kernel(FrontArgs<T> a, cd *__re
   __syncthreads();
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   // blocked upper solve from the bottom: warp 0 solves each diagonal block,
-  // then every warp updates the rows above it
+  // then one thread per row above it subtracts the block (contiguous runs of the
+  // rows, all of a thread's loads in flight at once)
   for (int je = k; je > 0; je -= 32) {
     const int jb = max(0, je - 32), bw = je - jb;
     stage_diag(D, F, ld, jb, bw);
@@ -1125,14 +1125,12 @@ __global__ void __launch_bounds__(256) front_bwd_kernel(FrontArgs<T> a, cd *__re
       if (lane < bw) z[jb + lane] = x;
     }
     __syncthreads();
-    const cplx<T> xt = lane < bw ? z[jb + lane] : cplx<T>{0, 0};
-    for (int r = wid; r < jb; r += nw) {
-      cplx<T> acc = lane < bw ? cmul(F[(int64_t)r * ld + jb + lane], xt) : cplx<T>{0, 0};
-      for (int o = 16; o > 0; o >>= 1) {
-        acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
-        acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
-      }
-      if (lane == 0) z[r] = z[r] - acc;
+    for (int r = threadIdx.x; r < jb; r += blockDim.x) {
+      const cplx<T> *Ur = F + (int64_t)r * ld + jb;
+      cplx<T> acc = z[r];
+#pragma unroll 8
+      for (int t = 0; t < bw; ++t) acc = cfms(acc, Ur[t], z[jb + t]);
+      z[r] = acc;
     }
     __syncthreads();
   }
@@ -1701,26 +1699,28 @@ int launch_condense(Handle &h) {
 
 namespace ss {
 
-// Krylov settings of one sweep: FGMRES restart length, restarts and the relative
-// residual target of the primal and adjoint solves (the handle's options; with
-// the dual-weighted correction the charge error is the product of the two
-// residuals' effects, ~1e-12 relative at the default target 1e-10)
+// Krylov settings of one sweep (the handle's options): FGMRES restart length,
+// restarts and the relative residual target of the primal and adjoint solves.
+// With the dual-weighted charge correction the charge error is about the product
+// of the two residuals' effects.
 struct SweepOpts {
   int krylov_m = 30;
-  int restarts = 4;
-  double tol = 1e-10;
+  int restarts = 1;
+  double tol = 1e-8;
 };
 
 // Fronts with m up to this are factored whole in shared memory (one CTA each);
 // wider ones take the level-batched panel path.  The ceiling is what one CTA's
 // shared memory holds (112^2 x 16 bytes, 160^2 x 8 bytes); SS_SMALL_FRONT_M
 // overrides the default (a tuning knob).  On the 262k-DOF ME1 cell the batched
-// path is as fast as the one-CTA kernel up to m = 96 and faster beyond it (one
-// CTA per SM at these shared-memory sizes leaves the pivot chain exposed).
+// path is as fast as the one-CTA kernel up to m = 96 and faster beyond it, in both
+// precisions (measured: the complex64 factorisation takes 1446 ms for 201 points
+// at 96, 1521 ms at 128, where the cell's 4256 leaves of m = 97 fall into the
+// one-CTA kernel).
 template <class T>
 static int small_limit() {
   const int cap = sizeof(T) == 8 ? 112 : 160;
-  int v = sizeof(T) == 8 ? 96 : 128;
+  int v = 96;
   if (const char *e = getenv("SS_SMALL_FRONT_M")) v = atoi(e);
   return std::max(0, std::min(cap, v));
 }

@@ -150,8 +150,8 @@ struct Handle {
   // solver options (ss_set_option); kept until changed
   struct Options {
     int krylov_m = 30;                   // FGMRES restart length of the mixed sweep
-    int krylov_cycles = 4;               // FGMRES restarts
-    double krylov_tol = 1e-10;           // relative residual target (primal and adjoint)
+    int krylov_cycles = 1;               // FGMRES restarts
+    double krylov_tol = 1e-8;            // relative residual target (primal and adjoint)
     double tiny_c128 = 1e-13;            // static pivot perturbation, complex128 fronts
     double tiny_c64 = 1e-6;              // static pivot perturbation, complex64 fronts
     int fp64_fallback = 1;               // re-solve unconverged mixed points in FP64

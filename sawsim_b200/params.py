@@ -203,6 +203,8 @@ class HexModel:
     nz: int = 48
     seed: int = 0
     stack: str = 'double'
+    f0: float = 1.6e9        # band (Hz); the PML is frozen at its top
+    f1: float = 2.0e9
     crystal: mt.Material = field(init=False)
     euler: np.ndarray = field(init=False)
 
@@ -244,7 +246,7 @@ class HexModel:
         bottom = float(pos_m[:, 2].min())
         pml = [cases.PML(tag=cell.pml_tag, kind='z', za=cell.pml_top_um * 1e-6, zp=bottom)]
         bc = cases.bc_periodic_3d(cell.sets, pos_m, pos_m.shape[0])
-        return cases.HexCase('hex_param', cell, pos_m, cell.HEXAS27, mats, idx, pml, bc, np.linspace(1.6e9, 2.0e9, 5),
+        return cases.HexCase('hex_param', cell, pos_m, cell.HEXAS27, mats, idx, pml, bc, np.linspace(self.f0, self.f1, 5),
                              dict(seed=self.seed, nx=self.nx, ny=self.ny, nz=self.nz))
 
     def engine(self, case, device=0):

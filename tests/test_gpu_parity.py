@@ -93,7 +93,11 @@ def test_adjoint_solves_transposed_system(pair, precision, tol):
     w = 2 * np.pi * case.freqs[len(case.freqs) // 3]
     A, _ = o.system(w)
     kq = (o._T.T @ o.kts)[o.active]
-    lam = g.solve_adjoint(w, precision)
+    g.set_option('krylov_tol', 1e-10)         # the adjoint alone, at a tight Krylov target
+    try:
+        lam = g.solve_adjoint(w, precision)
+    finally:
+        g.set_option('krylov_tol', 1e-8)
     At = A.T.tocsr()
     eta = np.linalg.norm(At @ lam - kq, np.inf) / (abs(At).sum(axis=1).max() * np.linalg.norm(lam, np.inf) +
                                                    np.linalg.norm(kq, np.inf))
