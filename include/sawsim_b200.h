@@ -194,7 +194,8 @@ int ss_adjoint_gradient(ss_handle *h, int n_f, const double *omega, double V, in
  *  18 refinement / Krylov steps of the last ss_sweep (sum over points),
  *  19 precision the last ss_sweep ran in (SS_PREC_FP64 or SS_PREC_MIXED),
  *  20-22 levels whose Schur update uses the autotuner's candidate 0, 1, 2
- *  (FP64 sweep: SIMT 128x64, SIMT 64x64, FP64 tensor-core DMMA 64x64; mixed
+ *  (FP64 sweep: SIMT 128x64, FP64 tensor-core DMMA 64x64 with three real
+ *  products per complex block, the same with four; mixed
  *  sweep: packed operands + TMA + tcgen05 3xTF32 with 128 / 64 complex columns
  *  per tile, SIMT FP32 128x64),
  *  23 1 if the panel-step GEMMs use DMMA tiles (128x32 / 32x128), else 0,
@@ -241,7 +242,8 @@ int ss_set_option(ss_handle *h, const char *name, double value);
  * warm-up.  kernel: 0 FP64 DMMA 64x64 tiles, 1 FP64 SIMT 128x64, 2 complex64
  * TMA + tcgen05 3xTF32 with 128-column tiles, 3 the same with 64-column tiles
  * (operands packed once before the timed launches), 4 complex64 SIMT FP32
- * 128x64.  Allocates and frees its fronts (at most 64 GB).
+ * 128x64, 5 FP64 DMMA 64x64 with three real products per complex block.
+ * Allocates and frees its fronts (at most 64 GB).
  */
 int ss_measure_gemm_ceiling(ss_handle *h, int kernel, int m, int k, int n_fronts, int reps,
                             double *tflops);

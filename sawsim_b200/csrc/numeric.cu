@@ -932,6 +932,113 @@ __global__ void __launch_bounds__(128, 3) front_dmma_kernel(FrontArgs<double> a,
   }
 }
 
+// The same 64x64 Schur tile with Gauss's three-multiplication complex product:
+// P1 = Ar Br, P2 = Ai Bi, P3 = (Ar + Ai)(Br + Bi), then Re = P1 - P2 and
+// Im = P3 - P1 - P2, so each 8x8x4 complex block is three real DMMAs instead of
+// four (the FP64 tensor pipe is the bound of this update).  The algorithmic flop
+// count is unchanged (8 per complex multiply-add).  Normwise the product is as
+// stable as the four-product form; the imaginary part's error is bounded by
+// u (|Ar| + |Ai|)(|Br| + |Bi|) per term instead of u (|Ar||Bi| + |Ai||Br|).
+// Three accumulator sets (96 doubles per thread): two CTAs per SM.
+__global__ void __launch_bounds__(128, 2) front_dmma3_kernel(FrontArgs<double> a, const GemmTask *__restrict__ tasks) {
+  constexpr int kDmmaBM = 64, kDmmaBN = 64, kDmmaBS = kDmmaBN + 2;
+  __shared__ __align__(16) cd As[2][kDmmaBM * kDmmaAS];
+  __shared__ __align__(16) cd Bs[2][kDmmaBK * kDmmaBS];
+  const GemmTask tk = tasks[blockIdx.x];
+  const int fq = blockIdx.y;
+  const int ld = a.ld[tk.f];
+  cd *F = a.arena + (int64_t)fq * a.stride + a.off[tk.f];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int wm = wid / 2, wn = wid % 2;          // warp tile origin (32 x 32 complex)
+  const int g = lane >> 2, t = lane & 3;
+  double p1[4][4][2], p2[4][4][2], p3[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) p1[i][j][e] = p2[i][j][e] = p3[i][j][e] = 0.0;
+  auto issue = [&](int buf, int kb) {
+#pragma unroll
+    for (int q = 0; q < kDmmaBM * kDmmaBK / 128; ++q) {
+      const int idx = threadIdx.x + 128 * q;
+      const int r = idx / kDmmaBK, k = idx % kDmmaBK;
+      const int gr = tk.r0 + r, gk = kb + k;
+      const bool ok = gr < tk.rhi && gk < tk.kk1;
+      cp_async16_cd((uint32_t)__cvta_generic_to_shared(&As[buf][r * kDmmaAS + dmma_acol(r, k)]),
+                    ok ? F + (int64_t)gr * ld + gk : F, ok ? 16u : 0u);
+    }
+#pragma unroll
+    for (int q = 0; q < kDmmaBK * kDmmaBN / 128; ++q) {
+      const int idx = threadIdx.x + 128 * q;
+      const int k = idx / kDmmaBN, c = idx % kDmmaBN;
+      const int gk = kb + k, gc = tk.c0 + c;
+      const bool ok = gk < tk.kk1 && gc < tk.chi;
+      cp_async16_cd((uint32_t)__cvta_generic_to_shared(&Bs[buf][k * kDmmaBS + c]),
+                    ok ? F + (int64_t)gk * ld + gc : F, ok ? 16u : 0u);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  const int nk = (tk.kk1 - tk.kk0 + kDmmaBK - 1) / kDmmaBK;
+  issue(0, tk.kk0);
+  for (int kc = 0; kc < nk; ++kc) {
+    const int buf = kc & 1;
+    if (kc + 1 < nk) {
+      issue(buf ^ 1, tk.kk0 + (kc + 1) * kDmmaBK);
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kDmmaBK; kk += 4) {
+      cd av[4];
+      double as[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int ar = wm * 32 + i * 8 + g;
+        av[i] = As[buf][ar * kDmmaAS + dmma_acol(ar, kk + t)];
+        as[i] = av[i].x + av[i].y;
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const cd bv = Bs[buf][(kk + t) * kDmmaBS + wn * 32 + j * 8 + g];
+        const double bs = bv.x + bv.y;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          dmma(p1[i][j][0], p1[i][j][1], av[i].x, bv.x);
+          dmma(p2[i][j][0], p2[i][j][1], av[i].y, bv.y);
+          dmma(p3[i][j][0], p3[i][j][1], as[i], bs);
+        }
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = tk.r0 + wm * 32 + i * 8 + g;
+    const bool rok = r < tk.rhi;
+    cd *Fr = F + (int64_t)(rok ? r : tk.r0) * ld;
+    cd cv[4][2];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int c = tk.c0 + wn * 32 + j * 8 + 2 * t + e;
+        cv[j][e] = (rok && c < tk.chi) ? Fr[c] : cd{0.0, 0.0};
+      }
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int c = tk.c0 + wn * 32 + j * 8 + 2 * t + e;
+        const double re = p1[i][j][e] - p2[i][j][e];
+        const double im = p3[i][j][e] - p1[i][j][e] - p2[i][j][e];
+        if (rok && c < tk.chi) Fr[c] = cv[j][e] - cd{re, im};
+      }
+  }
+}
+
 }  // namespace ss
 
 namespace ss {
@@ -1933,8 +2040,8 @@ struct Sweeper {
       front_gemm_kernel<T, kShort><<<dim3((unsigned)(t1 - t0), nb), 256, 0, h.stream>>>(b, tasks + t0);
   }
 
-  // FP64 Schur update of level l with candidate tile c (0 SIMT 128x64, 1 SIMT
-  // 64x64, 2 DMMA 64x64)
+  // FP64 Schur update of level l with candidate tile c (0 SIMT 128x64, 1 DMMA
+  // 64x64 with three real products per complex block, 2 DMMA 64x64 with four)
   void schur_launch(const FrontArgs<T> &b, int l, int c, int nb) {
     const GemmTask *tasks = P.d_tasks.template as<GemmTask>();
     if constexpr (sizeof(T) == 4) {
@@ -1971,10 +2078,12 @@ struct Sweeper {
       return;
     }
     const int64_t t0 = P.schur_ptr_b[l], t1 = P.schur_ptr_b[l + 1];
-    if (c == 1)
-      front_gemm_kernel<T, kSquare64><<<dim3((unsigned)(t1 - t0), nb), 256, 0, h.stream>>>(b, tasks + t0);
-    else if constexpr (sizeof(T) == 8)
-      front_dmma_kernel<2, 2><<<dim3((unsigned)(t1 - t0), nb), 128, 0, h.stream>>>(b, tasks + t0);
+    if constexpr (sizeof(T) == 8) {
+      if (c == 1)
+        front_dmma3_kernel<<<dim3((unsigned)(t1 - t0), nb), 128, 0, h.stream>>>(b, tasks + t0);
+      else
+        front_dmma_kernel<2, 2><<<dim3((unsigned)(t1 - t0), nb), 128, 0, h.stream>>>(b, tasks + t0);
+    }
   }
 
   // Autotuner: time every candidate on every level with Schur work, on the chunk's
@@ -2742,7 +2851,8 @@ __global__ void fill_hash_kernel(int64_t n, cplx<T> *x) {
 // launches after one warm-up; returns the median algorithmic rate (8 real flops
 // per complex multiply-add).  kernel: 0 FP64 DMMA 64x64, 1 FP64 SIMT 128x64,
 // 2 / 3 complex64 TMA + tcgen05 3xTF32 with 128 / 64-column tiles (operands
-// packed once before the timed launches),
+// packed once before the timed launches), 5 FP64 DMMA 64x64 with three real
+// products per complex block,
 // 4 complex64 SIMT FP32 128x64.
 template <class T>
 static int measure_ceiling_impl(Handle &h, int kernel, int m, int k, int nb, int reps, double *tflops) {
@@ -2753,7 +2863,7 @@ static int measure_ceiling_impl(Handle &h, int kernel, int m, int k, int nb, int
   std::vector<int> vld(1, ld);
   std::vector<int64_t> voff(1, 0);
   std::vector<GemmTask> tasks;
-  if (kernel == 0)
+  if (kernel == 0 || kernel == 5)
     add_tiles(tasks, kSquare64, 0, k, m, k, m, 0, k);
   else
     add_tiles(tasks, kSquare, 0, k, m, k, m, 0, k);
@@ -2809,6 +2919,8 @@ static int measure_ceiling_impl(Handle &h, int kernel, int m, int k, int nb, int
     if constexpr (sizeof(T) == 8) {
       if (kernel == 0)
         front_dmma_kernel<2, 2><<<dim3(nt, nb), 128, 0, h.stream>>>(a, tk);
+      else if (kernel == 5)
+        front_dmma3_kernel<<<dim3(nt, nb), 128, 0, h.stream>>>(a, tk);
       else
         front_gemm_kernel<T, kSquare><<<dim3(nt, nb), 256, 0, h.stream>>>(a, tk);
     } else {
@@ -2853,7 +2965,7 @@ static int measure_ceiling_impl(Handle &h, int kernel, int m, int k, int nb, int
 }
 
 int measure_ceiling(Handle &h, int kernel, int m, int k, int nb, int reps, double *tflops) {
-  if (kernel <= 1) return measure_ceiling_impl<double>(h, kernel, m, k, nb, reps, tflops);
+  if (kernel <= 1 || kernel == 5) return measure_ceiling_impl<double>(h, kernel, m, k, nb, reps, tflops);
   return measure_ceiling_impl<float>(h, kernel, m, k, nb, reps, tflops);
 }
 

@@ -19,7 +19,7 @@ def bench():
 
 
 def test_fp64_kernel_name_lists_the_picked_tiles(bench):
-    s = dict(schur_tile_simt128=1.0, schur_tile_simt64=0.0, schur_tile_dmma=13.0)
+    s = dict(schur_candidate0=1.0, schur_candidate1=0.0, schur_candidate2=13.0)
     name = bench.schur_kernel_name(s, 'fp64')
     assert 'front_dmma_kernel<2,2> (FP64 DMMA 64x64) on 13 levels' in name
     assert 'SIMT 128x64 on 1 levels' in name
@@ -27,7 +27,7 @@ def test_fp64_kernel_name_lists_the_picked_tiles(bench):
 
 
 def test_mixed_kernel_name_lists_the_picked_tiles(bench):
-    s = dict(schur_tile_simt128=5.0, schur_tile_simt64=1.0, schur_tile_dmma=7.0)
+    s = dict(schur_candidate0=5.0, schur_candidate1=1.0, schur_candidate2=7.0)
     name = bench.schur_kernel_name(s, 'mixed')
     assert 'tc::tma_gemm_kernel<128,2>' in name and 'on 5 levels' in name
     assert 'tc::tma_gemm_kernel<64,3>' in name and 'on 1 levels' in name
@@ -51,10 +51,10 @@ class _FakeEngine:
 def test_rooflines_fp64_entries(bench):
     from types import SimpleNamespace
     c = SimpleNamespace(name='me1_64x256', mesh=SimpleNamespace(ne=2, N=6))
-    s = dict(schur_launches=2.0, schur_gemm_flops=4e12, solve_ms=10.0, schur_tile_dmma=14.0)
+    s = dict(schur_launches=2.0, schur_gemm_flops=4e12, solve_ms=10.0, schur_candidate2=14.0)
     st0 = dict(n_active=100.0, nnz_lu=1e6, element_kernel_ms=1.0, scatter_kernel_ms=1.0)
     roof = bench.rooflines(_FakeEngine(), c, s, st0, 'fp64', [100.0], 4, dict(hbm_gbs=6500.0), 'measured',
-                           {'fp64_dmma': 40.0})
+                           {'fp64_dmma': 34.0, 'fp64_dmma_3m': 40.0})
     assert [r['bound'] for r in roof] == ['tensor', 'hbm', 'hbm']
     # 2 TFLOP per launch in 50 ms = 40 TFLOP/s = the measured ceiling
     assert roof[0]['achieved'] == pytest.approx(40.0) and roof[0]['frac'] == pytest.approx(1.0)
@@ -69,7 +69,7 @@ def test_rooflines_fp64_entries(bench):
 def test_rooflines_mixed_peak_is_tf32(bench):
     from types import SimpleNamespace
     c = SimpleNamespace(name='hex_8x4x48', hexas=[[0] * 27] * 3, N=10)
-    s = dict(schur_launches=1.0, schur_gemm_flops=1e12, solve_ms=0.0, schur_tile_simt128=1.0)
+    s = dict(schur_launches=1.0, schur_gemm_flops=1e12, solve_ms=0.0, schur_candidate0=1.0)
     st0 = dict(n_active=100.0, nnz_lu=1e6, element_kernel_ms=0.0, scatter_kernel_ms=0.0)
     roof = bench.rooflines(_FakeEngine(), c, s, st0, 'mixed', [10.0], 4, dict(bf16_tflops=1600.0), 'measured', {})
     assert len(roof) == 1 and roof[0]['peak'] == 800.0 and roof[0]['traffic'] is None

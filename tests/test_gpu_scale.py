@@ -72,12 +72,14 @@ def test_mixed_matches_fp64(mid):
         assert d[key] is None or abs(d[key]) <= 1e-3
 
 
-@pytest.mark.parametrize('tile', [1, 2])
+@pytest.mark.parametrize('tile', [0, 1, 2])
 def test_every_schur_tile_candidate_is_exact(mid, tile, monkeypatch):
-    """The autotuner's candidates (SIMT 128x64 / 64x64, FP64 tensor-core DMMA 64x64;
-    SS_SCHUR_TILE=2 also puts the panel-step GEMMs on DMMA tiles), each forced on
-    every level, give the same charges as the default choice."""
-    case, _, g = mid
+    """The autotuner's FP64 candidates (SIMT 128x64; FP64 tensor-core DMMA 64x64 with
+    three or four real products per complex block; SS_SCHUR_TILE=2 also puts the
+    panel-step GEMMs on DMMA tiles), each forced on every level, give the same
+    charges as the default choice, and each solution has a backward error below
+    1e-12 in the oracle's system."""
+    case, o, g = mid
     f = np.linspace(case.freqs[0], case.freqs[-1], 5)
     Q0, _, _ = g.charges(2 * np.pi * f, 1.0, 'fp64')
     monkeypatch.setenv('SS_SCHUR_TILE', str(tile))
@@ -85,12 +87,16 @@ def test_every_schur_tile_candidate_is_exact(mid, tile, monkeypatch):
     try:
         Q, st, _ = e.charges(2 * np.pi * f, 1.0, 'fp64')
         s = e.stats()
+        w = 2 * np.pi * f[2]
+        A, rhs = o.system(w)
+        disp, _, _ = e.solve(w)
     finally:
         e.close()
     assert (st == 0).all()
-    counts = [s['schur_tile_simt128'], s['schur_tile_simt64'], s['schur_tile_dmma']]
+    counts = [s['schur_candidate0'], s['schur_candidate1'], s['schur_candidate2']]
     assert counts[tile] > 0 and sum(counts) == counts[tile]
     assert s['panel_gemm_dmma'] == (1.0 if tile == 2 else 0.0)
+    assert _backward_error(A, disp[o.active], rhs) < 1e-12
     assert np.max(np.abs(Q - Q0) / np.abs(Q0)) < 1e-9
 
 
@@ -111,7 +117,7 @@ def test_every_complex64_schur_candidate_converges(mid, tile, monkeypatch):
     finally:
         e.close()
     assert (st == 0).all() and s['fp64_resolved'] == 0      # converged in mixed precision
-    counts = [s['schur_tile_simt128'], s['schur_tile_simt64'], s['schur_tile_dmma']]
+    counts = [s['schur_candidate0'], s['schur_candidate1'], s['schur_candidate2']]
     # levels whose fronts would be mostly padding in 128-row tensor-core tiles
     # always run the SIMT tiles
     if tile < 2:
