@@ -939,9 +939,12 @@ __global__ void __launch_bounds__(128, 3) front_dmma_kernel(FrontArgs<double> a,
 // count is unchanged (8 per complex multiply-add).  Normwise the product is as
 // stable as the four-product form; the imaginary part's error is bounded by
 // u (|Ar| + |Ai|)(|Br| + |Bi|) per term instead of u (|Ar||Bi| + |Ai||Br|).
-// Three accumulator sets (96 doubles per thread): two CTAs per SM.
+// Three accumulator sets (96 doubles per thread): two CTAs per SM.  WM x WN warps
+// of 32x32 complex, as front_dmma_kernel (2x2 Schur tiles, 4x1 / 1x4 panel steps).
+template <int WM, int WN>
 __global__ void __launch_bounds__(128, 2) front_dmma3_kernel(FrontArgs<double> a, const GemmTask *__restrict__ tasks) {
-  constexpr int kDmmaBM = 64, kDmmaBN = 64, kDmmaBS = kDmmaBN + 2;
+  constexpr int kDmmaBM = 32 * WM, kDmmaBN = 32 * WN, kDmmaBS = kDmmaBN + 2;
+  static_assert(WM * WN == 4, "four warps");
   __shared__ __align__(16) cd As[2][kDmmaBM * kDmmaAS];
   __shared__ __align__(16) cd Bs[2][kDmmaBK * kDmmaBS];
   const GemmTask tk = tasks[blockIdx.x];
@@ -949,7 +952,7 @@ __global__ void __launch_bounds__(128, 2) front_dmma3_kernel(FrontArgs<double> a
   const int ld = a.ld[tk.f];
   cd *F = a.arena + (int64_t)fq * a.stride + a.off[tk.f];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int wm = wid / 2, wn = wid % 2;          // warp tile origin (32 x 32 complex)
+  const int wm = wid / WN, wn = wid % WN;       // warp tile origin (32 x 32 complex)
   const int g = lane >> 2, t = lane & 3;
   double p1[4][4][2], p2[4][4][2], p3[4][4][2];
 #pragma unroll
@@ -1539,8 +1542,9 @@ struct Plan {
   // first factorisation, so that every sweep of the plan runs the same tiles
   std::vector<int64_t> schur_ptr_b;
   std::vector<int64_t> step_ptr_d;         // panel-step tasks in DMMA tiles (same indexing as step_ptr)
-  bool panel_dmma = false;                 // panel-step GEMMs on DMMA (tuned once per plan)
-  float panel_ms[2] = {0, 0};              // tuner's panel-GEMM times: SIMT, DMMA
+  int panel_dmma = 0;                      // panel-step GEMMs: 0 SIMT, 1 DMMA, 2 DMMA with three
+                                           // real products per complex block (tuned once per plan)
+  float panel_ms[3] = {0, 0, 0};           // tuner's panel-GEMM times: SIMT, DMMA, DMMA 3M
   std::vector<char> pick;                  // per level candidate
   std::vector<float> tune_ms;              // [candidate][level] measured times
   bool tuned = true;
@@ -2025,10 +2029,18 @@ struct Sweeper {
       if (P.panel_dmma) {
         const int64_t t0 = P.step_ptr_d[q + which], t1 = P.step_ptr_d[q + which + 1];
         if (t1 == t0) return;
-        if (which == 0)
-          front_dmma_kernel<4, 1><<<dim3((unsigned)(t1 - t0), nb), 128, 0, h.stream>>>(b, tasks + t0);
-        else
-          front_dmma_kernel<1, 4><<<dim3((unsigned)(t1 - t0), nb), 128, 0, h.stream>>>(b, tasks + t0);
+        const dim3 grid((unsigned)(t1 - t0), nb);
+        if (P.panel_dmma == 2) {
+          if (which == 0)
+            front_dmma3_kernel<4, 1><<<grid, 128, 0, h.stream>>>(b, tasks + t0);
+          else
+            front_dmma3_kernel<1, 4><<<grid, 128, 0, h.stream>>>(b, tasks + t0);
+        } else {
+          if (which == 0)
+            front_dmma_kernel<4, 1><<<grid, 128, 0, h.stream>>>(b, tasks + t0);
+          else
+            front_dmma_kernel<1, 4><<<grid, 128, 0, h.stream>>>(b, tasks + t0);
+        }
         return;
       }
     }
@@ -2080,7 +2092,7 @@ struct Sweeper {
     const int64_t t0 = P.schur_ptr_b[l], t1 = P.schur_ptr_b[l + 1];
     if constexpr (sizeof(T) == 8) {
       if (c == 1)
-        front_dmma3_kernel<<<dim3((unsigned)(t1 - t0), nb), 128, 0, h.stream>>>(b, tasks + t0);
+        front_dmma3_kernel<2, 2><<<dim3((unsigned)(t1 - t0), nb), 128, 0, h.stream>>>(b, tasks + t0);
       else
         front_dmma_kernel<2, 2><<<dim3((unsigned)(t1 - t0), nb), 128, 0, h.stream>>>(b, tasks + t0);
     }
@@ -2116,12 +2128,13 @@ struct Sweeper {
         }
       for (auto &x : e) cudaEventDestroy(x);
       if constexpr (sizeof(T) == 8) {
-      // panel-step GEMMs (FP64): all of them once with SIMT tiles, once with DMMA tiles
-      cudaEvent_t pe[4];
+      // panel-step GEMMs (FP64): all of them once with SIMT tiles, once with DMMA
+      // tiles, once with DMMA tiles of three real products per complex block
+      cudaEvent_t pe[6];
       for (auto &x : pe) SS_CK(cudaEventCreate(&x));
-      float pt[2] = {0, 0};
-      for (int c = 0; c < 2; ++c) {
-        P.panel_dmma = c == 1;
+      float pt[3] = {0, 0, 0};
+      for (int c = 0; c < 3; ++c) {
+        P.panel_dmma = c;
         cudaEventRecord(pe[2 * c], h.stream);
         for (int l = 0; l < S.nlevel; ++l) {
           FrontArgs<T> b = a;
@@ -2136,14 +2149,16 @@ struct Sweeper {
       }
       SS_CK(cudaGetLastError());
       SS_CK(cudaStreamSynchronize(h.stream));
-      for (int c = 0; c < 2; ++c) cudaEventElapsedTime(&pt[c], pe[2 * c], pe[2 * c + 1]);
+      for (int c = 0; c < 3; ++c) cudaEventElapsedTime(&pt[c], pe[2 * c], pe[2 * c + 1]);
       for (auto &x : pe) cudaEventDestroy(x);
-      P.panel_dmma = pt[1] < pt[0];
-      P.panel_ms[0] = pt[0];
-      P.panel_ms[1] = pt[1];
+      P.panel_dmma = 0;
+      for (int c = 1; c < 3; ++c)
+        if (pt[c] < pt[P.panel_dmma]) P.panel_dmma = c;
+      for (int c = 0; c < 3; ++c) P.panel_ms[c] = pt[c];
       }
     } else {
-      P.panel_dmma = sizeof(T) == 8 && atoi(force) == 2;
+      // a forced DMMA Schur tile puts the panel-step GEMMs on the same kind of tile
+      P.panel_dmma = sizeof(T) != 8 ? 0 : atoi(force) == 2 ? 1 : atoi(force) == 1 ? 2 : 0;
     }
     for (int l = 0; l < S.nlevel; ++l) {
       int best = 0;
@@ -2703,9 +2718,9 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
   h.st[31] = (double)steps_a;
   h.st[32] = nfail;
   h.st[20] = h.st[21] = h.st[22] = 0;
-  h.st[23] = P.panel_dmma ? 1.0 : 0.0;
+  h.st[23] = P.panel_dmma;
   h.st[24] = P.panel_ms[0];
-  h.st[25] = P.panel_ms[1];
+  h.st[25] = std::min(P.panel_ms[1], P.panel_ms[2]);
   h.st[26] = (double)P.fronts_small.size();
   h.st[27] = 0;
   for (float t : P.tune_ms) h.st[27] += t;
@@ -2920,7 +2935,7 @@ static int measure_ceiling_impl(Handle &h, int kernel, int m, int k, int nb, int
       if (kernel == 0)
         front_dmma_kernel<2, 2><<<dim3(nt, nb), 128, 0, h.stream>>>(a, tk);
       else if (kernel == 5)
-        front_dmma3_kernel<<<dim3(nt, nb), 128, 0, h.stream>>>(a, tk);
+        front_dmma3_kernel<2, 2><<<dim3(nt, nb), 128, 0, h.stream>>>(a, tk);
       else
         front_gemm_kernel<T, kSquare><<<dim3(nt, nb), 256, 0, h.stream>>>(a, tk);
     } else {
