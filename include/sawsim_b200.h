@@ -39,6 +39,7 @@ typedef struct ss_handle ss_handle;
 #define SS_Q9_ME0   0      /* plane strain [ux | uy | phi], 3 DOF/node           */
 #define SS_Q9_ME1   1      /* [ux | uy | uz | phi], 4 DOF/node                   */
 #define SS_HEX27    2      /* u interleaved 3n+c, phi at 3N+n                    */
+#define SS_MATRIX   3      /* assembled global matrices from ss_set_csr          */
 
 /* precision modes for ss_sweep */
 #define SS_PREC_FP64   0   /* complex128 fronts, FP64 throughout (the drop-in)   */
@@ -118,6 +119,37 @@ int ss_set_bc(ss_handle *h, int64_t gdof, int64_t n_fix, const int64_t *fix,
  * the reference rebuilds its engine for every sweep (agent.py:406-477 runs 2-9
  * of them per locate). */
 int ss_assemble(ss_handle *h);
+
+/*
+ * Assembled-matrix input, the alternative to ss_set_mesh + ss_assemble: the
+ * arguments of the reference engine's constructor,
+ *   src/sawsim/saw2d/sweep.py:283  FrequencySolver(K, M, fix, zheng, fu, merge_groups)
+ *   src/sawsim/saw2d/saw3d/bc_solve.py:108  FrequencySolver3D(K, M, boundary, t_fb, t_lr)
+ * as a global pattern here, values by ss_set_values and the boundary sets by
+ * ss_set_bc.  The pattern is CSR over gdof rows with strictly ascending columns in
+ * each row; K, M (and D) share it (pass the union of their patterns).
+ *   dof_node : gdof node ids in [0, n_nodes), or NULL.  The DOFs of one node are
+ *              eliminated together; without it, DOFs whose condensed rows have
+ *              the same columns are grouped.
+ *   node_xyz : n_nodes x dim coordinates (dim 2 or 3), or NULL; needs dof_node.
+ *              With them the fill-reducing ordering is the geometric nested
+ *              dissection of the mesh path (the same ordering as ss_set_mesh on
+ *              the same mesh); without them a graph nested dissection (level-set
+ *              separators from a pseudo-peripheral node), which needs no geometry
+ *              but leaves more fill.
+ * Resets the mesh, the values and any analysis.
+ */
+int ss_set_csr(ss_handle *h, int64_t gdof, const int64_t *indptr, const int64_t *indices,
+               int64_t n_nodes, int dim, const int64_t *dof_node, const double *node_xyz);
+
+/*
+ * Values on the ss_set_csr pattern, complex interleaved (2 x nnz doubles):
+ * which = SS_MAT_K, SS_MAT_M or SS_MAT_D (the Rayleigh-damped part of K,
+ * sweep.py:316-323; ss_set_damping sets beta).  On an analysed handle only the
+ * condensed values are gathered again: the analysis, the factorisation plans and
+ * their autotuner picks are kept (a new PML freeze frequency, new damping).
+ */
+int ss_set_values(ss_handle *h, int which, const double *vals);
 
 /*
  * Copy a matrix to host.  Call with vals == NULL to get sizes in *nnz.

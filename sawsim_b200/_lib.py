@@ -14,7 +14,7 @@ import numpy as np
 LIB_PATH = Path(__file__).resolve().parent / 'libsawsim_b200.so'
 
 SS_OK, SS_EINVAL, SS_ECUDA, SS_ESINGULAR, SS_ENOCONV, SS_ETIMEOUT, SS_ENOMEM, SS_ESTATE = 0, -1, -2, -3, -4, -5, -6, -7
-SS_Q9_ME0, SS_Q9_ME1, SS_HEX27 = 0, 1, 2
+SS_Q9_ME0, SS_Q9_ME1, SS_HEX27, SS_MATRIX = 0, 1, 2, 3
 SS_PREC_FP64, SS_PREC_MIXED, SS_PREC_AUTO = 0, 1, 2
 SS_MAT_K, SS_MAT_M, SS_MAT_D, SS_MAT_KC, SS_MAT_MC = 0, 1, 2, 3, 4
 
@@ -38,6 +38,8 @@ SIGNATURES = [
     ('ss_set_bc', C.c_int, [_P, C.c_int64, C.c_int64, _I64P, C.c_int64, _I64P, C.c_int64, _I64P, C.c_int64,
                             _I64P, _I64P, C.c_int64]),
     ('ss_assemble', C.c_int, [_P]),
+    ('ss_set_csr', C.c_int, [_P, C.c_int64, _I64P, _I64P, C.c_int64, C.c_int, _I64P, _DP]),
+    ('ss_set_values', C.c_int, [_P, C.c_int, _DP]),
     ('ss_export_csr', C.c_int, [_P, C.c_int, _I64P, _I64P, _I64P, _I64P, _DP]),
     ('ss_analyze', C.c_int, [_P]),
     ('ss_set_damping', C.c_int, [_P, C.c_double]),

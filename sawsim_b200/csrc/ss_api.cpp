@@ -75,7 +75,7 @@ static void reset_derived(Handle &h) {
 extern "C" int ss_set_mesh(ss_handle *hp, int kind, int64_t n_nodes, const double *pos, int64_t n_elem,
                            const int64_t *conn, const int32_t *emat) {
   H_CHECK(hp);
-  if (kind < SS_Q9_ME0 || kind > SS_HEX27) return fail(h, SS_EINVAL, "unknown element kind");
+  if (kind < SS_Q9_ME0 || kind > SS_HEX27) return fail(h, SS_EINVAL, "unknown element kind (SS_MATRIX: ss_set_csr)");
   if (n_nodes <= 0 || n_elem <= 0 || !pos || !conn || !emat) return fail(h, SS_EINVAL, "empty mesh or null array");
   if (!all_finite(pos, n_nodes * (kind == SS_HEX27 ? 3 : 2))) return fail(h, SS_EINVAL, "non-finite coordinate");
   h.kind = kind;
@@ -85,6 +85,7 @@ extern "C" int ss_set_mesh(ss_handle *hp, int kind, int64_t n_nodes, const doubl
   h.N = n_nodes;
   h.ne = n_elem;
   h.pos.assign(pos, pos + n_nodes * h.dim);
+  h.dof_node.clear();
   h.conn.assign(conn, conn + n_elem * h.npe);
   h.emat.assign(emat, emat + n_elem);
   for (int64_t v : h.conn)
@@ -173,7 +174,7 @@ extern "C" int ss_set_bc(ss_handle *hp, int64_t gdof, int64_t n_fix, const int64
 
 extern "C" int ss_assemble(ss_handle *hp) {
   H_CHECK(hp);
-  if (h.kind < 0) return fail(h, SS_ESTATE, "assemble: no mesh");
+  if (h.kind < 0 || h.kind == SS_MATRIX) return fail(h, SS_ESTATE, "assemble: no mesh (matrix input takes ss_set_values)");
   if (h.nmat[0] <= 0) return fail(h, SS_ESTATE, "assemble: no materials");
   int mx = *std::max_element(h.emat.begin(), h.emat.end());
   if (mx >= h.nmat[0]) return fail(h, SS_EINVAL, "element material index >= number of materials");
@@ -207,6 +208,83 @@ extern "C" int ss_assemble(ss_handle *hp) {
   return SS_OK;
 }
 
+extern "C" int ss_set_csr(ss_handle *hp, int64_t gdof, const int64_t *indptr, const int64_t *indices,
+                          int64_t n_nodes, int dim, const int64_t *dof_node, const double *node_xyz) {
+  H_CHECK(hp);
+  if (gdof <= 0 || !indptr || !indices) return fail(h, SS_EINVAL, "csr: empty pattern or null array");
+  if (indptr[0] != 0) return fail(h, SS_EINVAL, "csr: indptr[0] must be 0");
+  for (int64_t r = 0; r < gdof; ++r) {
+    if (indptr[r + 1] < indptr[r]) return fail(h, SS_EINVAL, "csr: indptr not ascending");
+    for (int64_t s = indptr[r]; s < indptr[r + 1]; ++s) {
+      if (indices[s] < 0 || indices[s] >= gdof) return fail(h, SS_EINVAL, "csr: column out of range");
+      if (s > indptr[r] && indices[s] <= indices[s - 1])
+        return fail(h, SS_EINVAL, "csr: columns of a row not strictly ascending");
+    }
+  }
+  if (node_xyz && !dof_node) return fail(h, SS_EINVAL, "csr: node coordinates need dof_node");
+  if (dof_node) {
+    if (n_nodes <= 0) return fail(h, SS_EINVAL, "csr: n_nodes must be positive with dof_node");
+    for (int64_t d = 0; d < gdof; ++d)
+      if (dof_node[d] < 0 || dof_node[d] >= n_nodes) return fail(h, SS_EINVAL, "csr: dof_node out of range");
+  }
+  if (node_xyz && (dim < 2 || dim > 3)) return fail(h, SS_EINVAL, "csr: dim must be 2 or 3");
+  if (node_xyz && !all_finite(node_xyz, n_nodes * dim)) return fail(h, SS_EINVAL, "csr: non-finite coordinate");
+  reset_derived(h);
+  h.kind = SS_MATRIX;
+  h.npe = 0;
+  h.nc = 0;
+  h.ne = 0;
+  h.conn.clear();
+  h.emat.clear();
+  h.elem_region.clear();
+  h.npml = 0;
+  h.nmat[0] = h.nmat[1] = 0;
+  h.nadj_ptr.clear();
+  h.nadj.clear();
+  h.N = dof_node ? n_nodes : 0;
+  h.dim = node_xyz ? dim : 0;
+  h.pos.assign(node_xyz ? node_xyz : nullptr, node_xyz ? node_xyz + n_nodes * dim : nullptr);
+  h.dof_node.assign(dof_node ? dof_node : nullptr, dof_node ? dof_node + gdof : nullptr);
+  h.gdof = gdof;
+  h.indptr.assign(indptr, indptr + gdof + 1);
+  h.nnz = h.indptr[gdof];
+  h.indices.assign(indices, indices + h.nnz);
+  h.have_K = h.have_M = h.have_D = false;
+  h.have_bc = false;
+  h.beta = 0;
+  return SS_OK;
+}
+
+extern "C" int ss_set_values(ss_handle *hp, int which, const double *vals) {
+  H_CHECK(hp);
+  if (h.kind != SS_MATRIX) return fail(h, SS_ESTATE, "set_values: no ss_set_csr pattern");
+  if (which != SS_MAT_K && which != SS_MAT_M && which != SS_MAT_D)
+    return fail(h, SS_EINVAL, "set_values: which must be K, M or D");
+  if (!vals) return fail(h, SS_EINVAL, "set_values: null array");
+  if (!all_finite(vals, 2 * h.nnz)) return fail(h, SS_EINVAL, "set_values: non-finite value");
+  DBuf &dst = which == SS_MAT_K ? h.dK : which == SS_MAT_M ? h.dM : h.dD;
+  cudaError_t e = dalloc(dst, (size_t)h.nnz * 16 + 16);
+  if (e != cudaSuccess) return cuda_fail(h, e, "set_values alloc");
+  e = cudaMemcpyAsync(dst.p, vals, (size_t)h.nnz * 16, cudaMemcpyHostToDevice, h.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h.stream);
+  if (e != cudaSuccess) return cuda_fail(h, e, "set_values copy");
+  const bool had_D = h.have_D;
+  (which == SS_MAT_K ? h.have_K : which == SS_MAT_M ? h.have_M : h.have_D) = true;
+  if (h.analyzed) {
+    // same pattern and boundary sets: keep the analysis and the plans, gather the
+    // condensed values again (as a value-only reassembly does)
+    if (h.have_D != had_D) free_plans(h);
+    int rc = gather_values(h);
+    if (rc) {
+      reset_derived(h);
+      return rc;
+    }
+    h.scale_w = -1;
+    h.auto_prec = -1;
+  }
+  return SS_OK;
+}
+
 extern "C" int ss_export_csr(ss_handle *hp, int which, int64_t *n_out, int64_t *nnz_out, int64_t *indptr,
                              int64_t *indices, double *vals) {
   H_CHECK(hp);
@@ -223,7 +301,7 @@ extern "C" int ss_export_csr(ss_handle *hp, int which, int64_t *n_out, int64_t *
     };
     std::vector<char> keep;
     int64_t nnz = h.nnz;
-    if (which == SS_MAT_M) {
+    if (which == SS_MAT_M && h.kind != SS_MATRIX) {
       keep.assign(h.nnz, 0);
       nnz = 0;
       for (int64_t r = 0; r < h.gdof; ++r)
@@ -299,7 +377,7 @@ extern "C" int ss_analyze(ss_handle *hp) {
 extern "C" int ss_set_damping(ss_handle *hp, double beta) {
   H_CHECK(hp);
   if (!std::isfinite(beta) || beta < 0.0) return fail(h, SS_EINVAL, "damping: beta must be finite and >= 0");
-  if (beta != 0.0 && !h.have_D) return fail(h, SS_ESTATE, "damping: assemble D first (damping materials)");
+  if (beta != 0.0 && !h.have_D) return fail(h, SS_ESTATE, "damping: assemble D first (damping materials, or ss_set_values)");
   h.beta = beta;
   h.scale_w = -1;
   free_plans(h);   // the captured launch graphs bake beta and the damping matrix in
@@ -405,6 +483,7 @@ extern "C" int ss_adjoint_gradient(ss_handle *hp, int n_f, const double *omega, 
                                    const double *douter, double *Q, double *dQ, int *status) {
   H_CHECK(hp);
   if (!h.analyzed) return fail(h, SS_ESTATE, "gradient: analyze first");
+  if (h.kind == SS_MATRIX) return fail(h, SS_ESTATE, "gradient: the element derivatives need a mesh (ss_set_mesh)");
   if (n_f <= 0 || !omega || !Q || !dQ || n_params <= 0) return fail(h, SS_EINVAL, "gradient: bad arguments");
   if (precision != SS_PREC_FP64 && precision != SS_PREC_MIXED && precision != SS_PREC_AUTO)
     return fail(h, SS_EINVAL, "gradient: bad precision");

@@ -85,6 +85,7 @@ struct Handle {
   std::vector<double> pos;
   std::vector<int64_t> conn;
   std::vector<int32_t> emat;
+  std::vector<int64_t> dof_node;         // SS_MATRIX: node of each global DOF (empty: none given)
   // materials (per which: 0 K/M, 1 D)
   int nmat[2] = {0, 0};
   std::vector<double> rho[2], C[2], e[2], eps[2];

@@ -24,6 +24,7 @@ static inline int64_t dof_of(const Handle &h, int64_t node, int c) {
   return (int64_t)c * h.N + node;
 }
 static inline int64_t node_of_dof(const Handle &h, int64_t d) {
+  if (h.kind == SS_MATRIX) return h.dof_node[d];
   if (h.kind == SS_HEX27) return d < 3 * h.N ? d / 3 : d - 3 * h.N;
   return d % h.N;
 }
@@ -242,15 +243,57 @@ int build_condensation(Handle &h) {
     h.vg_ptr[n + P + 1] = (int64_t)h.vg_src.size();
   }
   // supervariables: active DOFs of one mesh node
-  std::vector<int64_t> sv_of_node(h.N, -1);
   h.sv_of_act.resize(n);
   h.sv_xyz.clear();
   h.nsv = 0;
+  if (h.kind == SS_MATRIX && h.dof_node.empty()) {
+    // no node map: active DOFs whose condensed rows hold the same columns
+    // (indistinguishable in the elimination) form one supervariable
+    std::vector<uint64_t> hv(n);
+    for (int64_t P = 0; P < n; ++P) {
+      uint64_t x = 1469598103934665603ull ^ (uint64_t)(h.a_ptr[P + 1] - h.a_ptr[P]);
+      for (int64_t t = h.a_ptr[P]; t < h.a_ptr[P + 1]; ++t) x = (x ^ (uint64_t)h.a_idx[t]) * 1099511628211ull;
+      hv[P] = x;
+    }
+    std::vector<int64_t> by(n);
+    std::iota(by.begin(), by.end(), 0);
+    std::sort(by.begin(), by.end(), [&](int64_t a, int64_t b) { return hv[a] != hv[b] ? hv[a] < hv[b] : a < b; });
+    auto same = [&](int64_t a, int64_t b) {
+      return hv[a] == hv[b] && h.a_ptr[a + 1] - h.a_ptr[a] == h.a_ptr[b + 1] - h.a_ptr[b] &&
+             std::equal(h.a_idx.begin() + h.a_ptr[a], h.a_idx.begin() + h.a_ptr[a + 1], h.a_idx.begin() + h.a_ptr[b]);
+    };
+    // group leader = the smallest P of its group; ids in ascending leader order
+    std::vector<int64_t> lead(n);
+    for (int64_t i = 0; i < n;) {
+      int64_t j = i;
+      while (j < n && hv[by[j]] == hv[by[i]]) ++j;
+      // within one hash bucket, match each DOF against the bucket's earlier leaders
+      std::vector<int64_t> leaders;
+      for (int64_t t = i; t < j; ++t) {
+        const int64_t P = by[t];
+        int64_t L = -1;
+        for (int64_t q : leaders)
+          if (same(q, P)) { L = q; break; }
+        if (L < 0) leaders.push_back(L = P);
+        lead[P] = L;
+      }
+      i = j;
+    }
+    std::vector<int64_t> sv_of_lead(n, -1);
+    for (int64_t P = 0; P < n; ++P) {
+      const int64_t L = lead[P];
+      if (sv_of_lead[L] < 0) sv_of_lead[L] = h.nsv++;
+      h.sv_of_act[P] = sv_of_lead[L];
+    }
+    return SS_OK;
+  }
+  std::vector<int64_t> sv_of_node(h.N, -1);
   for (int64_t P = 0; P < n; ++P) {
     const int64_t nd = node_of_dof(h, h.active[P]);
     if (sv_of_node[nd] < 0) {
       sv_of_node[nd] = h.nsv++;
-      for (int c = 0; c < 3; ++c) h.sv_xyz.push_back(c < h.dim ? h.pos[nd * h.dim + c] : 0.0);
+      if (!h.pos.empty())
+        for (int c = 0; c < 3; ++c) h.sv_xyz.push_back(c < h.dim ? h.pos[nd * h.dim + c] : 0.0);
     }
     h.sv_of_act[P] = sv_of_node[nd];
   }
@@ -268,6 +311,11 @@ namespace ss {
 // around the median on every axis are scored by |S| / balance, so a Bloch
 // cylinder is cut into rings before it is cut lengthwise.  The separator tree is
 // the assembly tree: leaves are whole subdomains, interior fronts separators.
+// Without coordinates (assembled-matrix input) the cut is a breadth-first level
+// set from a pseudo-peripheral supervariable (George and Liu's level structure),
+// chosen among the levels that leave at least a quarter of the set on each side
+// by the same |S| / balance score and trimmed to its vertices that touch the next
+// level.
 // ------------------------------------------------------------------------------
 struct ND {
   const std::vector<int64_t> &ap, &aj;   // supervariable adjacency
@@ -276,12 +324,103 @@ struct ND {
   int leaf;
   std::vector<int64_t> stamp, side;
   int64_t tick = 0;
+  std::vector<int64_t> vis, lvl;         // breadth-first search marks and levels
+  int64_t vtick = 0;
   std::vector<std::vector<int64_t>> piv;  // pivots (supervariables) per front
   std::vector<std::vector<int>> kids;
 
   ND(const std::vector<int64_t> &p, const std::vector<int64_t> &j, const std::vector<double> &x, int d, int lf,
      int64_t n)
-      : ap(p), aj(j), xyz(x), dim(d), leaf(lf), stamp(n, -1), side(n, 0) {}
+      : ap(p), aj(j), xyz(x), dim(d), leaf(lf), stamp(n, -1), side(n, 0), vis(n, -1), lvl(n, 0) {}
+
+  // breadth-first levels of the set stamped t from root: level l is
+  // order[lptr[l] .. lptr[l+1]); returns the number of levels
+  int64_t bfs(int64_t root, int64_t t, std::vector<int64_t> &order, std::vector<int64_t> &lptr) {
+    const int64_t mark = ++vtick;
+    order.clear();
+    lptr.assign(1, 0);
+    order.push_back(root);
+    vis[root] = mark;
+    lvl[root] = 0;
+    int64_t cur = 0;
+    for (size_t head = 0; head < order.size(); ++head) {
+      const int64_t v = order[head];
+      if (lvl[v] != cur) {
+        lptr.push_back((int64_t)head);
+        cur = lvl[v];
+      }
+      for (int64_t q = ap[v]; q < ap[v + 1]; ++q) {
+        const int64_t w = aj[q];
+        if (stamp[w] == t && vis[w] != mark) {
+          vis[w] = mark;
+          lvl[w] = lvl[v] + 1;
+          order.push_back(w);
+        }
+      }
+    }
+    lptr.push_back((int64_t)order.size());
+    return (int64_t)lptr.size() - 1;
+  }
+
+  // level-set separator of a connected set stamped t (no coordinates)
+  std::vector<int64_t> graph_separator(const std::vector<int64_t> &nodes, int64_t t) {
+    const int64_t nn = (int64_t)nodes.size();
+    auto deg = [&](int64_t v) { return ap[v + 1] - ap[v]; };
+    int64_t r = nodes[0];
+    for (int64_t v : nodes)
+      if (deg(v) < deg(r)) r = v;
+    std::vector<int64_t> order, lptr;
+    int64_t nl = bfs(r, t, order, lptr);
+    for (int it = 0; it < 8; ++it) {   // pseudo-peripheral root
+      int64_t c = order[lptr[nl - 1]];
+      for (int64_t i = lptr[nl - 1]; i < lptr[nl]; ++i)
+        if (deg(order[i]) < deg(c)) c = order[i];
+      std::vector<int64_t> o2, l2;
+      const int64_t n2 = bfs(c, t, o2, l2);
+      if (n2 <= nl) break;
+      order.swap(o2);
+      lptr.swap(l2);
+      nl = n2;
+      r = c;
+    }
+    if (nl < 3) return nodes;
+    nl = bfs(r, t, order, lptr);   // the levels (and marks) of the kept root
+    const int64_t mark = vtick;
+    // per level: its vertices with a neighbour in the next level
+    std::vector<int64_t> touch(nl, 0);
+    std::vector<char> keep(order.size(), 0);
+    for (int64_t l = 0; l + 1 < nl; ++l)
+      for (int64_t i = lptr[l]; i < lptr[l + 1]; ++i) {
+        const int64_t v = order[i];
+        for (int64_t q = ap[v]; q < ap[v + 1]; ++q) {
+          const int64_t w = aj[q];
+          if (stamp[w] == t && vis[w] == mark && lvl[w] == l + 1) {
+            keep[i] = 1;
+            ++touch[l];
+            break;
+          }
+        }
+      }
+    double best = 1e300;
+    int64_t bl = -1;
+    for (int64_t l = 1; l + 1 < nl; ++l) {
+      const int64_t before = lptr[l + 1] - touch[l], after = nn - lptr[l + 1];
+      if (touch[l] == 0 || before <= 0 || after <= 0) continue;
+      const double bal = (double)std::min(before, after) / (double)nn;
+      if (bal < 0.25) continue;
+      const double score = (double)touch[l] / bal;
+      if (score < best) best = score, bl = l;
+    }
+    if (bl < 0) {   // no balanced level: the one holding the median vertex
+      bl = std::min<int64_t>(std::max<int64_t>(lvl[order[nn / 2]], 1), nl - 2);
+      if (touch[bl] == 0) return nodes;
+    }
+    std::vector<int64_t> S;
+    for (int64_t i = lptr[bl]; i < lptr[bl + 1]; ++i)
+      if (keep[i]) S.push_back(order[i]);
+    std::sort(S.begin(), S.end());
+    return S;
+  }
 
   void components(const std::vector<int64_t> &nodes, std::vector<std::vector<int64_t>> &out) {
     const int64_t t = ++tick;
@@ -315,6 +454,7 @@ struct ND {
     const int64_t nn = (int64_t)nodes.size();
     const int64_t t = ++tick;
     for (int64_t v : nodes) stamp[v] = t;
+    if (xyz.empty()) return graph_separator(nodes, t);
     double best = 1e300;
     std::vector<int64_t> bestS;
     std::vector<int64_t> key(nn);
@@ -423,7 +563,10 @@ int build_symbolic(Handle &h) {
   for (int64_t v = 0; v < nsv; ++v) std::copy(sadj[v].begin(), sadj[v].end(), aj.begin() + ap[v]);
   sadj.clear();
 
+  // leaf subdomain size: 12 supervariables in 2D, 8 in 3D (without coordinates,
+  // 3D is told apart by the mean supervariable degree: ~20 for Q9, ~60 for Hex27)
   int leaf = h.dim == 3 ? 8 : 12;
+  if (h.dim == 0 && nsv > 0 && (double)ap[nsv] / (double)nsv > 40.0) leaf = 8;
   if (const char *e = getenv("SS_ND_LEAF")) leaf = std::max(1, atoi(e));
   ND nd(ap, aj, h.sv_xyz, h.dim, leaf, nsv);
   std::vector<int64_t> all(nsv);

@@ -3,11 +3,13 @@
 ``FrequencySolver`` mirrors the engine the reference's pipeline builds and
 drives (``src/sawsim/saw2d/sweep.py:275-393``): ``solve(omega, V)`` returns
 ``(disp, Q, |Y|)``, ``sweep(freqs, V)`` the charges, ``n_active`` the size of the
-condensed system.  Construction goes from the inputs of the reference's
+condensed system.  Construction goes either from the inputs of the reference's
 assembly (``piezo_fem.assemble``, ``piezo_fem.py:283``) and boundary builder
-(``sweep.bc_periodic``, ``sweep.py:41``), because assembly, condensation and
-every frequency's factorisation run on the GPU.  All numerical work is done by
-``libsawsim_b200.so``; there is no CPU path.
+(``sweep.bc_periodic``, ``sweep.py:41``), so that assembly, condensation and
+every frequency's factorisation run on the GPU (``from_q9``, ``from_hex27``), or
+from the reference engine's own constructor arguments, the assembled K and M and
+the boundary sets (``from_matrices``, ``from_matrices_3d``).  All numerical work
+is done by ``libsawsim_b200.so``; there is no CPU path.
 """
 from __future__ import annotations
 
@@ -76,6 +78,52 @@ def _bc_arrays(bc):
     gptr[1:] = np.cumsum([g.size for g in groups])
     gd = np.concatenate(groups) if groups else np.zeros(0, dtype=np.int64)
     return L.i64(fix), L.i64(zheng), L.i64(fu), L.i64(gptr), L.i64(gd)
+
+
+def _canonical(A, n):
+    """Complex CSR with sorted columns and duplicates summed (explicit zeros kept,
+    as the reference's COO -> CSR assembly keeps them)."""
+    A = sp.csr_matrix(A, dtype=np.complex128, copy=True)
+    if A.shape != (n, n):
+        raise ValueError(f'matrix shape {A.shape} != ({n}, {n})')
+    A.sum_duplicates()
+    return A
+
+
+def _keys(A):
+    rows = np.repeat(np.arange(A.shape[0], dtype=np.int64), np.diff(A.indptr))
+    return rows * A.shape[1] + A.indices.astype(np.int64)
+
+
+def _union_pattern(mats):
+    """CSR pattern (indptr, indices) holding every stored entry of ``mats``."""
+    n = mats[0].shape[0]
+    keys = np.unique(np.concatenate([_keys(A) for A in mats]))
+    rows = keys // n
+    indptr = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(np.bincount(rows, minlength=n), out=indptr[1:])
+    return indptr, (keys % n).astype(np.int64), keys
+
+
+def _on_pattern(A, keys):
+    """Values of canonical ``A`` scattered onto the pattern with sorted ``keys``."""
+    k = _keys(A)
+    pos = np.searchsorted(keys, k)
+    if k.size and (pos.max() >= keys.size or not np.array_equal(keys[np.minimum(pos, keys.size - 1)], k)):
+        raise ValueError('matrix has entries outside the engine\'s pattern')
+    v = np.zeros(keys.size, dtype=np.complex128)
+    v[pos] = A.data
+    return v
+
+
+def _fold_pairs(T):
+    """(slave, master) pairs of a fold operator (bc_solve.py:25-33: row ``slave``
+    holds a single 1 in column ``master``; other rows are identity rows)."""
+    T = sp.csr_matrix(T)
+    rows = np.repeat(np.arange(T.shape[0], dtype=np.int64), np.diff(T.indptr))
+    cols = T.indices.astype(np.int64)
+    off = rows != cols
+    return rows[off], cols[off]
 
 
 class FrequencySolver:
@@ -149,6 +197,79 @@ class FrequencySolver:
         eng.omega_top = float(omega_top)
         eng._set_bc((fix, zheng, fu, groups), two_stage=two_stage)
         return eng
+
+    @classmethod
+    def from_matrices(cls, K, M, fix, zheng, fu, merge_groups, dof_node=None, node_xyz=None, device=0):
+        """The reference engine's constructor, ``sweep.FrequencySolver(K, M, fix,
+        zheng, fu, merge_groups)`` (sweep.py:283-314): assembled global K and M
+        (any mesh, e.g. the Gmsh-meshed templates), the fixed DOFs, the electrode
+        DOFs and the periodic merge groups.  Fold, condensation, analysis and every
+        frequency's factorisation run on the GPU.  Optional ``dof_node`` (node of
+        each DOF) and ``node_xyz`` (node coordinates, n_nodes x 2 or 3) give the
+        geometric nested dissection of the mesh path; without them the ordering
+        is a graph nested dissection of the matrix (more fill)."""
+        return cls._from_csr(K, M, (fix, zheng, fu, merge_groups), 0, dof_node, node_xyz, device)
+
+    @classmethod
+    def from_matrices_3d(cls, K, M, boundary, t_fb, t_lr, dof_node=None, node_xyz=None, device=0):
+        """``FrequencySolver3D(K, M, boundary, t_fb, t_lr)`` (bc_solve.py:108-136):
+        the unfolded K and M, the boundary DOF container (an object with the
+        ``machine`` / ``electric`` dicts of boundary.py:84-148, or the pair of
+        dicts) and the two fold operators of ``build_periodic_operators``
+        (front/back first, then left/right)."""
+        s_fb, m_fb = _fold_pairs(t_fb)
+        s_lr, m_lr = _fold_pairs(t_lr)
+        groups = [[m, s] for s, m in zip(s_fb, m_fb)] + [[m, s] for s, m in zip(s_lr, m_lr)]
+        mach, elec = (boundary.machine, boundary.electric) if hasattr(boundary, 'machine') else boundary
+        bc = (np.asarray(mach['fix'], dtype=np.int64), elec['zheng'], elec['fu'], groups)
+        return cls._from_csr(K, M, bc, len(s_fb), dof_node, node_xyz, device)
+
+    @classmethod
+    def _from_csr(cls, K, M, bc, two_stage, dof_node, node_xyz, device):
+        n = K.shape[0]
+        Kc, Mc = _canonical(K, n), _canonical(M, n)
+        indptr, indices, keys = _union_pattern([Kc, Mc])
+        h = Handle(device)
+        dn = None if dof_node is None else L.i64(dof_node)
+        xyz = None if node_xyz is None else L.f64(node_xyz)
+        if dn is not None and dn.size != n:
+            raise ValueError('dof_node needs one node id per DOF')
+        n_nodes = 0 if dn is None else int(dn.max()) + 1 if xyz is None else xyz.shape[0]
+        dim = 0 if xyz is None else xyz.shape[1]
+        h('ss_set_csr', n, L.ptr(indptr, C.c_int64), L.ptr(indices, C.c_int64), n_nodes, dim,
+          None if dn is None else L.ptr(dn, C.c_int64), None if xyz is None else L.ptr(xyz, C.c_double))
+        for which, A in ((L.SS_MAT_K, Kc), (L.SS_MAT_M, Mc)):
+            v = L.cplx(_on_pattern(A, keys))
+            h('ss_set_values', which, L.ptr(v, C.c_double))
+        eng = cls(h, n, 0, L.SS_MATRIX, bc[1], bc[2])
+        eng._keys = keys
+        eng._set_bc(bc, two_stage=two_stage)
+        return eng
+
+    def update_matrices(self, K=None, M=None):
+        """New K and/or M values on the engine's pattern (e.g. reassembled with the
+        PML frozen at a new top frequency): the analysis, the factorisation plans and
+        their autotuner picks are kept."""
+        self._matrix_only('update_matrices')
+        for which, A in ((L.SS_MAT_K, K), (L.SS_MAT_M, M)):
+            if A is not None:
+                v = L.cplx(_on_pattern(_canonical(A, self.gdof), self._keys))
+                self._h('ss_set_values', which, L.ptr(v, C.c_double))
+
+    def set_damping(self, D=None, beta: float = 0.0):
+        """Rayleigh stiffness damping A = K + i w beta D - w^2 M (sweep.py:316-323).
+        Matrix engines take D itself (the damped part of K, on the engine's
+        pattern); mesh engines assemble D from their damping materials and take
+        ``beta`` only."""
+        if D is not None:
+            self._matrix_only('set_damping(D)')
+            v = L.cplx(_on_pattern(_canonical(D, self.gdof), self._keys))
+            self._h('ss_set_values', L.SS_MAT_D, L.ptr(v, C.c_double))
+        self._h('ss_set_damping', float(beta))
+
+    def _matrix_only(self, what):
+        if self.kind != L.SS_MATRIX:
+            raise ValueError(f'{what}: the engine was built from a mesh; it assembles its own matrices')
 
     def _set_bc(self, bc, two_stage=0):
         fix, zheng, fu, gptr, gd = _bc_arrays(bc)

@@ -133,3 +133,45 @@ def test_auto_decision_kept_until_an_option_changes(small):
     g.charges(w, 1.0, 'auto')
     s = g.stats()
     assert s['auto_probe_ms'] > 0 and s['sweep_device_ms'] >= s['auto_probe_ms']
+
+
+def test_matrix_input_errors(built_lib):
+    """ss_set_csr / ss_set_values reject bad patterns and out-of-order calls; a
+    matrix handle has no mesh to assemble or differentiate."""
+    h = Handle(0)
+    try:
+        v = np.zeros(2 * 3)
+        assert _rc(h, 'ss_set_values', L.SS_MAT_K, L.ptr(v, C.c_double)) == L.SS_ESTATE     # no pattern yet
+        ip, ix = L.i64([0, 2, 3]), L.i64([1, 0, 1])                                          # row 0 not ascending
+        assert _rc(h, 'ss_set_csr', 2, L.ptr(ip, C.c_int64), L.ptr(ix, C.c_int64), 0, 0, None, None) == L.SS_EINVAL
+        ix = L.i64([0, 2, 1])                                                                 # column out of range
+        assert _rc(h, 'ss_set_csr', 2, L.ptr(ip, C.c_int64), L.ptr(ix, C.c_int64), 0, 0, None, None) == L.SS_EINVAL
+        ix = L.i64([0, 1, 1])
+        xyz = L.f64([[0.0, 0.0]])
+        assert _rc(h, 'ss_set_csr', 2, L.ptr(ip, C.c_int64), L.ptr(ix, C.c_int64), 1, 2, None,
+                   L.ptr(xyz, C.c_double)) == L.SS_EINVAL                                     # coordinates need dof_node
+        dn = L.i64([0, 1])
+        assert _rc(h, 'ss_set_csr', 2, L.ptr(ip, C.c_int64), L.ptr(ix, C.c_int64), 1, 0, L.ptr(dn, C.c_int64),
+                   None) == L.SS_EINVAL                                                       # node id out of range
+        assert _rc(h, 'ss_set_csr', 2, L.ptr(ip, C.c_int64), L.ptr(ix, C.c_int64), 0, 0, None, None) == L.SS_OK
+        assert _rc(h, 'ss_set_values', 7, L.ptr(v, C.c_double)) == L.SS_EINVAL
+        bad = np.array([1.0, 0.0, np.nan, 0.0, 1.0, 0.0])
+        assert _rc(h, 'ss_set_values', L.SS_MAT_K, L.ptr(bad, C.c_double)) == L.SS_EINVAL
+        assert _rc(h, 'ss_assemble') == L.SS_ESTATE
+        assert _rc(h, 'ss_analyze') == L.SS_ESTATE                                            # no values yet
+    finally:
+        h.close()
+    case = cases.make_case('me1_64x256', cols=8, rows=16, points=3)
+    g = cases.engine_for(case)
+    try:
+        e = FrequencySolver.from_matrices(g.export(L.SS_MAT_K), g.export(L.SS_MAT_M), *case.bc)
+        try:
+            with pytest.raises(L.SawsimError) as ex:
+                e.gradient(2 * np.pi * case.freqs[:1], [dict(drho=np.ones(2))])
+            assert ex.value.code == L.SS_ESTATE
+        finally:
+            e.close()
+        with pytest.raises(ValueError):
+            g.update_matrices(K=None)                       # a mesh engine assembles its own matrices
+    finally:
+        g.close()
