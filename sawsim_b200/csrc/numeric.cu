@@ -321,25 +321,60 @@ namespace ss {
 
 constexpr int kPanel = 32;      // panel width of the blocked partial LU
 
-// rows per CTA of the large-front assembly: about 16k elements per CTA, at least
-// 32 rows, a whole front when it is that small (narrow fronts would otherwise
-// make hundreds of thousands of near-empty CTAs)
-static inline int asm_rows(int maxm) { return std::max(32, std::min(maxm, 16384 / std::max(1, maxm))); }
-// Which assembly kernel: the row-owned one for complex64 fronts, the row-chunk one
-// for complex128 (measured: 94.7 vs 92.1 points/s on the Hex27 slab's mixed sweep,
-// 72.4 vs 74.6 on the ME1 cell's FP64 sweep); SS_ASM_BY_ROWS=0|1 overrides.
-template <class T>
-static inline bool asm_by_rows() {
-  if (const char *e = getenv("SS_ASM_BY_ROWS")) return atoi(e) != 0;
-  return sizeof(T) == 4;
+// rows per CTA of the large-front assembly: about SS_ASM_ELEMS elements per CTA
+// (default 16k), at least 32 rows, a whole front when it is that small (narrow
+// fronts would otherwise make hundreds of thousands of near-empty CTAs)
+static inline int asm_rows(int maxm) {
+  int elems = 16384;
+  if (const char *e = getenv("SS_ASM_ELEMS")) elems = std::max(1024, atoi(e));
+  return std::max(32, std::min(maxm, elems / std::max(1, maxm)));
 }
 
-// Large fronts, assembly in global memory: CTA (front, frequency, row chunk)
+// Whole-element accesses of arena entries: one 16-byte (complex128) or 8-byte
+// (complex64) load or store; the arena is cudaMalloc'd and every front offset is
+// a whole number of elements, so each entry is aligned to its size.  ld_once
+// marks data read once (a child's update block) as evict-first, so that it does
+// not push the parent rows being summed out of L2.
+template <class T> struct VecOf;
+template <> struct VecOf<double> { using V = double2; };
+template <> struct VecOf<float> { using V = float2; };
+template <class T>
+__device__ __forceinline__ cplx<T> ld_el(const cplx<T> *p) {
+  const auto v = *reinterpret_cast<const typename VecOf<T>::V *>(p);
+  return {v.x, v.y};
+}
+template <class T>
+__device__ __forceinline__ cplx<T> ld_once(const cplx<T> *p) {
+  const auto v = __ldcs(reinterpret_cast<const typename VecOf<T>::V *>(p));
+  return {v.x, v.y};
+}
+template <class T>
+__device__ __forceinline__ void st_el(cplx<T> *p, cplx<T> v) {
+  typename VecOf<T>::V w;
+  w.x = v.x;
+  w.y = v.y;
+  *reinterpret_cast<typename VecOf<T>::V *>(p) = w;
+}
+// Which assembly kernel: 0 the row-chunk one, 1 the row-owned one in global
+// memory, 2 the row-owned one with each row staged in shared memory.  Defaults:
+// the row-owned one for complex64 fronts, the row-chunk one for complex128
+// (measured: 94.7 vs 92.1 points/s on the Hex27 slab's mixed sweep, 72.4 vs 74.6 on
+// the ME1 cell's FP64 sweep); SS_ASM_BY_ROWS=0|1|2 overrides.
+template <class T>
+static inline int asm_variant() {
+  if (const char *e = getenv("SS_ASM_BY_ROWS")) return std::max(0, std::min(2, atoi(e)));
+  return sizeof(T) == 4 ? 1 : 0;
+}
+constexpr int kAsmSmemMax = 227 * 1024;   // shared memory of one CTA of the staged kernel
+
+// Large fronts, assembly in global memory: CTA (frequency, front, row chunk)
 // zeroes its rows, drops in the arrowhead entries of those rows, then adds the
 // children's update rows that map into them (children in order: deterministic).
+// Frequencies are the fastest grid index, so the CTAs of one front's chunk run
+// together and read its arrowhead entries (shared by all frequencies) from L2.
 template <class T>
 __global__ void __launch_bounds__(256) front_assemble_large_kernel(FrontArgs<T> a, int rows) {
-  const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
+  const int f = a.fronts[blockIdx.y], fq = blockIdx.x;
   const int k = a.k[f], m = a.m[f], ld = a.ld[f];
   const int r0 = blockIdx.z * rows;
   if (r0 >= m) return;
@@ -349,7 +384,7 @@ __global__ void __launch_bounds__(256) front_assemble_large_kernel(FrontArgs<T> 
   cplx<T> *F = arena + a.off[f];
   for (int t = threadIdx.x; t < (r1 - r0) * m; t += blockDim.x) {
     const int r = r0 + t / m, c = t % m;
-    F[(int64_t)r * ld + c] = cplx<T>{0, 0};
+    st_el(F + (int64_t)r * ld + c, cplx<T>{0, 0});
   }
   __syncthreads();
   {
@@ -396,15 +431,15 @@ __global__ void __launch_bounds__(256) front_assemble_large_kernel(FrontArgs<T> 
         if (t < tot) {
           const int i = i0 + t / nn, j = t % nn;
           dp[u] = F + (int64_t)rel[i] * ld + rel[j];
-          cv[u] = CB[(int64_t)i * ldc + j];
+          cv[u] = ld_once(CB + (int64_t)i * ldc + j);
         }
       }
 #pragma unroll
       for (int u = 0; u < U; ++u)
-        if (dp[u]) dv[u] = *dp[u];
+        if (dp[u]) dv[u] = ld_el(dp[u]);
 #pragma unroll
       for (int u = 0; u < U; ++u)
-        if (dp[u]) *dp[u] = dv[u] + cv[u];
+        if (dp[u]) st_el(dp[u], dv[u] + cv[u]);
     }
     __syncthreads();
   }
@@ -419,7 +454,7 @@ __global__ void __launch_bounds__(256) front_assemble_large_kernel(FrontArgs<T> 
 constexpr int kAsmRowsPerCta = 32;
 template <class T>
 __global__ void __launch_bounds__(256) front_assemble_rows_kernel(FrontArgs<T> a) {
-  const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
+  const int f = a.fronts[blockIdx.y], fq = blockIdx.x;
   const int m = a.m[f], ld = a.ld[f];
   const int r0 = blockIdx.z * kAsmRowsPerCta;
   if (r0 >= m) return;
@@ -463,17 +498,83 @@ __global__ void __launch_bounds__(256) front_assemble_rows_kernel(FrontArgs<T> a
         for (int u = 0; u < U; ++u) {
           const int j = j0 + 32 * u;
           cj[u] = j < nn ? rel[j] : -1;
-          if (cj[u] >= 0) cv[u] = src[j];
+          if (cj[u] >= 0) cv[u] = ld_once(src + j);
         }
 #pragma unroll
         for (int u = 0; u < U; ++u)
-          if (cj[u] >= 0) dv[u] = row[cj[u]];
+          if (cj[u] >= 0) dv[u] = ld_el(row + cj[u]);
 #pragma unroll
         for (int u = 0; u < U; ++u)
-          if (cj[u] >= 0) row[cj[u]] = dv[u] + cv[u];
+          if (cj[u] >= 0) st_el(row + cj[u], dv[u] + cv[u]);
       }
       __syncwarp();
     }
+  }
+}
+
+// The row-owned assembly with each warp's row staged in shared memory (rows of
+// `sld` elements): the zero, the arrowhead entries and the children's update rows
+// are summed there in the same order as in the two kernels above (so all three
+// give identical fronts), and the finished row is written to the arena once: the
+// arena sees each front written once and each child block read once, with no
+// read-modify-write of global memory.  Each warp owns rows r0 + wid, + nw, ...
+template <class T>
+__global__ void __launch_bounds__(256) front_assemble_rows_smem_kernel(FrontArgs<T> a, int rows_per_cta, int sld) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int f = a.fronts[blockIdx.y], fq = blockIdx.x;
+  const int m = a.m[f], ld = a.ld[f];
+  const int r0 = blockIdx.z * rows_per_cta;
+  if (r0 >= m) return;
+  const int r1 = min(m, r0 + rows_per_cta);
+  const double w = a.omega[fq];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  cplx<T> *srow = reinterpret_cast<cplx<T> *>(smem_raw) + (int64_t)wid * sld;
+  cplx<T> *arena = a.arena + (int64_t)fq * a.stride;
+  cplx<T> *F = arena + a.off[f];
+  const int64_t alo = a.arrow_ptr[f], ahi = a.arrow_ptr[f + 1];
+  for (int r = r0 + wid; r < r1; r += nw) {
+    for (int c = lane; c < m; c += 32) srow[c] = cplx<T>{0, 0};
+    __syncwarp();
+    {
+      int64_t b = alo, e = ahi;
+      while (b < e) {
+        const int64_t mid = (b + e) / 2;
+        if (a.arrow_pos[mid] < r * ld) b = mid + 1; else e = mid;
+      }
+      for (int64_t q = b + lane; q < ahi && a.arrow_pos[q] < (r + 1) * ld; q += 32)
+        srow[a.arrow_pos[q] - r * ld] = to_t<T>(a_entry(a.Kc, a.Mc, a.Dc, a.arrow_slot[q], w, a.beta));
+    }
+    __syncwarp();
+    for (int64_t cc = a.child_ptr[f]; cc < a.child_ptr[f + 1]; ++cc) {
+      const int ch = a.child[cc];
+      const int kc = a.k[ch], nn = a.m[ch] - kc, ldc = a.ld[ch];
+      const int *rel = a.relpos + a.relpos_ptr[ch];
+      int b = 0, e = nn;
+      while (b < e) {
+        const int mid = (b + e) / 2;
+        if (rel[mid] < r) b = mid + 1; else e = mid;
+      }
+      if (b == nn || rel[b] != r) continue;
+      const cplx<T> *src = arena + a.off[ch] + (int64_t)(kc + b) * ldc + kc;
+      constexpr int U = 4;
+      for (int j0 = lane; j0 < nn; j0 += 32 * U) {
+        int cj[U];
+        cplx<T> cv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int j = j0 + 32 * u;
+          cj[u] = j < nn ? rel[j] : -1;
+          if (cj[u] >= 0) cv[u] = ld_once(src + j);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+          if (cj[u] >= 0) srow[cj[u]] = srow[cj[u]] + cv[u];
+      }
+      __syncwarp();
+    }
+    cplx<T> *row = F + (int64_t)r * ld;
+    for (int c = lane; c < m; c += 32) st_el(row + c, srow[c]);
+    __syncwarp();
   }
 }
 
@@ -1574,6 +1675,30 @@ static void add_tiles(std::vector<GemmTask> &v, int shape, int f, int r0, int r1
   add_tiles(v, tile_bm(shape), tile_bn(shape), f, r0, r1, c0, c1, k0, k1);
 }
 
+// Panel-step GEMMs of one front at panel j0 (left-looking, blocked in two levels).
+// The pivots are taken in blocks of kOuter columns [b0, b1): when a block starts,
+// its columns (rows [b0, m)) get every earlier pivot at once (K = [0, b0)), so the
+// L columns left of the block are read once per block instead of once per panel;
+// the block's later panels then need only the pivots [b0, j0).  The U rows of a
+// panel are updated after its row swaps: their columns inside the block by the
+// pivots [b0, j0) (the block update already applied [0, b0)), the columns right of
+// the block by all pivots [0, j0).  (Row swaps stay inside [j0, k), and every row in
+// [b0, m) received the same block update, so the swaps keep the updates consistent.)
+constexpr int kOuter = 128;
+static void add_panel_col_tiles(std::vector<GemmTask> &v, int bm, int bn, int f, int k, int m, int j0) {
+  const int b0 = j0 / kOuter * kOuter, b1 = std::min(k, b0 + kOuter);
+  if (j0 == b0) {
+    if (j0 > 0) add_tiles(v, bm, bn, f, j0, m, j0, b1, 0, j0);
+  } else {
+    add_tiles(v, bm, bn, f, j0, m, j0, std::min(k, j0 + kPanel), b0, j0);
+  }
+}
+static void add_panel_row_tiles(std::vector<GemmTask> &v, int bm, int bn, int f, int k, int m, int j0) {
+  const int b0 = j0 / kOuter * kOuter, b1 = std::min(k, b0 + kOuter), j1 = std::min(k, j0 + kPanel);
+  if (j0 > b0 && j1 < b1) add_tiles(v, bm, bn, f, j0, j1, j1, b1, b0, j0);
+  if (j0 > 0 && std::max(j1, b1) < m) add_tiles(v, bm, bn, f, j0, j1, std::max(j1, b1), m, 0, j0);
+}
+
 Plan *build_plan(Handle &h, int small_m, bool tensor_schur) {
   Symbolic &S = h.sym;
   Plan *P = new Plan();
@@ -1617,19 +1742,11 @@ Plan *build_plan(Handle &h, int small_m, bool tensor_schur) {
     // pivots (skinny GEMM, K = j0), after it the U row block does (short GEMM)
     for (int s = 0; s < ns; ++s) {
       const int j0 = s * kPanel;
-      for (int f : large) {
-        const int k = S.k[f], m = S.m[f];
-        if (j0 >= k || j0 == 0) continue;
-        const int j1 = std::min(k, j0 + kPanel);
-        add_tiles(P->tasks, kSkinny, f, j0, m, j0, j1, 0, j0);
-      }
+      for (int f : large)
+        if (j0 < S.k[f]) add_panel_col_tiles(P->tasks, tile_bm(kSkinny), tile_bn(kSkinny), f, S.k[f], S.m[f], j0);
       P->step_ptr.push_back((int64_t)P->tasks.size());
-      for (int f : large) {
-        const int k = S.k[f], m = S.m[f];
-        if (j0 >= k || j0 == 0) continue;
-        const int j1 = std::min(k, j0 + kPanel);
-        if (j1 < m) add_tiles(P->tasks, kShort, f, j0, j1, j1, m, 0, j0);
-      }
+      for (int f : large)
+        if (j0 < S.k[f]) add_panel_row_tiles(P->tasks, tile_bm(kShort), tile_bn(kShort), f, S.k[f], S.m[f], j0);
       P->step_ptr.push_back((int64_t)P->tasks.size());
     }
     P->schur_ptr.push_back((int64_t)P->tasks.size());
@@ -1706,16 +1823,13 @@ Plan *build_plan(Handle &h, int small_m, bool tensor_schur) {
       for (int st = 0; st < P->nsteps[l]; ++st) {
         const int j0 = st * kPanel;
         for (int q = P->large_ptr[l]; q < P->large_ptr[l + 1]; ++q) {
-          const int f = P->fronts_large[q], k = S.k[f], m = S.m[f];
-          if (j0 >= k || j0 == 0) continue;
-          add_tiles(P->tasks, 128, 32, f, j0, m, j0, std::min(k, j0 + kPanel), 0, j0);
+          const int f = P->fronts_large[q];
+          if (j0 < S.k[f]) add_panel_col_tiles(P->tasks, 128, 32, f, S.k[f], S.m[f], j0);
         }
         P->step_ptr_d.push_back((int64_t)P->tasks.size());
         for (int q = P->large_ptr[l]; q < P->large_ptr[l + 1]; ++q) {
-          const int f = P->fronts_large[q], k = S.k[f], m = S.m[f];
-          if (j0 >= k || j0 == 0) continue;
-          const int j1 = std::min(k, j0 + kPanel);
-          if (j1 < m) add_tiles(P->tasks, 32, 128, f, j0, j1, j1, m, 0, j0);
+          const int f = P->fronts_large[q];
+          if (j0 < S.k[f]) add_panel_row_tiles(P->tasks, 32, 128, f, S.k[f], S.m[f], j0);
         }
         P->step_ptr_d.push_back((int64_t)P->tasks.size());
       }
@@ -2196,14 +2310,29 @@ struct Sweeper {
       FrontArgs<T> b = a;
       b.fronts = P.d_large.as<int>() + P.large_ptr[l];
       const int ml = P.maxm_large[l];
-      if (asm_by_rows<T>()) {
-        front_assemble_rows_kernel<T><<<dim3(nl, nb, (ml + kAsmRowsPerCta - 1) / kAsmRowsPerCta), 256, 0,
-                                        h.stream>>>(b);
-      } else {
-        const int ar = asm_rows(ml);
-        front_assemble_large_kernel<T><<<dim3(nl, nb, (ml + ar - 1) / ar), 256, 0, h.stream>>>(b, ar);
+      // grid (frequency, front, row chunk); gridDim.y is at most 65535, so a
+      // level with more large fronts is launched in slices of fronts
+      for (int s0 = 0; s0 < nl; s0 += 65535) {
+        const int ns1 = std::min(nl - s0, 65535);
+        FrontArgs<T> bs = b;
+        bs.fronts = b.fronts + s0;
+        const int av = asm_variant<T>();
+        // staged kernel: as many warps (<= 8) as rows of the level's widest front
+        // fit in one CTA's shared memory, four rows per warp
+        const int snw = std::min(8, kAsmSmemMax / (ml * (int)sizeof(cplx<T>)));
+        if (av == 2 && snw >= 1) {
+          const int rpc = 4 * snw;
+          front_assemble_rows_smem_kernel<T><<<dim3(nb, ns1, (ml + rpc - 1) / rpc), 32 * snw,
+                                               (size_t)snw * ml * sizeof(cplx<T>), h.stream>>>(bs, rpc, ml);
+        } else if (av >= 1) {
+          front_assemble_rows_kernel<T><<<dim3(nb, ns1, (ml + kAsmRowsPerCta - 1) / kAsmRowsPerCta), 256, 0,
+                                          h.stream>>>(bs);
+        } else {
+          const int ar = asm_rows(ml);
+          front_assemble_large_kernel<T><<<dim3(nb, ns1, (ml + ar - 1) / ar), 256, 0, h.stream>>>(bs, ar);
+        }
+        ++launches;
       }
-      ++launches;
       const GemmTask *tasks = P.d_tasks.as<GemmTask>();
       // row/column-parallel panel kernels: CTAs no wider than the level's fronts
       // (narrow fronts then run more CTAs per SM instead of idle threads)
@@ -2366,6 +2495,8 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
                                small_limit<T>() * small_limit<T>() * (int)sizeof(cplx<T>)));
     SS_CK(cudaFuncSetAttribute(front_panel_smem_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                kPanelSmemMax));
+    SS_CK(cudaFuncSetAttribute(front_assemble_rows_smem_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               kAsmSmemMax));
     SS_CK(cudaFuncSetAttribute(tc::tma_gemm_kernel<128, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                tc::TmaCfg<128, 2>::SMEM));
     SS_CK(cudaFuncSetAttribute(tc::tma_gemm_kernel<64, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,

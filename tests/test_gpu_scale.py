@@ -130,8 +130,9 @@ def test_every_complex64_schur_candidate_converges(mid, tile, monkeypatch):
 
 @pytest.mark.parametrize('precision', ['fp64', 'mixed'])
 def test_assembly_kernels_agree_bit_for_bit(mid, precision, monkeypatch):
-    """The row-chunk and the row-owned front assembly perform the same additions in
-    the same order, so sweeps through either give identical charges (with the
+    """The row-chunk, the row-owned and the shared-memory-staged row-owned front
+    assembly perform the same additions in the same order, so sweeps through any of
+    them give identical charges (with the
     Schur kernels forced: two engines' autotuners may pick different tiles of equal
     speed, whose sums round differently)."""
     case, _, _ = mid
@@ -139,7 +140,7 @@ def test_assembly_kernels_agree_bit_for_bit(mid, precision, monkeypatch):
     monkeypatch.setenv('SS_SCHUR_TILE', '2')
     monkeypatch.setenv('SS_SCHUR_TILE_C64', '0')
     Q = []
-    for by_rows in ('0', '1'):
+    for by_rows in ('0', '1', '2'):
         monkeypatch.setenv('SS_ASM_BY_ROWS', by_rows)
         e = cases.engine_for(case)
         try:
@@ -148,4 +149,4 @@ def test_assembly_kernels_agree_bit_for_bit(mid, precision, monkeypatch):
             e.close()
         assert (st == 0).all()
         Q.append(q)
-    assert np.array_equal(Q[0], Q[1])
+    assert np.array_equal(Q[0], Q[1]) and np.array_equal(Q[0], Q[2])
