@@ -271,19 +271,42 @@ __global__ void __launch_bounds__(kSmallThreads) front_small_kernel(FrontArgs<T>
       if (pert) atomicAdd(a.nperturb + fq, 1);
     }
     const cplx<T> inv = cdiv(cplx<T>{1, 0}, pv);
-    // rows below the pivot: multiplier, then the rank-1 update of the row
+    // rows below the pivot: multiplier, then the rank-1 update of the row.  The
+    // pivot row's columns are held in registers (CU per lane covers m - 1 columns
+    // at the widest small front), and each row's loads are all issued before its
+    // stores, so that a warp keeps them in flight together.
+    constexpr int CU = sizeof(T) == 8 ? 4 : 5;
     const cplx<T> *prow = F + j * m;
+    cplx<T> pr[CU];
+#pragma unroll
+    for (int u = 0; u < CU; ++u) {
+      const int c = j + 1 + lane + 32 * u;
+      pr[u] = c < m ? prow[c] : cplx<T>{0, 0};
+    }
     T best = (T)-1;
     int bi = j + 1;
     for (int r = j + 1 + wid; r < m; r += nw) {
       cplx<T> *row = F + r * m;
       const cplx<T> l = cmul(row[j], inv);
-      for (int c = j + 1 + lane; c < m; c += 32) row[c] = cfms(row[c], l, prow[c]);
+      cplx<T> rv[CU];
+#pragma unroll
+      for (int u = 0; u < CU; ++u) {
+        const int c = j + 1 + lane + 32 * u;
+        if (c < m) rv[u] = row[c];
+      }
+#pragma unroll
+      for (int u = 0; u < CU; ++u) {
+        const int c = j + 1 + lane + 32 * u;
+        if (c < m) {
+          rv[u] = cfms(rv[u], l, pr[u]);
+          row[c] = rv[u];
+        }
+      }
       __syncwarp();
       if (lane == 0) {
         row[j] = l;
         if (r < k && j + 1 < k) {
-          const T v = cabs1(row[j + 1]);
+          const T v = cabs1(rv[0]);   // the updated F[r][j + 1]: lane 0's first column
           if (v > best) best = v, bi = r;
         }
       }
@@ -298,12 +321,14 @@ __global__ void __launch_bounds__(kSmallThreads) front_small_kernel(FrontArgs<T>
     pv_prev = pv;
     __syncthreads();
     if (j + 1 < k) {
-      T bv = (T)-1;
-      int bq = j + 1;
-      for (int q = 0; q < nw; ++q) {
-        const T v = s_cv[j & 1][q];
-        const int i = s_ci[j & 1][q];
-        if (v > bv || (v == bv && i < bq)) bv = v, bq = i;
+      // largest modulus, lowest row on ties: a total order, so the shuffle tree
+      // gives the same row in every warp (and as a serial scan would)
+      T bv = lane < nw ? s_cv[j & 1][lane] : (T)-1;
+      int bq = lane < nw ? s_ci[j & 1][lane] : j + 1;
+      for (int o = 16; o > 0; o >>= 1) {
+        const T ov = __shfl_xor_sync(0xffffffffu, bv, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bq, o);
+        if (ov > bv || (ov == bv && oi < bq)) bv = ov, bq = oi;
       }
       p = bq;
     }
@@ -581,26 +606,13 @@ __global__ void __launch_bounds__(256) front_assemble_rows_smem_kernel(FrontArgs
 // Rows [k, m) of the panel columns: L21[:, j0:j1] = F21[:, j0:j1] U_jj^-1 (each
 // row independent, one thread per row; U_jj and its diagonal reciprocals staged in
 // shared memory).  The 32 columns go in two halves of 16 held in registers: the
-// second half first takes the first half's finished values back from the row
-// (still in L1) in the order t = 0, 1, ..., so every entry sees the operations of a
-// single 32-column substitution in the same order.
+// second half first takes the first half's finished values back from the row in
+// the order t = 0, 1, ..., so every entry sees the operations of a single
+// 32-column substitution in the same order.  `row` is the row in global memory or
+// in a staged tile.
 template <class T>
-__global__ void __launch_bounds__(256) front_l21_kernel(FrontArgs<T> a, int j0) {
+__device__ __forceinline__ void l21_row(cplx<T> *row, int w, const cplx<T> (*U)[kPanel], const cplx<T> *Uinv) {
   constexpr int H = kPanel / 2;
-  __shared__ cplx<T> U[kPanel][kPanel];
-  __shared__ cplx<T> Uinv[kPanel];          // reciprocals of the diagonal, once per CTA
-  const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
-  const int k = a.k[f], m = a.m[f], ld = a.ld[f];
-  if (j0 >= k) return;
-  const int j1 = min(k, j0 + kPanel), w = j1 - j0;
-  const cplx<T> *Fc = a.arena + (int64_t)fq * a.stride + a.off[f];
-  for (int t = threadIdx.x; t < w * w; t += blockDim.x) U[t / w][t % w] = Fc[(int64_t)(j0 + t / w) * ld + j0 + t % w];
-  __syncthreads();
-  if (threadIdx.x < w) Uinv[threadIdx.x] = cdiv(cplx<T>{1, 0}, U[threadIdx.x][threadIdx.x]);
-  __syncthreads();
-  const int r = k + blockIdx.z * blockDim.x + threadIdx.x;
-  if (r >= m) return;
-  cplx<T> *row = a.arena + (int64_t)fq * a.stride + a.off[f] + (int64_t)r * ld + j0;
   for (int h0 = 0; h0 < w; h0 += H) {
     const int hw = min(H, w - h0);
     cplx<T> x[H];
@@ -627,6 +639,61 @@ __global__ void __launch_bounds__(256) front_l21_kernel(FrontArgs<T> a, int j0) 
       if (c < hw) row[h0 + c] = x[c];
   }
 }
+
+// STAGED: each warp stages its 32 rows of the panel columns in shared memory with
+// coalesced loads (lane = column), solves them with lane = row, and writes them
+// back coalesced.  Otherwise each thread works on its row in global memory (a
+// warp's loads then touch 32 rows at once).  The arithmetic is the same.  Staging
+// is the default for complex64 (Hex27 slab mixed sweep 140.2 vs 132.0 points/s);
+// complex128 keeps the direct form (77.5 vs 77.2 points/s on the ME1 cell: its
+// staged tiles take 135 KB per 256-thread CTA); SS_L21_STAGED=0|1 overrides.
+template <class T, bool STAGED>
+__global__ void __launch_bounds__(256) front_l21_kernel(FrontArgs<T> a, int j0) {
+  constexpr int TS = kPanel + 1;            // staged tile row stride (conflict-free)
+  __shared__ cplx<T> U[kPanel][kPanel];
+  __shared__ cplx<T> Uinv[kPanel];          // reciprocals of the diagonal, once per CTA
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int f = a.fronts[blockIdx.x], fq = blockIdx.y;
+  const int k = a.k[f], m = a.m[f], ld = a.ld[f];
+  if (j0 >= k) return;
+  const int j1 = min(k, j0 + kPanel), w = j1 - j0;
+  const cplx<T> *Fc = a.arena + (int64_t)fq * a.stride + a.off[f];
+  for (int t = threadIdx.x; t < w * w; t += blockDim.x) U[t / w][t % w] = Fc[(int64_t)(j0 + t / w) * ld + j0 + t % w];
+  __syncthreads();
+  if (threadIdx.x < w) Uinv[threadIdx.x] = cdiv(cplx<T>{1, 0}, U[threadIdx.x][threadIdx.x]);
+  __syncthreads();
+  cplx<T> *F = a.arena + (int64_t)fq * a.stride + a.off[f];
+  if constexpr (!STAGED) {
+    const int r = k + blockIdx.z * blockDim.x + threadIdx.x;
+    if (r < m) l21_row<T>(F + (int64_t)r * ld + j0, w, U, Uinv);
+  } else {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int rw = k + blockIdx.z * blockDim.x + wid * 32;
+    if (rw >= m) return;
+    const int nr = min(32, m - rw);
+    cplx<T> *tile = reinterpret_cast<cplx<T> *>(smem_raw) + wid * 32 * TS;
+    cplx<T> *gp = F + (int64_t)rw * ld + j0;
+    if (lane < w) {
+#pragma unroll 8
+      for (int i = 0; i < nr; ++i) tile[i * TS + lane] = ld_el(gp + (int64_t)i * ld + lane);
+    }
+    __syncwarp();
+    if (lane < nr) l21_row<T>(tile + lane * TS, w, U, Uinv);
+    __syncwarp();
+    if (lane < w) {
+#pragma unroll 8
+      for (int i = 0; i < nr; ++i) st_el(gp + (int64_t)i * ld + lane, tile[i * TS + lane]);
+    }
+  }
+}
+template <class T>
+static inline bool l21_staged() {
+  if (const char *e = getenv("SS_L21_STAGED")) return atoi(e) != 0;
+  return sizeof(T) == 4;
+}
+// dynamic shared memory of front_l21_kernel for a CTA of `threads` threads
+template <class T>
+static inline size_t l21_smem(int threads) { return (size_t)(threads / 32) * 32 * (kPanel + 1) * sizeof(cplx<T>); }
 
 // Unblocked LU of panel columns [j0, j1) over the fully-summed rows [j0, k).
 template <class T>
@@ -2353,7 +2420,10 @@ struct Sweeper {
           front_panel_smem_kernel<T><<<dim3(nl, nb), pth, psm, h.stream>>>(b, j0);
         else
           front_panel_kernel<T><<<dim3(nl, nb), 256, 0, h.stream>>>(b, j0);
-        front_l21_kernel<T><<<dim3(nl, nb, zc), bs, 0, h.stream>>>(b, j0);
+        if (l21_staged<T>())
+          front_l21_kernel<T, true><<<dim3(nl, nb, zc), bs, l21_smem<T>(bs), h.stream>>>(b, j0);
+        else
+          front_l21_kernel<T, false><<<dim3(nl, nb, zc), bs, 0, h.stream>>>(b, j0);
         front_swap_kernel<T><<<dim3(nl, nb, zc), bs, 0, h.stream>>>(b, j0);
         if (g2 > g1) {   // U row block <- earlier pivots
           panel_gemm(b, q, 1, nb);
@@ -2497,6 +2567,8 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
                                kPanelSmemMax));
     SS_CK(cudaFuncSetAttribute(front_assemble_rows_smem_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                kAsmSmemMax));
+    SS_CK(cudaFuncSetAttribute(front_l21_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)l21_smem<T>(256)));
     SS_CK(cudaFuncSetAttribute(tc::tma_gemm_kernel<128, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                tc::TmaCfg<128, 2>::SMEM));
     SS_CK(cudaFuncSetAttribute(tc::tma_gemm_kernel<64, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2727,8 +2799,12 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
       SS_CK(cudaMemcpyAsync(hn.data(), nrm.p, 2 * nb * sizeof(double), cudaMemcpyDeviceToHost, h.stream));
       SS_CK(cudaStreamSynchronize(h.stream));
       bool all = true;
-      if (getenv("SS_DEBUG_IR"))
-        fprintf(stderr, "IR it %d: dx/x f0 %.3e f_last %.3e\n", it, hn[0] / hn[1], hn[2 * (nb - 1)] / hn[2 * nb - 1]);
+      if (getenv("SS_DEBUG_IR")) {
+        double mx = 0;
+        for (int f = 0; f < nb; ++f) mx = std::max(mx, hn[2 * f] / hn[2 * f + 1]);
+        fprintf(stderr, "IR it %d: dx/x f0 %.3e f_last %.3e max %.3e\n", it, hn[0] / hn[1],
+                hn[2 * (nb - 1)] / hn[2 * nb - 1], mx);
+      }
       for (int f = 0; f < nb; ++f) {
         if (!conv[f]) {
           ++hit[f];

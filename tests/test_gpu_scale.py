@@ -150,3 +150,24 @@ def test_assembly_kernels_agree_bit_for_bit(mid, precision, monkeypatch):
         assert (st == 0).all()
         Q.append(q)
     assert np.array_equal(Q[0], Q[1]) and np.array_equal(Q[0], Q[2])
+
+
+@pytest.mark.parametrize('precision', ['fp64', 'mixed'])
+def test_l21_forms_agree_bit_for_bit(mid, precision, monkeypatch):
+    """The panel-column solve L21 = F21 U11^-1 staged through shared memory and in
+    place in global memory perform the same arithmetic: identical charges."""
+    case, _, _ = mid
+    w = 2 * np.pi * np.linspace(case.freqs[0], case.freqs[-1], 4)
+    monkeypatch.setenv('SS_SCHUR_TILE', '2')
+    monkeypatch.setenv('SS_SCHUR_TILE_C64', '0')
+    Q = []
+    for staged in ('0', '1'):
+        monkeypatch.setenv('SS_L21_STAGED', staged)
+        e = cases.engine_for(case)
+        try:
+            q, st, _ = e.charges(w, 1.0, precision)
+        finally:
+            e.close()
+        assert (st == 0).all()
+        Q.append(q)
+    assert np.array_equal(Q[0], Q[1])
