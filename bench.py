@@ -267,8 +267,9 @@ def schur_kernel_name(s, used):
     else:
         names = ['front_gemm_kernel<double> SIMT 128x64',
                  'front_dmma3_kernel (FP64 DMMA 64x64, three real products per complex block)',
-                 'front_dmma_kernel<2,2> (FP64 DMMA 64x64)']
-    keys = ['schur_candidate0', 'schur_candidate1', 'schur_candidate2']
+                 'front_dmma_kernel<2,2> (FP64 DMMA 64x64)',
+                 'front_dmma3_kernel<2,2,CST> (the same with the C tile staged in shared memory)']
+    keys = ['schur_candidate0', 'schur_candidate1', 'schur_candidate2', 'schur_candidate3']
     parts = [f'{n} on {int(s[k])} levels' for n, k in zip(names, keys) if s.get(k, 0) > 0]
     return 'Schur update F22 -= F21 F12: ' + ', '.join(parts)
 
@@ -341,7 +342,8 @@ def rooflines(eng, c, s, st0, used, schur_ms, nf, pk, pk_kind, ceilings):
                      f'flops over the per-level mix of tcgen05 3xTF32 tiles (three MMA passes each) and SIMT FP32 '
                      f'tiles; own-kernel ceilings on dense 2560-row fronts: {ceilings}')
     else:
-        peak = max(ceilings.get('fp64_dmma', 0.0), ceilings.get('fp64_dmma_3m', 0.0)) or None
+        peak = max(ceilings.get('fp64_dmma', 0.0), ceilings.get('fp64_dmma_3m', 0.0),
+                   ceilings.get('fp64_dmma_3m_cst', 0.0)) or None
         peak_note = ('measured ceiling of this library\'s fastest FP64 Schur tile on 8 dense fronts of 2560 rows '
                      'with 512 pivots (ss_measure_gemm_ceiling, median of 5 launches; DMMA with three real products '
                      'per complex block counts the algorithmic complex flops, so it can exceed the nominal FP64 '
@@ -452,7 +454,8 @@ def b200_arm(a, rank, world, local):
     s = s_timed           # counters of the last timed sweep
     # untimed: both precision modes on this rank's points, and the measured ceilings
     modes = None if a.no_modes else mode_comparison(eng, f_all[mine], w, 2)
-    ceilings = {'fp64_dmma': eng.gemm_ceiling(0), 'fp64_dmma_3m': eng.gemm_ceiling(5)}
+    ceilings = {'fp64_dmma': eng.gemm_ceiling(0), 'fp64_dmma_3m': eng.gemm_ceiling(5),
+                'fp64_dmma_3m_cst': eng.gemm_ceiling(6)}
     if used == 'mixed' or modes is not None:
         ceilings.update(c64_tma_tcgen05_128=eng.gemm_ceiling(2), c64_tma_tcgen05_64=eng.gemm_ceiling(3),
                         c64_simt=eng.gemm_ceiling(4))

@@ -231,7 +231,7 @@ int ss_adjoint_gradient(ss_handle *h, int n_f, const double *omega, double V, in
  *  sweep: packed operands + TMA + tcgen05 3xTF32 with 128 / 64 complex columns
  *  per tile, SIMT FP32 128x64),
  *  23 panel-step GEMM tiles (128x32 / 32x128): 0 SIMT, 1 DMMA, 2 DMMA with
- *  three real products per complex block, 24-25 autotuner time of all
+ *  three real products per complex block, 3 the same with C staged, 24-25 autotuner time of all
  *  panel-step GEMMs with SIMT / the faster DMMA tiles (ms),
  *  26 fronts factored whole in shared memory, 27 autotuner time of all
  *  Schur candidates (ms, sum over candidates and levels),
@@ -241,7 +241,9 @@ int ss_adjoint_gradient(ss_handle *h, int n_f, const double *omega, double V, in
  *  whose mixed refinement did not converge (before any FP64 re-solve), 33 device
  *  time of the FP64 re-solves (ms, included in 17), 34 / 35 device time of the
  *  element kernel / of the scatter into the CSR pattern of the last
- *  ss_assemble (ms, CUDA events).  Slots past 35 read 0.
+ *  ss_assemble (ms, CUDA events), 36 levels whose FP64 Schur update uses
+ *  candidate 3 (DMMA 64x64, three real products, C tile staged in shared
+ *  memory while the K loop runs).  Slots past 36 read 0.
  */
 int ss_stats(const ss_handle *h, double *out, int n);
 
@@ -275,7 +277,8 @@ int ss_set_option(ss_handle *h, const char *name, double value);
  * warm-up.  kernel: 0 FP64 DMMA 64x64 tiles, 1 FP64 SIMT 128x64, 2 complex64
  * TMA + tcgen05 3xTF32 with 128-column tiles, 3 the same with 64-column tiles
  * (operands packed once before the timed launches), 4 complex64 SIMT FP32
- * 128x64, 5 FP64 DMMA 64x64 with three real products per complex block.
+ * 128x64, 5 FP64 DMMA 64x64 with three real products per complex block, 6 the
+ * same with the C tile staged in shared memory while the K loop runs.
  * Allocates and frees its fronts (at most 64 GB).
  */
 int ss_measure_gemm_ceiling(ss_handle *h, int kernel, int m, int k, int n_fronts, int reps,

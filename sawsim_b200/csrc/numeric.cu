@@ -1109,12 +1109,20 @@ __global__ void __launch_bounds__(128, 3) front_dmma_kernel(FrontArgs<double> a,
 // u (|Ar| + |Ai|)(|Br| + |Bi|) per term instead of u (|Ar||Bi| + |Ai||Br|).
 // Three accumulator sets (96 doubles per thread): two CTAs per SM.  WM x WN warps
 // of 32x32 complex, as front_dmma_kernel (2x2 Schur tiles, 4x1 / 1x4 panel steps).
+// CST: the C tile is copied into shared memory by cp.async when the CTA starts (row
+// stride BN + 1: conflict-free fragment reads), so its DRAM latency overlaps the K
+// loop instead of following it; for the updates with short K (12-36 pivots on the
+// lower levels of a nested dissection), where the tile's read-modify-write of C is
+// most of its time.  Dynamic shared memory: dmma_cst_bytes<WM, WN>().
 template <int WM, int WN>
+constexpr int dmma_cst_bytes() { return 32 * WM * (32 * WN + 1) * (int)sizeof(cd); }
+template <int WM, int WN, bool CST = false>
 __global__ void __launch_bounds__(128, 2) front_dmma3_kernel(FrontArgs<double> a, const GemmTask *__restrict__ tasks) {
-  constexpr int kDmmaBM = 32 * WM, kDmmaBN = 32 * WN, kDmmaBS = kDmmaBN + 2;
+  constexpr int kDmmaBM = 32 * WM, kDmmaBN = 32 * WN, kDmmaBS = kDmmaBN + 2, kCS = kDmmaBN + 1;
   static_assert(WM * WN == 4, "four warps");
   __shared__ __align__(16) cd As[2][kDmmaBM * kDmmaAS];
   __shared__ __align__(16) cd Bs[2][kDmmaBK * kDmmaBS];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   const GemmTask tk = tasks[blockIdx.x];
   const int fq = blockIdx.y;
   const int ld = a.ld[tk.f];
@@ -1122,6 +1130,19 @@ __global__ void __launch_bounds__(128, 2) front_dmma3_kernel(FrontArgs<double> a
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int wm = wid / WN, wn = wid % WN;       // warp tile origin (32 x 32 complex)
   const int g = lane >> 2, t = lane & 3;
+  cd *Cs = reinterpret_cast<cd *>(smem_raw);
+  if constexpr (CST) {
+    // the C tile (zeros outside the front's block), one cp.async group of its own
+    // committed before the first operand chunk's
+    for (int idx = threadIdx.x; idx < kDmmaBM * kDmmaBN; idx += 128) {
+      const int r = idx / kDmmaBN, c = idx % kDmmaBN;
+      const int gr = tk.r0 + r, gc = tk.c0 + c;
+      const bool ok = gr < tk.rhi && gc < tk.chi;
+      cp_async16_cd((uint32_t)__cvta_generic_to_shared(&Cs[r * kCS + c]), ok ? F + (int64_t)gr * ld + gc : F,
+                    ok ? 16u : 0u);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
   double p1[4][4][2], p2[4][4][2], p3[4][4][2];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
@@ -1185,9 +1206,15 @@ __global__ void __launch_bounds__(128, 2) front_dmma3_kernel(FrontArgs<double> a
     }
     __syncthreads();
   }
+  if constexpr (CST) {
+    if (nk == 0) {   // no operand chunk waited for the C tile
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+      __syncthreads();
+    }
+  }
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const int r = tk.r0 + wm * 32 + i * 8 + g;
+    const int rl = wm * 32 + i * 8 + g, r = tk.r0 + rl;
     const bool rok = r < tk.rhi;
     cd *Fr = F + (int64_t)(rok ? r : tk.r0) * ld;
     cd cv[4][2];
@@ -1195,8 +1222,11 @@ __global__ void __launch_bounds__(128, 2) front_dmma3_kernel(FrontArgs<double> a
     for (int j = 0; j < 4; ++j)
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
-        const int c = tk.c0 + wn * 32 + j * 8 + 2 * t + e;
-        cv[j][e] = (rok && c < tk.chi) ? Fr[c] : cd{0.0, 0.0};
+        const int cl = wn * 32 + j * 8 + 2 * t + e, c = tk.c0 + cl;
+        if constexpr (CST)
+          cv[j][e] = Cs[rl * kCS + cl];
+        else
+          cv[j][e] = (rok && c < tk.chi) ? Fr[c] : cd{0.0, 0.0};
       }
 #pragma unroll
     for (int j = 0; j < 4; ++j)
@@ -1711,8 +1741,9 @@ struct Plan {
   std::vector<int64_t> schur_ptr_b;
   std::vector<int64_t> step_ptr_d;         // panel-step tasks in DMMA tiles (same indexing as step_ptr)
   int panel_dmma = 0;                      // panel-step GEMMs: 0 SIMT, 1 DMMA, 2 DMMA with three
-                                           // real products per complex block (tuned once per plan)
-  float panel_ms[3] = {0, 0, 0};           // tuner's panel-GEMM times: SIMT, DMMA, DMMA 3M
+                                           // real products per complex block, 3 the same with the
+                                           // C tile staged (tuned once per plan)
+  float panel_ms[4] = {0, 0, 0, 0};        // tuner's panel-GEMM times: SIMT, DMMA, DMMA 3M, DMMA 3M C staged
   std::vector<char> pick;                  // per level candidate
   std::vector<float> tune_ms;              // [candidate][level] measured times
   bool tuned = true;
@@ -2211,7 +2242,12 @@ struct Sweeper {
         const int64_t t0 = P.step_ptr_d[q + which], t1 = P.step_ptr_d[q + which + 1];
         if (t1 == t0) return;
         const dim3 grid((unsigned)(t1 - t0), nb);
-        if (P.panel_dmma == 2) {
+        if (P.panel_dmma == 3) {
+          if (which == 0)
+            front_dmma3_kernel<4, 1, true><<<grid, 128, dmma_cst_bytes<4, 1>(), h.stream>>>(b, tasks + t0);
+          else
+            front_dmma3_kernel<1, 4, true><<<grid, 128, dmma_cst_bytes<1, 4>(), h.stream>>>(b, tasks + t0);
+        } else if (P.panel_dmma == 2) {
           if (which == 0)
             front_dmma3_kernel<4, 1><<<grid, 128, 0, h.stream>>>(b, tasks + t0);
           else
@@ -2274,6 +2310,9 @@ struct Sweeper {
     if constexpr (sizeof(T) == 8) {
       if (c == 1)
         front_dmma3_kernel<2, 2><<<dim3((unsigned)(t1 - t0), nb), 128, 0, h.stream>>>(b, tasks + t0);
+      else if (c == 3)
+        front_dmma3_kernel<2, 2, true><<<dim3((unsigned)(t1 - t0), nb), 128, dmma_cst_bytes<2, 2>(), h.stream>>>(
+            b, tasks + t0);
       else
         front_dmma_kernel<2, 2><<<dim3((unsigned)(t1 - t0), nb), 128, 0, h.stream>>>(b, tasks + t0);
     }
@@ -2287,7 +2326,9 @@ struct Sweeper {
     if (P.tuned) return SS_OK;
     const Symbolic &S = h.sym;
     const char *force = getenv(sizeof(T) == 8 ? "SS_SCHUR_TILE" : "SS_SCHUR_TILE_C64");
-    constexpr int NC = 3;
+    // FP64: SIMT 128x64, DMMA three products, DMMA four products, DMMA three
+    // products with C staged; complex64: TMA 128 / 64 columns, SIMT
+    constexpr int NC = sizeof(T) == 8 ? 4 : 3;
     P.tune_ms.assign((size_t)NC * S.nlevel, 0.f);
     if (!force) {
       std::vector<cudaEvent_t> e(2 * NC * S.nlevel);
@@ -2310,11 +2351,13 @@ struct Sweeper {
       for (auto &x : e) cudaEventDestroy(x);
       if constexpr (sizeof(T) == 8) {
       // panel-step GEMMs (FP64): all of them once with SIMT tiles, once with DMMA
-      // tiles, once with DMMA tiles of three real products per complex block
-      cudaEvent_t pe[6];
+      // tiles, once with DMMA tiles of three real products per complex block, once
+      // with those tiles staging C in shared memory
+      constexpr int NP = 4;
+      cudaEvent_t pe[2 * NP];
       for (auto &x : pe) SS_CK(cudaEventCreate(&x));
-      float pt[3] = {0, 0, 0};
-      for (int c = 0; c < 3; ++c) {
+      float pt[NP] = {0, 0, 0, 0};
+      for (int c = 0; c < NP; ++c) {
         P.panel_dmma = c;
         cudaEventRecord(pe[2 * c], h.stream);
         for (int l = 0; l < S.nlevel; ++l) {
@@ -2330,16 +2373,16 @@ struct Sweeper {
       }
       SS_CK(cudaGetLastError());
       SS_CK(cudaStreamSynchronize(h.stream));
-      for (int c = 0; c < 3; ++c) cudaEventElapsedTime(&pt[c], pe[2 * c], pe[2 * c + 1]);
+      for (int c = 0; c < NP; ++c) cudaEventElapsedTime(&pt[c], pe[2 * c], pe[2 * c + 1]);
       for (auto &x : pe) cudaEventDestroy(x);
       P.panel_dmma = 0;
-      for (int c = 1; c < 3; ++c)
+      for (int c = 1; c < NP; ++c)
         if (pt[c] < pt[P.panel_dmma]) P.panel_dmma = c;
-      for (int c = 0; c < 3; ++c) P.panel_ms[c] = pt[c];
+      for (int c = 0; c < NP; ++c) P.panel_ms[c] = pt[c];
       }
     } else {
       // a forced DMMA Schur tile puts the panel-step GEMMs on the same kind of tile
-      P.panel_dmma = sizeof(T) != 8 ? 0 : atoi(force) == 2 ? 1 : atoi(force) == 1 ? 2 : 0;
+      P.panel_dmma = sizeof(T) != 8 ? 0 : atoi(force) == 2 ? 1 : atoi(force) == 1 ? 2 : atoi(force) == 3 ? 3 : 0;
     }
     for (int l = 0; l < S.nlevel; ++l) {
       int best = 0;
@@ -2567,6 +2610,14 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
                                kPanelSmemMax));
     SS_CK(cudaFuncSetAttribute(front_assemble_rows_smem_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                kAsmSmemMax));
+    if constexpr (sizeof(T) == 8) {
+      SS_CK(cudaFuncSetAttribute(front_dmma3_kernel<2, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 dmma_cst_bytes<2, 2>()));
+      SS_CK(cudaFuncSetAttribute(front_dmma3_kernel<4, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 dmma_cst_bytes<4, 1>()));
+      SS_CK(cudaFuncSetAttribute(front_dmma3_kernel<1, 4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 dmma_cst_bytes<1, 4>()));
+    }
     SS_CK(cudaFuncSetAttribute(front_l21_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)l21_smem<T>(256)));
     SS_CK(cudaFuncSetAttribute(tc::tma_gemm_kernel<128, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2924,15 +2975,15 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
   h.st[30] = (double)steps_p;
   h.st[31] = (double)steps_a;
   h.st[32] = nfail;
-  h.st[20] = h.st[21] = h.st[22] = 0;
+  h.st[20] = h.st[21] = h.st[22] = h.st[36] = 0;
   h.st[23] = P.panel_dmma;
   h.st[24] = P.panel_ms[0];
-  h.st[25] = std::min(P.panel_ms[1], P.panel_ms[2]);
+  h.st[25] = std::min(std::min(P.panel_ms[1], P.panel_ms[2]), P.panel_ms[3]);
   h.st[26] = (double)P.fronts_small.size();
   h.st[27] = 0;
   for (float t : P.tune_ms) h.st[27] += t;
   for (size_t l = 0; l < P.pick.size(); ++l)
-    if (P.schur_ptr[l + 1] > P.schur_ptr[l]) h.st[20 + P.pick[l]] += 1;
+    if (P.schur_ptr[l + 1] > P.schur_ptr[l]) h.st[P.pick[l] == 3 ? 36 : 20 + P.pick[l]] += 1;
   {
     double tot = 0;
     if (iters)
@@ -3075,7 +3126,8 @@ __global__ void fill_hash_kernel(int64_t n, cplx<T> *x) {
 // 2 / 3 complex64 TMA + tcgen05 3xTF32 with 128 / 64-column tiles (operands
 // packed once before the timed launches), 5 FP64 DMMA 64x64 with three real
 // products per complex block,
-// 4 complex64 SIMT FP32 128x64.
+// 4 complex64 SIMT FP32 128x64, 6 FP64 DMMA 64x64 with three real products and
+// the C tile staged in shared memory.
 template <class T>
 static int measure_ceiling_impl(Handle &h, int kernel, int m, int k, int nb, int reps, double *tflops) {
   const int ld = (m + 3) / 4 * 4;
@@ -3085,7 +3137,7 @@ static int measure_ceiling_impl(Handle &h, int kernel, int m, int k, int nb, int
   std::vector<int> vld(1, ld);
   std::vector<int64_t> voff(1, 0);
   std::vector<GemmTask> tasks;
-  if (kernel == 0 || kernel == 5)
+  if (kernel == 0 || kernel == 5 || kernel == 6)
     add_tiles(tasks, kSquare64, 0, k, m, k, m, 0, k);
   else
     add_tiles(tasks, kSquare, 0, k, m, k, m, 0, k);
@@ -3143,6 +3195,8 @@ static int measure_ceiling_impl(Handle &h, int kernel, int m, int k, int nb, int
         front_dmma_kernel<2, 2><<<dim3(nt, nb), 128, 0, h.stream>>>(a, tk);
       else if (kernel == 5)
         front_dmma3_kernel<2, 2><<<dim3(nt, nb), 128, 0, h.stream>>>(a, tk);
+      else if (kernel == 6)
+        front_dmma3_kernel<2, 2, true><<<dim3(nt, nb), 128, dmma_cst_bytes<2, 2>(), h.stream>>>(a, tk);
       else
         front_gemm_kernel<T, kSquare><<<dim3(nt, nb), 256, 0, h.stream>>>(a, tk);
     } else {
@@ -3187,7 +3241,12 @@ static int measure_ceiling_impl(Handle &h, int kernel, int m, int k, int nb, int
 }
 
 int measure_ceiling(Handle &h, int kernel, int m, int k, int nb, int reps, double *tflops) {
-  if (kernel <= 1 || kernel == 5) return measure_ceiling_impl<double>(h, kernel, m, k, nb, reps, tflops);
+  if (kernel <= 1 || kernel == 5 || kernel == 6) {
+    cudaError_t e = cudaFuncSetAttribute(front_dmma3_kernel<2, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         dmma_cst_bytes<2, 2>());
+    if (e != cudaSuccess) return cuda_fail(h, e, "ceiling: shared memory attribute");
+    return measure_ceiling_impl<double>(h, kernel, m, k, nb, reps, tflops);
+  }
   return measure_ceiling_impl<float>(h, kernel, m, k, nb, reps, tflops);
 }
 

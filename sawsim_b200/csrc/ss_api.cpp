@@ -497,7 +497,7 @@ extern "C" int ss_adjoint_gradient(ss_handle *hp, int n_f, const double *omega, 
 extern "C" int ss_measure_gemm_ceiling(ss_handle *hp, int kernel, int m, int k, int n_fronts, int reps,
                                        double *tflops) {
   H_CHECK(hp);
-  if (!tflops || kernel < 0 || kernel > 5 || k <= 0 || m <= k || n_fronts <= 0 || reps <= 0 || reps > 1000)
+  if (!tflops || kernel < 0 || kernel > 6 || k <= 0 || m <= k || n_fronts <= 0 || reps <= 0 || reps > 1000)
     return fail(h, SS_EINVAL, "ceiling: bad arguments");
   if ((double)n_fronts * m * m * 16.0 > 64e9) return fail(h, SS_EINVAL, "ceiling: more than 64 GB of fronts");
   return measure_ceiling(h, kernel, m, k, n_fronts, reps, tflops);

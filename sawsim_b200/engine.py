@@ -299,7 +299,8 @@ class FrequencySolver:
                  'sweep_device_ms', 'refine_solves', 'precision_used', 'schur_candidate0', 'schur_candidate1',
                  'schur_candidate2', 'panel_gemm_dmma', 'panel_tune_simt_ms', 'panel_tune_dmma_ms', 'small_fronts',
                  'schur_tune_ms', 'auto_probe_ms', 'fp64_resolved', 'krylov_steps_primal', 'krylov_steps_adjoint',
-                 'mixed_not_converged', 'fp64_resolve_ms', 'element_kernel_ms', 'scatter_kernel_ms']
+                 'mixed_not_converged', 'fp64_resolve_ms', 'element_kernel_ms', 'scatter_kernel_ms',
+                 'schur_candidate3']
 
     def stats(self) -> dict:
         n = len(self.STAT_KEYS)
@@ -311,7 +312,8 @@ class FrequencySolver:
         """Measured algorithmic TFLOP/s of a Schur-update kernel on dense fronts
         (``ss_measure_gemm_ceiling``; kernel 0 FP64 DMMA, 1 FP64 SIMT, 2 / 3
         complex64 TMA + tcgen05 3xTF32 with 128 / 64-column tiles, 4 complex64
-        SIMT FP32, 5 FP64 DMMA with three real products per complex block)."""
+        SIMT FP32, 5 FP64 DMMA with three real products per complex block, 6 the
+        same with the C tile staged in shared memory)."""
         out = C.c_double()
         self._h('ss_measure_gemm_ceiling', int(kernel), int(m), int(k), int(n_fronts), int(reps), C.byref(out))
         return out.value

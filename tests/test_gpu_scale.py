@@ -72,11 +72,12 @@ def test_mixed_matches_fp64(mid):
         assert d[key] is None or abs(d[key]) <= 1e-3
 
 
-@pytest.mark.parametrize('tile', [0, 1, 2])
+@pytest.mark.parametrize('tile', [0, 1, 2, 3])
 def test_every_schur_tile_candidate_is_exact(mid, tile, monkeypatch):
     """The autotuner's FP64 candidates (SIMT 128x64; FP64 tensor-core DMMA 64x64 with
-    three or four real products per complex block; a forced DMMA tile also puts the
-    panel-step GEMMs on DMMA tiles of its kind), each forced on every level, give the same
+    three or four real products per complex block; three products with the C tile
+    staged in shared memory; a forced DMMA tile also puts the panel-step GEMMs on
+    DMMA tiles of its kind), each forced on every level, give the same
     charges as the default choice, and each solution has a backward error below
     1e-12 in the oracle's system."""
     case, o, g = mid
@@ -93,10 +94,10 @@ def test_every_schur_tile_candidate_is_exact(mid, tile, monkeypatch):
     finally:
         e.close()
     assert (st == 0).all()
-    counts = [s['schur_candidate0'], s['schur_candidate1'], s['schur_candidate2']]
+    counts = [s['schur_candidate0'], s['schur_candidate1'], s['schur_candidate2'], s['schur_candidate3']]
     assert counts[tile] > 0 and sum(counts) == counts[tile]
     # a forced DMMA Schur tile puts the panel-step GEMMs on the same kind of tile
-    assert s['panel_gemm_dmma'] == {0: 0.0, 1: 2.0, 2: 1.0}[tile]
+    assert s['panel_gemm_dmma'] == {0: 0.0, 1: 2.0, 2: 1.0, 3: 3.0}[tile]
     assert _backward_error(A, disp[o.active], rhs) < 1e-12
     assert np.max(np.abs(Q - Q0) / np.abs(Q0)) < 1e-9
 
