@@ -231,7 +231,8 @@ int ss_adjoint_gradient(ss_handle *h, int n_f, const double *omega, double V, in
  *  sweep: packed operands + TMA + tcgen05 3xTF32 with 128 / 64 complex columns
  *  per tile, SIMT FP32 128x64),
  *  23 panel-step GEMM tiles (128x32 / 32x128): 0 SIMT, 1 DMMA, 2 DMMA with
- *  three real products per complex block, 3 the same with C staged, 24-25 autotuner time of all
+ *  three real products per complex block, 3 the same with C staged, 4 SIMT
+ *  with C staged (complex64), 24-25 autotuner time of all
  *  panel-step GEMMs with SIMT / the faster DMMA tiles (ms),
  *  26 fronts factored whole in shared memory, 27 autotuner time of all
  *  Schur candidates (ms, sum over candidates and levels),

@@ -890,23 +890,44 @@ static inline int tile_bm(int s) { return s == kSquare ? 128 : s == kSkinny ? 25
 static inline int tile_bn(int s) { return s == kSquare ? 64 : s == kSkinny ? 32 : s == kShort ? 256 : 64; }
 
 // One BMxBN complex tile of C -= A B per CTA, TMxTN outputs per thread; K in
-// chunks of 8 with the next chunk prefetched into registers.
+// chunks of 8 with the next chunk prefetched into registers.  CST: the C tile is
+// copied into shared memory by cp.async when the CTA starts (row stride BN + 1),
+// so that its latency overlaps the K loop (dynamic shared memory gemm_cst_bytes).
 template <class T, int S>
+constexpr int gemm_cst_bytes() { return Tile<S>::BM * (Tile<S>::BN + 1) * (int)sizeof(cplx<T>); }
+template <class T, int S, bool CST = false>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) front_gemm_kernel(FrontArgs<T> a,
                                                                                 const GemmTask *__restrict__ tasks) {
   constexpr int BM = Tile<S>::BM, BN = Tile<S>::BN, TM = Tile<S>::TM, TN = Tile<S>::TN, BK = kGemmBK;
-  constexpr int TX = BN / TN, TY = BM / TM;
+  constexpr int TX = BN / TN, TY = BM / TM, CS = BN + 1;
   static_assert(TX * TY == 256, "256 threads");
   constexpr int NA = BM * BK / 256, NBt = BN * BK / 256;
   // A rows padded by 4: the transposing stores (8 k values x 4 rows per warp) hit
   // 32 distinct slots
   __shared__ cplx<T> As[BK][BM + 4];
   __shared__ cplx<T> Bs[BK][BN];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   const GemmTask tk = tasks[blockIdx.x];
   const int fq = blockIdx.y;
   const int ld = a.ld[tk.f];
   cplx<T> *F = a.arena + (int64_t)fq * a.stride + a.off[tk.f];
   const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
+  cplx<T> *Cs = reinterpret_cast<cplx<T> *>(smem_raw);
+  if constexpr (CST) {
+    constexpr uint32_t EB = sizeof(cplx<T>);
+    for (int idx = threadIdx.x; idx < BM * BN; idx += 256) {
+      const int r = idx / BN, c = idx % BN;
+      const int gr = tk.r0 + r, gc = tk.c0 + c;
+      const bool ok = gr < tk.rhi && gc < tk.chi;
+      const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&Cs[r * CS + c]);
+      const void *src = ok ? (const void *)(F + (int64_t)gr * ld + gc) : (const void *)F;
+      if constexpr (EB == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(ok ? 16u : 0u) : "memory");
+      else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(ok ? 8u : 0u) : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
   cplx<T> acc[TM][TN];
 #pragma unroll
   for (int i = 0; i < TM; ++i)
@@ -958,6 +979,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) front_gemm_kernel
     }
     __syncthreads();
   }
+  if constexpr (CST) {
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
+  }
   // epilogue: per output row, all TN loads of C first, then the stores
 #pragma unroll
   for (int i = 0; i < TM; ++i) {
@@ -968,7 +993,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) front_gemm_kernel
 #pragma unroll
     for (int j = 0; j < TN; ++j) {
       const int c = tk.c0 + tx + TX * j;
-      cv[j] = (rok && c < tk.chi) ? Fr[c] : cplx<T>{0, 0};
+      if constexpr (CST)
+        cv[j] = Cs[(ty + TY * i) * CS + tx + TX * j];
+      else
+        cv[j] = (rok && c < tk.chi) ? Fr[c] : cplx<T>{0, 0};
     }
 #pragma unroll
     for (int j = 0; j < TN; ++j) {
@@ -1744,6 +1772,7 @@ struct Plan {
                                            // real products per complex block, 3 the same with the
                                            // C tile staged (tuned once per plan)
   float panel_ms[4] = {0, 0, 0, 0};        // tuner's panel-GEMM times: SIMT, DMMA, DMMA 3M, DMMA 3M C staged
+  bool panel_cst = false;                  // complex64 SIMT panel-step tiles stage C (tuned once per plan)
   std::vector<char> pick;                  // per level candidate
   std::vector<float> tune_ms;              // [candidate][level] measured times
   bool tuned = true;
@@ -2263,10 +2292,18 @@ struct Sweeper {
     }
     const int64_t t0 = P.step_ptr[q + which], t1 = P.step_ptr[q + which + 1];
     if (t1 == t0) return;
-    if (which == 0)
-      front_gemm_kernel<T, kSkinny><<<dim3((unsigned)(t1 - t0), nb), 256, 0, h.stream>>>(b, tasks + t0);
-    else
-      front_gemm_kernel<T, kShort><<<dim3((unsigned)(t1 - t0), nb), 256, 0, h.stream>>>(b, tasks + t0);
+    const dim3 grid((unsigned)(t1 - t0), nb);
+    if (P.panel_cst) {
+      if (which == 0)
+        front_gemm_kernel<T, kSkinny, true><<<grid, 256, gemm_cst_bytes<T, kSkinny>(), h.stream>>>(b, tasks + t0);
+      else
+        front_gemm_kernel<T, kShort, true><<<grid, 256, gemm_cst_bytes<T, kShort>(), h.stream>>>(b, tasks + t0);
+    } else {
+      if (which == 0)
+        front_gemm_kernel<T, kSkinny><<<grid, 256, 0, h.stream>>>(b, tasks + t0);
+      else
+        front_gemm_kernel<T, kShort><<<grid, 256, 0, h.stream>>>(b, tasks + t0);
+    }
   }
 
   // FP64 Schur update of level l with candidate tile c (0 SIMT 128x64, 1 DMMA
@@ -2379,10 +2416,40 @@ struct Sweeper {
       for (int c = 1; c < NP; ++c)
         if (pt[c] < pt[P.panel_dmma]) P.panel_dmma = c;
       for (int c = 0; c < NP; ++c) P.panel_ms[c] = pt[c];
+      } else {
+      // panel-step GEMMs (complex64, SIMT tiles): once reading C after the K loop,
+      // once with C staged in shared memory while it runs
+      cudaEvent_t pe[4];
+      for (auto &x : pe) SS_CK(cudaEventCreate(&x));
+      float pt[2] = {0, 0};
+      for (int c = 0; c < 2; ++c) {
+        P.panel_cst = c == 1;
+        cudaEventRecord(pe[2 * c], h.stream);
+        for (int l = 0; l < S.nlevel; ++l) {
+          FrontArgs<T> b = a;
+          b.fronts = P.d_large.as<int>() + P.large_ptr[l];
+          for (int st = 0; st < P.nsteps[l]; ++st) {
+            const int64_t q = P.level_step0[l] + 2 * st;
+            panel_gemm(b, q, 0, nb);
+            panel_gemm(b, q, 1, nb);
+          }
+        }
+        cudaEventRecord(pe[2 * c + 1], h.stream);
+      }
+      SS_CK(cudaGetLastError());
+      SS_CK(cudaStreamSynchronize(h.stream));
+      for (int c = 0; c < 2; ++c) cudaEventElapsedTime(&pt[c], pe[2 * c], pe[2 * c + 1]);
+      for (auto &x : pe) cudaEventDestroy(x);
+      P.panel_cst = pt[1] < pt[0];
+      P.panel_ms[0] = pt[0];
+      P.panel_ms[3] = pt[1];
       }
     } else {
       // a forced DMMA Schur tile puts the panel-step GEMMs on the same kind of tile
       P.panel_dmma = sizeof(T) != 8 ? 0 : atoi(force) == 2 ? 1 : atoi(force) == 1 ? 2 : atoi(force) == 3 ? 3 : 0;
+    }
+    if constexpr (sizeof(T) == 4) {
+      if (const char *e = getenv("SS_PANEL_CST")) P.panel_cst = atoi(e) != 0;   // measurement override
     }
     for (int l = 0; l < S.nlevel; ++l) {
       int best = 0;
@@ -2610,6 +2677,10 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
                                kPanelSmemMax));
     SS_CK(cudaFuncSetAttribute(front_assemble_rows_smem_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                kAsmSmemMax));
+    SS_CK(cudaFuncSetAttribute(front_gemm_kernel<T, kSkinny, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               gemm_cst_bytes<T, kSkinny>()));
+    SS_CK(cudaFuncSetAttribute(front_gemm_kernel<T, kShort, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               gemm_cst_bytes<T, kShort>()));
     if constexpr (sizeof(T) == 8) {
       SS_CK(cudaFuncSetAttribute(front_dmma3_kernel<2, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  dmma_cst_bytes<2, 2>()));
@@ -2976,7 +3047,7 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
   h.st[31] = (double)steps_a;
   h.st[32] = nfail;
   h.st[20] = h.st[21] = h.st[22] = h.st[36] = 0;
-  h.st[23] = P.panel_dmma;
+  h.st[23] = P.panel_cst ? 4 : P.panel_dmma;
   h.st[24] = P.panel_ms[0];
   h.st[25] = std::min(std::min(P.panel_ms[1], P.panel_ms[2]), P.panel_ms[3]);
   h.st[26] = (double)P.fronts_small.size();

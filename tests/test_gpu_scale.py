@@ -172,3 +172,23 @@ def test_l21_forms_agree_bit_for_bit(mid, precision, monkeypatch):
         assert (st == 0).all()
         Q.append(q)
     assert np.array_equal(Q[0], Q[1])
+
+
+def test_complex64_panel_tiles_with_staged_c_agree_bit_for_bit(mid, monkeypatch):
+    """The complex64 panel-step GEMM tiles read C after their K loop or from a copy
+    staged in shared memory during it: the same arithmetic, identical charges."""
+    case, _, _ = mid
+    w = 2 * np.pi * np.linspace(case.freqs[0], case.freqs[-1], 4)
+    monkeypatch.setenv('SS_SCHUR_TILE_C64', '0')
+    Q = []
+    for cst in ('0', '1'):
+        monkeypatch.setenv('SS_PANEL_CST', cst)
+        e = cases.engine_for(case)
+        try:
+            q, st, _ = e.charges(w, 1.0, 'mixed')
+            assert e.stats()['panel_gemm_dmma'] == (4.0 if cst == '1' else 0.0)
+        finally:
+            e.close()
+        assert (st == 0).all()
+        Q.append(q)
+    assert np.array_equal(Q[0], Q[1])
