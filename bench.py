@@ -542,8 +542,10 @@ def gradient_arm(a):
     d = fa - fr
     f = np.linspace(fr - 0.25 * d, fa + 0.25 * d, a.points or 64)
     t = time.perf_counter()
-    Y, dY, st = autograd.y11_and_jacobian(model, v, f, a.precision)
+    es = {}
+    Y, dY, st = autograd.y11_and_jacobian(model, v, f, a.precision, stats=es)
     wall = time.perf_counter() - t
+    used = 'mixed' if int(es.get('precision_used', 0)) == 1 else 'fp64'
     # central differences (relative step 1e-5, FP64 sweeps) of two parameters at two points
     idx = [int(np.argmin(np.abs(f - fr))), int(np.argmin(np.abs(f - fa)))]
     checks = []
@@ -559,9 +561,10 @@ def gradient_arm(a):
                                                           for q, i in enumerate(idx)]))
     return dict(metric='Y11 and dY11/dp points/s (adjoint)', value=f.size / wall, unit='points/s', n_gpus=1,
                 steps=1, warmup=0, higher_is_better=True, scaling='weak', vs_baseline=None,
-                dtype='c64+f64' if a.precision != 'fp64' else 'c128', data='synthetic',
+                dtype='c64+f64' if used == 'mixed' else 'c128', data='synthetic',
                 config=dict(workload=f'{a.case} parametrised ({type(model).__name__}), {f.size} points spanning fr..fa',
                             n_params=len(model.names), params=model.names, precision=a.precision,
+                            precision_used=used,
                             fr_ghz=r['fr_ghz'], fa_ghz=r['fa_ghz'], points_not_converged=int(np.sum(st != 0)),
                             wall_s_including_engine_build=wall, fd_checks=checks))
 

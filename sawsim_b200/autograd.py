@@ -16,16 +16,19 @@ import torch
 from . import cases
 
 
-def y11_and_jacobian(model, params, freqs, precision='fp64', V=1.0, device=0):
+def y11_and_jacobian(model, params, freqs, precision='fp64', V=1.0, device=0, stats=None):
     """(Y[n_f], dY/dp[n_f, n_params], status) at parameters ``params`` of a
     ``params.Q9Model`` or ``params.HexModel`` (the model fixes the Y11 sign and
-    normalisation of its pipeline)."""
+    normalisation of its pipeline).  A dict passed as ``stats`` receives the
+    engine's counters (``FrequencySolver.stats``) of the run."""
     p = np.asarray(params, dtype=float)
     case = model.build(p)
     eng = model.engine(case, device=device)
     try:
         w = 2 * np.pi * np.asarray(freqs, dtype=float)
         Q, dQ, st = eng.gradient(w, model.seeds(p), V, precision)
+        if stats is not None:
+            stats.update(eng.stats())
     finally:
         eng.close()
     Y = model.y11(w, Q, V, case)
