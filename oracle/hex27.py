@@ -15,7 +15,8 @@ Restates the reference's 2.5D slab path (src/sawsim/saw2d/saw3d/):
 * boundary sets and the periodic DOF lists: ``boundary.py:32-148``;
 * two-stage fold (front/back, then left/right), prescribed DOFs, the
   per-frequency solve and Q = sum over the + electrode rows of the unfolded K
-  times disp: ``bc_solve.py:25-175``.
+  times disp: ``bc_solve.py:25-175``; the finite-device variant (front/back, then
+  the floating electrodes' equipotential fold): ``bc_solve.py:214-335``.
 
 Element matrices are formed per element from gradient Grams (the reference forms
 global B^T D B products); the two agree to rounding.
@@ -261,3 +262,60 @@ class FrequencySolver3D:
 
     def sweep(self, freqs, V=1.0):
         return np.array([self.solve(2 * np.pi * f, V)[1] for f in np.asarray(freqs, float)])
+
+
+class FrequencySolver3DFP(FrequencySolver3D):
+    """bc_solve.FrequencySolver3D_FP (bc_solve.py:214-335): the finite-device variant.
+    Front/back fold, then the equipotential fold of the floating electrodes XFL / XFR
+    (each node's phi onto the set's first node); no left/right periodicity.
+    ``boundary`` = (machine, electric) dicts with electric['XFL'], ['XFR']."""
+
+    def __init__(self, K, M, boundary):
+        m, e = boundary
+        self.K = K.tocsr()
+        self.gdof = K.shape[0]
+        t_fb = _fold(np.concatenate([m['period_B'], e['period_B']]), np.concatenate([m['period_F'], e['period_F']]),
+                     self.gdof)
+        t_fl = float_fold(e, self.gdof)
+        kf = (t_fl.T @ (t_fb.T @ self.K @ t_fb) @ t_fl).tocsr()
+        mf = (t_fl.T @ (t_fb.T @ M.tocsr() @ t_fb) @ t_fl).tocsr()
+        xfl, xfr = e['XFL'], e['XFR']
+        prescribed = np.unique(np.concatenate([m['fix'], m['period_B'], e['period_B'], xfl[1:], xfr[1:],
+                                               e['zheng'], e['fu']]))
+        self.active = np.setdiff1d(np.arange(self.gdof), prescribed)
+        self.n_active = self.active.size
+        self.zheng, self.fu, self.m, self.e = e['zheng'], e['fu'], m, e
+        self.k_aa = kf[self.active][:, self.active].tocsr()
+        self.m_aa = mf[self.active][:, self.active].tocsr()
+        self.k_az = kf[self.active][:, self.zheng]
+        self.m_az = mf[self.active][:, self.zheng]
+        self.kz_rows = self.K[self.zheng, :].tocsr()
+
+    def solve(self, omega, V=1.0):
+        A, rhs = self.system(omega, V)
+        u = spla.splu(A.tocsc()).solve(rhs)
+        disp = np.zeros(self.gdof, complex)
+        disp[self.active] = u
+        m, e = self.m, self.e
+        disp[m['period_B']] = disp[m['period_F']]            # bc_solve.py:242-253
+        disp[e['period_B']] = disp[e['period_F']]
+        for xs in (e['XFL'], e['XFR']):
+            if xs.size > 1:
+                disp[xs[1:]] = disp[xs[0]]
+        disp[self.zheng] = V
+        disp[self.fu] = 0.0
+        Q = (self.kz_rows @ disp).sum()
+        return disp, Q, abs(1j * omega * Q / V)
+
+
+def float_fold(e, gdof):
+    """The equipotential fold operator of bc_solve.py:219-231 (XFL / XFR slaves onto
+    their first node)."""
+    s, mst = [], []
+    for xs in (e['XFL'], e['XFR']):
+        if xs.size > 1:
+            s.append(xs[1:])
+            mst.append(np.full(xs.size - 1, xs[0]))
+    slaves = np.concatenate(s) if s else np.zeros(0, np.int64)
+    masters = np.concatenate(mst) if mst else np.zeros(0, np.int64)
+    return _fold(slaves, masters, gdof)

@@ -32,12 +32,26 @@ sys.path.insert(0, str(Path(os.environ.get('SAWSIM_REFERENCE', '/root/reference'
 sys.modules.setdefault('gmsh', types.ModuleType('gmsh'))
 
 from sawsim.saw2d.saw3d.assembly import form_stiffness_mass_3d          # noqa: E402
-from sawsim.saw2d.saw3d.bc_solve import FrequencySolver3D, build_periodic_operators  # noqa: E402
+from sawsim.saw2d.saw3d.bc_solve import (FrequencySolver3D, FrequencySolver3D_FP,  # noqa: E402
+                                         build_periodic_operators, build_periodic_operators_fp)
 from sawsim.saw2d.saw3d.boundary import boundary_idx_vect_3ds            # noqa: E402
 
 from sawsim_b200 import cases                                            # noqa: E402
 
 SMALL = [(8, 1, 6, 4), (8, 2, 12, 3)]
+FP = (8, 2, 12, 3)      # slab of the finite-device fixture
+
+
+def floating_strips(c):
+    """Synthetic floating electrodes on the slab: the substrate-surface nodes (z = 0)
+    outside the driven pair and the front/back faces, in the outer tenth of the cell
+    on either side (XFL, XFR); phi DOFs at 3N + node, ascending."""
+    P, S = c.pos_m, c.cell.sets
+    surf = np.where(np.isclose(P[:, 2], 0.0))[0]
+    free = np.setdiff1d(surf, np.concatenate([S['zheng'], S['fu'], S['front'], S['back']]))
+    w = P[:, 0].max()
+    gu = 3 * c.N
+    return np.sort(free[P[free, 0] < 0.1 * w]) + gu, np.sort(free[P[free, 0] > 0.9 * w]) + gu
 
 
 def reference_inputs(c):
@@ -72,6 +86,17 @@ def main():
                             kaa_w=eng.k_aa @ w, maa_w=eng.m_aa @ w, active=eng.active, frequency_hz=c.freqs, Q=Q,
                             **lists)
         print(nx, ny, nz, 'nodes', c.N, 'K nnz', K.nnz, 'active', eng.n_act)
+        if (nx, ny, nz, nf) == FP:
+            # the finite-device solver (bc_solve.py:214-335) on the same slab with two
+            # floating strips added to the electric sets
+            xfl, xfr = floating_strips(c)
+            bnd.electric['XFL'], bnd.electric['XFR'] = xfl, xfr
+            tfb, tfl = build_periodic_operators_fp(bnd, 4 * c.N)
+            fp = FrequencySolver3D_FP(K, M, bnd, tfb, tfl)
+            Qfp = np.array([fp.solve(2 * np.pi * f, 1.0)[1] for f in c.freqs])
+            np.savez_compressed(HERE / f'ref_hex_fp_{nx}x{ny}x{nz}.npz', XFL=xfl, XFR=xfr, active=fp.active,
+                                frequency_hz=c.freqs, Q=Qfp)
+            print('finite device: active', fp.n_act)
 
 
 if __name__ == '__main__':

@@ -183,3 +183,39 @@ def test_hex_matrix_input_matches_oracle(built_lib, ordering):
         assert _backward_error(A, disp[o.active], rhs) < 1e-12
     finally:
         g.close()
+
+
+def test_hex_finite_device_matrix_input_matches_oracle(built_lib):
+    """``FrequencySolver3D_FP(K, M, boundary, t_fb, t_float)`` (bc_solve.py:214-335): the
+    finite-device variant, front/back periodic only, with two floating electrodes whose
+    potentials fold onto one DOF each.  Its fold operators go to ``from_matrices_3d``
+    unchanged.  The floating strips are the reference fixture's (surface nodes beside
+    the driven pair: a synthetic finite device on the slab mesh, ref_hex_fp_8x2x12.npz)."""
+    from conftest import GOLDEN
+    from test_gpu_hex import _oracle
+    c = cases.make_hex_case('hex_8x4x48', nx=8, ny=2, nz=12, points=3)
+    ref = np.load(GOLDEN / 'ref_hex_fp_8x2x12.npz')
+    K, M, _ = _oracle(c)
+    m, e = oh.boundary_idx_vect_3ds(c.cell.sets, c.pos_m, 3 * c.N)
+    e = dict(e, XFL=ref['XFL'], XFR=ref['XFR'])
+    o = oh.FrequencySolver3DFP(K, M, (m, e))
+    t_fb = oh._fold(np.concatenate([m['period_B'], e['period_B']]), np.concatenate([m['period_F'], e['period_F']]),
+                    K.shape[0])
+    t_float = oh.float_fold(e, K.shape[0])
+    g = FrequencySolver.from_matrices_3d(K, M, (m, e), t_fb, t_float)
+    try:
+        assert g.n_active == o.n_active
+        Q, st, _ = g.charges(2 * np.pi * c.freqs, 1.0, 'fp64')
+        assert (st == 0).all()
+        Qo = o.sweep(c.freqs)
+        assert np.max(np.abs(Q - Qo) / np.abs(Qo)) < 2e-5
+        assert np.max(np.abs(Q - ref['Q']) / np.abs(ref['Q'])) < 2e-5      # the reference's own solver
+        w0 = 2 * np.pi * c.freqs[1]
+        A, rhs = o.system(w0)
+        disp, _, _ = g.solve(w0)
+        assert _backward_error(A, disp[o.active], rhs) < 1e-12
+        # the floating electrodes are equipotential
+        for xs in (e['XFL'], e['XFR']):
+            assert np.allclose(disp[xs], disp[xs[0]], rtol=0, atol=0)
+    finally:
+        g.close()

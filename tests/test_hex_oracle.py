@@ -96,3 +96,20 @@ def test_four_layer_slab_pairs_match_coordinates():
     assert np.allclose(P[s[fb], 1] - P[m[fb], 1], c.cell.aperture_um * 1e-6, atol=1e-13)
     assert np.allclose(P[m[lr]][:, [1, 2]], P[s[lr]][:, [1, 2]], atol=1e-13)
     assert np.allclose(P[s[lr], 0] - P[m[lr], 0], c.cell.period_um * 1e-6, atol=1e-13)
+
+
+def test_finite_device_solver_matches_reference():
+    """The oracle's finite-device solver (front/back fold, then the floating
+    electrodes' equipotential fold) against the reference's FrequencySolver3D_FP
+    (bc_solve.py:214-335) on the 8x2x12 slab with two floating strips
+    (ref_hex_fp_8x2x12.npz)."""
+    c = cases.make_hex_case('hex_8x4x48', nx=8, ny=2, nz=12, points=3)
+    g = np.load(GOLDEN / 'ref_hex_fp_8x2x12.npz')
+    mats, pml = _inputs(c)
+    M, K = oh.form_stiffness_mass_3d(c.hexas, c.pos_m, mats, pml, c.omega_top)
+    m, e = oh.boundary_idx_vect_3ds(c.cell.sets, c.pos_m, 3 * c.N)
+    e = dict(e, XFL=g['XFL'], XFR=g['XFR'])
+    eng = oh.FrequencySolver3DFP(K, M, (m, e))
+    assert np.array_equal(eng.active, g['active'])
+    Q = eng.sweep(g['frequency_hz'])
+    assert np.max(np.abs(Q - g['Q']) / np.abs(g['Q'])) < 2e-5
