@@ -640,14 +640,15 @@ __device__ __forceinline__ void l21_row(cplx<T> *row, int w, const cplx<T> (*U)[
   }
 }
 
-// STAGED: each warp stages its 32 rows of the panel columns in shared memory with
-// coalesced loads (lane = column), solves them with lane = row, and writes them
-// back coalesced.  Otherwise each thread works on its row in global memory (a
-// warp's loads then touch 32 rows at once).  The arithmetic is the same.  Staging
-// is the default for complex64 (Hex27 slab mixed sweep 140.2 vs 132.0 points/s);
-// complex128 keeps the direct form (77.5 vs 77.2 points/s on the ME1 cell: its
-// staged tiles take 135 KB per 256-thread CTA); SS_L21_STAGED=0|1 overrides.
-template <class T, bool STAGED>
+// RPW > 0 (staged): each warp stages RPW rows of the panel columns in shared memory
+// with coalesced loads (lane = column), solves them with lanes 0..RPW-1 = rows,
+// and writes them back coalesced.  RPW = 0: each thread works on its row in global
+// memory (a warp's loads then touch 32 rows at once).  The arithmetic is the same.
+// Defaults (measured): 32 staged rows per warp for complex64 (Hex27 slab mixed sweep
+// 139.6 points/s, 137.3 with 16, 132.0 direct); 16 for complex128, whose 32-row tiles
+// take 135 KB per 256-thread CTA (ME1 FP64 sweep 80.2 points/s, 79.1 with 32, 79.4
+// direct); SS_L21_STAGED=0|16|32 overrides.
+template <class T, int RPW>
 __global__ void __launch_bounds__(256) front_l21_kernel(FrontArgs<T> a, int j0) {
   constexpr int TS = kPanel + 1;            // staged tile row stride (conflict-free)
   __shared__ cplx<T> U[kPanel][kPanel];
@@ -663,15 +664,15 @@ __global__ void __launch_bounds__(256) front_l21_kernel(FrontArgs<T> a, int j0) 
   if (threadIdx.x < w) Uinv[threadIdx.x] = cdiv(cplx<T>{1, 0}, U[threadIdx.x][threadIdx.x]);
   __syncthreads();
   cplx<T> *F = a.arena + (int64_t)fq * a.stride + a.off[f];
-  if constexpr (!STAGED) {
+  if constexpr (RPW == 0) {
     const int r = k + blockIdx.z * blockDim.x + threadIdx.x;
     if (r < m) l21_row<T>(F + (int64_t)r * ld + j0, w, U, Uinv);
   } else {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int rw = k + blockIdx.z * blockDim.x + wid * 32;
+    const int rw = k + blockIdx.z * (blockDim.x / 32) * RPW + wid * RPW;
     if (rw >= m) return;
-    const int nr = min(32, m - rw);
-    cplx<T> *tile = reinterpret_cast<cplx<T> *>(smem_raw) + wid * 32 * TS;
+    const int nr = min(RPW, m - rw);
+    cplx<T> *tile = reinterpret_cast<cplx<T> *>(smem_raw) + wid * RPW * TS;
     cplx<T> *gp = F + (int64_t)rw * ld + j0;
     if (lane < w) {
 #pragma unroll 8
@@ -687,13 +688,18 @@ __global__ void __launch_bounds__(256) front_l21_kernel(FrontArgs<T> a, int j0) 
   }
 }
 template <class T>
-static inline bool l21_staged() {
-  if (const char *e = getenv("SS_L21_STAGED")) return atoi(e) != 0;
-  return sizeof(T) == 4;
+static inline int l21_rpw() {
+  if (const char *e = getenv("SS_L21_STAGED")) {
+    const int v = atoi(e);
+    return v >= 32 ? 32 : v >= 16 ? 16 : 0;
+  }
+  return sizeof(T) == 4 ? 32 : 16;
 }
-// dynamic shared memory of front_l21_kernel for a CTA of `threads` threads
+// dynamic shared memory of the staged front_l21_kernel (RPW rows per warp)
 template <class T>
-static inline size_t l21_smem(int threads) { return (size_t)(threads / 32) * 32 * (kPanel + 1) * sizeof(cplx<T>); }
+static inline size_t l21_smem(int threads, int rpw) {
+  return (size_t)(threads / 32) * rpw * (kPanel + 1) * sizeof(cplx<T>);
+}
 
 // Unblocked LU of panel columns [j0, j1) over the fully-summed rows [j0, k).
 template <class T>
@@ -2530,10 +2536,17 @@ struct Sweeper {
           front_panel_smem_kernel<T><<<dim3(nl, nb), pth, psm, h.stream>>>(b, j0);
         else
           front_panel_kernel<T><<<dim3(nl, nb), 256, 0, h.stream>>>(b, j0);
-        if (l21_staged<T>())
-          front_l21_kernel<T, true><<<dim3(nl, nb, zc), bs, l21_smem<T>(bs), h.stream>>>(b, j0);
-        else
-          front_l21_kernel<T, false><<<dim3(nl, nb, zc), bs, 0, h.stream>>>(b, j0);
+        const int rpw = l21_rpw<T>();
+        if (rpw > 0) {
+          // rows per CTA: (bs / 32) warps x rpw rows
+          const unsigned zl = (unsigned)((ml + (bs / 32) * rpw - 1) / ((bs / 32) * rpw));
+          if (rpw == 32)
+            front_l21_kernel<T, 32><<<dim3(nl, nb, zl), bs, l21_smem<T>(bs, 32), h.stream>>>(b, j0);
+          else
+            front_l21_kernel<T, 16><<<dim3(nl, nb, zl), bs, l21_smem<T>(bs, 16), h.stream>>>(b, j0);
+        } else {
+          front_l21_kernel<T, 0><<<dim3(nl, nb, zc), bs, 0, h.stream>>>(b, j0);
+        }
         front_swap_kernel<T><<<dim3(nl, nb, zc), bs, 0, h.stream>>>(b, j0);
         if (g2 > g1) {   // U row block <- earlier pivots
           panel_gemm(b, q, 1, nb);
@@ -2689,8 +2702,10 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
       SS_CK(cudaFuncSetAttribute(front_dmma3_kernel<1, 4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  dmma_cst_bytes<1, 4>()));
     }
-    SS_CK(cudaFuncSetAttribute(front_l21_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)l21_smem<T>(256)));
+    SS_CK(cudaFuncSetAttribute(front_l21_kernel<T, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)l21_smem<T>(256, 32)));
+    SS_CK(cudaFuncSetAttribute(front_l21_kernel<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)l21_smem<T>(256, 16)));
     SS_CK(cudaFuncSetAttribute(tc::tma_gemm_kernel<128, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                tc::TmaCfg<128, 2>::SMEM));
     SS_CK(cudaFuncSetAttribute(tc::tma_gemm_kernel<64, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,

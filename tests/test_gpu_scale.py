@@ -155,14 +155,15 @@ def test_assembly_kernels_agree_bit_for_bit(mid, precision, monkeypatch):
 
 @pytest.mark.parametrize('precision', ['fp64', 'mixed'])
 def test_l21_forms_agree_bit_for_bit(mid, precision, monkeypatch):
-    """The panel-column solve L21 = F21 U11^-1 staged through shared memory and in
-    place in global memory perform the same arithmetic: identical charges."""
+    """The panel-column solve L21 = F21 U11^-1 staged through shared memory (16 or 32
+    rows per warp) and in place in global memory perform the same arithmetic:
+    identical charges."""
     case, _, _ = mid
     w = 2 * np.pi * np.linspace(case.freqs[0], case.freqs[-1], 4)
     monkeypatch.setenv('SS_SCHUR_TILE', '2')
     monkeypatch.setenv('SS_SCHUR_TILE_C64', '0')
     Q = []
-    for staged in ('0', '1'):
+    for staged in ('0', '16', '32'):
         monkeypatch.setenv('SS_L21_STAGED', staged)
         e = cases.engine_for(case)
         try:
@@ -171,7 +172,7 @@ def test_l21_forms_agree_bit_for_bit(mid, precision, monkeypatch):
             e.close()
         assert (st == 0).all()
         Q.append(q)
-    assert np.array_equal(Q[0], Q[1])
+    assert np.array_equal(Q[0], Q[1]) and np.array_equal(Q[0], Q[2])
 
 
 def test_complex64_panel_tiles_with_staged_c_agree_bit_for_bit(mid, monkeypatch):
