@@ -752,7 +752,11 @@ __global__ void __launch_bounds__(256) front_panel_kernel(FrontArgs<T> a, int j0
 // The same panel LU with the panel block -- rows [j0, k) x columns [j0, j1) -- held
 // in shared memory (row stride kPanel + 1 complex: row and column walks are both
 // conflict-free); one warp per row for the multipliers and the rank-1 update.
-// Operation for operation the arithmetic of front_panel_kernel.
+// Operation for operation the arithmetic of front_panel_kernel.  The next column's
+// pivot search rides on the update: lane 0 of each warp (which updates column
+// j + 1) keeps the largest |F[r][j+1]| of its rows, and after the barrier a warp
+// shuffle picks the largest over the warps, lowest row on ties, as a block-wide
+// argmax over the updated column would.
 constexpr int kPanelThreads = 512;
 constexpr int kPanelSmemMax = 224 * 1024;
 template <class T>
@@ -770,11 +774,13 @@ __global__ void __launch_bounds__(kPanelThreads) front_panel_smem_kernel(FrontAr
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   cplx<T> *F = a.arena + (int64_t)fq * a.stride + a.off[f] + (int64_t)j0 * ld + j0;
   int *piv = a.piv + (int64_t)fq * a.n + a.p0[f] + j0;
+  __shared__ T s_cv[2][kPanelThreads / 32];      // per-warp pivot candidates, by column parity
+  __shared__ int s_ci[2][kPanelThreads / 32];
   for (int r = wid; r < R; r += nw)
     if (lane < w) P[r * PS + lane] = F[(int64_t)r * ld + lane];
   __syncthreads();
+  int p = block_argmax<T>(0, R, [&](int r) { return P[r * PS]; }, s_v, s_i);
   for (int j = 0; j < w; ++j) {
-    const int p = block_argmax<T>(j, R, [&](int r) { return P[r * PS + j]; }, s_v, s_i);
     if (p != j) {   // p is the same in every thread
       if (threadIdx.x < w) {
         const cplx<T> t = P[j * PS + threadIdx.x];
@@ -797,14 +803,38 @@ __global__ void __launch_bounds__(kPanelThreads) front_panel_smem_kernel(FrontAr
     const cplx<T> inv = cdiv(cplx<T>{1, 0}, s_pivot);
     const int c = j + 1 + lane;
     const cplx<T> pc = c < w ? P[j * PS + c] : cplx<T>{0, 0};
+    T best = (T)-1;
+    int bi = j + 1;
     for (int r = j + 1 + wid; r < R; r += nw) {
       cplx<T> *row = P + r * PS;
       const cplx<T> l = cmul(row[j], inv);
-      if (c < w) row[c] = cfms(row[c], l, pc);
+      cplx<T> v{0, 0};
+      if (c < w) {
+        v = cfms(row[c], l, pc);
+        row[c] = v;
+      }
       __syncwarp();
-      if (lane == 0) row[j] = l;
+      if (lane == 0) {
+        row[j] = l;
+        const T av = cabs1(v);   // the updated F[r][j + 1] (c = j + 1 for lane 0)
+        if (j + 1 < w && av > best) best = av, bi = r;
+      }
+    }
+    if (lane == 0) {
+      s_cv[j & 1][wid] = best;
+      s_ci[j & 1][wid] = bi;
     }
     __syncthreads();
+    if (j + 1 < w) {
+      T bv = lane < nw ? s_cv[j & 1][lane] : (T)-1;
+      int bq = lane < nw ? s_ci[j & 1][lane] : j + 1;
+      for (int o = 16; o > 0; o >>= 1) {
+        const T ov = __shfl_xor_sync(0xffffffffu, bv, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bq, o);
+        if (ov > bv || (ov == bv && oi < bq)) bv = ov, bq = oi;
+      }
+      p = bq;
+    }
   }
   for (int r = wid; r < R; r += nw)
     if (lane < w) F[(int64_t)r * ld + lane] = P[r * PS + lane];
