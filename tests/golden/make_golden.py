@@ -18,7 +18,7 @@ It imports the reference's own modules (``sawsim.saw2d.piezo_fem``,
   Km_aa @ w, Mm_aa @ w, the active DOF list and the reference's Q at a few
   frequencies (SciPy SuperLU route, sweep.py:352-353).
 
-The fixtures are small; the GPU box never reads /root/reference.
+The fixtures are small; the tests read them, never the reference checkout.
 """
 from __future__ import annotations
 

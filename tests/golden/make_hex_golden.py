@@ -12,8 +12,8 @@ For small seeded slabs built by ``sawsim_b200.cells.hex_double_layer_slab``
 SciPy route) and records K @ v, M @ v for a seeded v, the periodic / prescribed
 DOF lists, the active set, k_aa @ w, m_aa @ w and Q at a few frequencies.  The
 reference's ``saw3d`` package imports gmsh at import time; a placeholder module
-stands in for it (no Gmsh call is made on this path).  The GPU box never reads
-/root/reference.
+stands in for it (no Gmsh call is made on this path).  The tests read the
+fixtures, never the reference checkout.
 """
 from __future__ import annotations
 

@@ -20,7 +20,7 @@ It records, with the reference's functions only:
   Euler angle at the seeded triples, the reference value of the d/dtheta
   tangent that the adjoint gradient seeds.
 
-The fixture is small; the GPU box never reads the reference.
+The fixture is small; the tests read it, never the reference checkout.
 """
 from __future__ import annotations
 

@@ -14,7 +14,7 @@ It feeds ``sawsim.metrics.resonances`` (src/sawsim/metrics.py:98-171) with
   capacitive background, plus band-edge and missing-antiresonance cases;
 
 and records the curves with the reference's fr_ghz / fa_ghz / k2eff / warning
-codes.  The GPU box never reads /root/reference.
+codes.  The tests read the fixture, never the reference checkout.
 """
 from __future__ import annotations
 
