@@ -13,8 +13,6 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from . import cases
-
 
 def y11_and_jacobian(model, params, freqs, precision='fp64', V=1.0, device=0, stats=None):
     """(Y[n_f], dY/dp[n_f, n_params], status) at parameters ``params`` of a
