@@ -520,7 +520,8 @@ def oracle_check(c, eng, case_name):
 def gradient_arm(a):
     """Y11 and dY11/dp by the adjoint (``autograd.y11_and_jacobian``) at points
     spanning fr..fa of a parametrised cell, with a central-difference check of
-    two parameters at two points (configs 4 and 5 of the gradient workload)."""
+    two parameters at two points (the four-layer ME1 128x512 cell and the
+    four-layer Hex27 12x6x80 slab)."""
     from sawsim_b200 import autograd, params
     from sawsim_b200.metrics import resonances
     models = {'me1_64x256': lambda: params.Q9Model(64, 256),

@@ -111,7 +111,8 @@ def _y_hex(model, v, f):
 
 @pytest.mark.parametrize('i', [0, 1], ids=['pitch_um', 't_film_um'])
 def test_hex_adjoint_matches_finite_differences(hex_jac, i):
-    """Hex27 slab (config-5 parameters: pitch and film thickness): the adjoint
+    """Hex27 slab (the parameters of the four-layer slab's gradient workload: pitch
+    and film thickness): the adjoint
     Jacobian of Y11 = +i w Q / V / aperture against central differences."""
     model, v, f, Y, dY = hex_jac
     fd = _fd(_y_hex, model, v, f, i)
