@@ -486,6 +486,11 @@ def b200_arm(a, rank, world, local):
                                 setup_s=setup_s, analyze_s=st0['analyze_s'], assemble_ms=st0['assemble_ms'],
                                 l2='inputs larger than L2 (front arena of GBs per chunk)',
                                 chunk=int(s['chunk']), points_not_converged=bad,
+                                panel_gemm=dict(tiles=int(s['panel_gemm_dmma']),
+                                                thin_tiles_per_point=int(s['panel_thin_tiles']),
+                                                note='0 SIMT, 1 DMMA, 2 DMMA three products, 3 the same with C '
+                                                     'staged, 4 SIMT with C staged; thin: tasks <= 8 wide in '
+                                                     'SIMT 128x8 / 8x128 tiles beside the DMMA ones'),
                                 mean_refinement_steps=float(np.mean(iters)),
                                 parallelism=f'interleaved frequency shards x{world}' if world > 1 else 'one GPU'),
                     e2e=dict(value=world * nf * a.steps / wall, unit='points/s', h2d_bytes_per_step=8 * nf,

@@ -244,7 +244,10 @@ int ss_adjoint_gradient(ss_handle *h, int n_f, const double *omega, double V, in
  *  element kernel / of the scatter into the CSR pattern of the last
  *  ss_assemble (ms, CUDA events), 36 levels whose FP64 Schur update uses
  *  candidate 3 (DMMA 64x64, three real products, C tile staged in shared
- *  memory while the K loop runs).  Slots past 36 read 0.
+ *  memory while the K loop runs), 37 panel-step GEMM tiles per point run as
+ *  thin SIMT 128x8 / 8x128 tiles (tasks at most 8 columns wide or 8 rows high,
+ *  beside the DMMA tiles; 0 when the autotuner kept them in DMMA tiles).
+ *  Slots past 37 read 0.
  */
 int ss_stats(const ss_handle *h, double *out, int n);
 

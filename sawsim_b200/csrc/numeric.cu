@@ -916,14 +916,22 @@ constexpr int kGemmBK = 8;
 // tile shapes: square (Schur update), skinny (panel column update), short (U row update)
 // tile shapes: square (Schur update; two candidates the autotuner picks from per
 // level), skinny (panel column update), short (U row update)
-enum GemmShape { kSquare = 0, kSkinny = 1, kShort = 2, kSquare64 = 3 };
+// thin column / row tiles: panel-step tasks at most 8 columns wide (panel columns)
+// or 8 rows high (U rows), e.g. a 4-pivot tail panel after a full 32-wide one
+enum GemmShape { kSquare = 0, kSkinny = 1, kShort = 2, kSquare64 = 3, kThinCol = 4, kThinRow = 5 };
 template <int S> struct Tile;
 template <> struct Tile<kSquare> { static constexpr int BM = 128, BN = 64, TM = 8, TN = 4; };
 template <> struct Tile<kSkinny> { static constexpr int BM = 256, BN = 32, TM = 8, TN = 4; };
 template <> struct Tile<kShort> { static constexpr int BM = 32, BN = 256, TM = 4, TN = 8; };
 template <> struct Tile<kSquare64> { static constexpr int BM = 64, BN = 64, TM = 4, TN = 4; };
-static inline int tile_bm(int s) { return s == kSquare ? 128 : s == kSkinny ? 256 : s == kShort ? 32 : 64; }
-static inline int tile_bn(int s) { return s == kSquare ? 64 : s == kSkinny ? 32 : s == kShort ? 256 : 64; }
+template <> struct Tile<kThinCol> { static constexpr int BM = 128, BN = 8, TM = 2, TN = 2; };
+template <> struct Tile<kThinRow> { static constexpr int BM = 8, BN = 128, TM = 2, TN = 2; };
+static inline int tile_bm(int s) {
+  return s == kSquare ? 128 : s == kSkinny ? 256 : s == kShort ? 32 : s == kThinCol ? 128 : s == kThinRow ? 8 : 64;
+}
+static inline int tile_bn(int s) {
+  return s == kSquare ? 64 : s == kSkinny ? 32 : s == kShort ? 256 : s == kThinCol ? 8 : s == kThinRow ? 128 : 64;
+}
 
 // One BMxBN complex tile of C -= A B per CTA, TMxTN outputs per thread; K in
 // chunks of 8 with the next chunk prefetched into registers.  CST: the C tile is
@@ -931,13 +939,17 @@ static inline int tile_bn(int s) { return s == kSquare ? 64 : s == kSkinny ? 32 
 // so that its latency overlaps the K loop (dynamic shared memory gemm_cst_bytes).
 template <class T, int S>
 constexpr int gemm_cst_bytes() { return Tile<S>::BM * (Tile<S>::BN + 1) * (int)sizeof(cplx<T>); }
+// (the thin tiles: four CTAs per SM, so that more tiles hide their load latency)
 template <class T, int S, bool CST = false>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) front_gemm_kernel(FrontArgs<T> a,
-                                                                                const GemmTask *__restrict__ tasks) {
+__global__ void __launch_bounds__(256, (S == kThinCol || S == kThinRow) ? 4 : sizeof(T) == 4 ? 2 : 1)
+    front_gemm_kernel(FrontArgs<T> a, const GemmTask *__restrict__ tasks) {
   constexpr int BM = Tile<S>::BM, BN = Tile<S>::BN, TM = Tile<S>::TM, TN = Tile<S>::TN, BK = kGemmBK;
   constexpr int TX = BN / TN, TY = BM / TM, CS = BN + 1;
   static_assert(TX * TY == 256, "256 threads");
-  constexpr int NA = BM * BK / 256, NBt = BN * BK / 256;
+  // staged A / B elements per thread; the thin tiles' narrow side has fewer than
+  // 256 elements per K chunk, so only the first BM*BK (BN*BK) threads load it
+  constexpr int NA = (BM * BK + 255) / 256, NBt = (BN * BK + 255) / 256;
+  constexpr bool A_ALL = BM * BK % 256 == 0, B_ALL = BN * BK % 256 == 0;
   // A rows padded by 4: the transposing stores (8 k values x 4 rows per warp) hit
   // 32 distinct slots
   __shared__ cplx<T> As[BK][BM + 4];
@@ -975,13 +987,13 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) front_gemm_kernel
     for (int q = 0; q < NA; ++q) {
       const int idx = threadIdx.x + 256 * q, rr = idx / BK, kk = idx % BK;
       const int r = tk.r0 + rr, c = kb + kk;
-      pa[q] = (r < tk.rhi && c < tk.kk1) ? F[(int64_t)r * ld + c] : cplx<T>{0, 0};
+      pa[q] = ((A_ALL || idx < BM * BK) && r < tk.rhi && c < tk.kk1) ? F[(int64_t)r * ld + c] : cplx<T>{0, 0};
     }
 #pragma unroll
     for (int q = 0; q < NBt; ++q) {
       const int idx = threadIdx.x + 256 * q, kk = idx / BN, cc = idx % BN;
       const int r = kb + kk, c = tk.c0 + cc;
-      pb[q] = (c < tk.chi && r < tk.kk1) ? F[(int64_t)r * ld + c] : cplx<T>{0, 0};
+      pb[q] = ((B_ALL || idx < BN * BK) && c < tk.chi && r < tk.kk1) ? F[(int64_t)r * ld + c] : cplx<T>{0, 0};
     }
   };
   fetch(tk.kk0);
@@ -989,12 +1001,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) front_gemm_kernel
 #pragma unroll
     for (int q = 0; q < NA; ++q) {
       const int idx = threadIdx.x + 256 * q;
-      As[idx % BK][idx / BK] = pa[q];
+      if (A_ALL || idx < BM * BK) As[idx % BK][idx / BK] = pa[q];
     }
 #pragma unroll
     for (int q = 0; q < NBt; ++q) {
       const int idx = threadIdx.x + 256 * q;
-      Bs[idx / BN][idx % BN] = pb[q];
+      if (B_ALL || idx < BN * BK) Bs[idx / BN][idx % BN] = pb[q];
     }
     __syncthreads();
     if (kb + BK < tk.kk1) fetch(kb + BK);
@@ -1808,6 +1820,14 @@ struct Plan {
                                            // real products per complex block, 3 the same with the
                                            // C tile staged (tuned once per plan)
   float panel_ms[4] = {0, 0, 0, 0};        // tuner's panel-GEMM times: SIMT, DMMA, DMMA 3M, DMMA 3M C staged
+  // FP64 panel-step GEMMs with thin tiles for the narrow tasks: the same (level,
+  // step) slots as step_ptr_d, each split into its wide tasks in DMMA tiles
+  // (step_ptr_tw) and its narrow ones (at most 8 columns or rows) in SIMT 128x8 /
+  // 8x128 tiles (step_ptr_tn); used with the DMMA candidates when panel_thin
+  std::vector<int64_t> step_ptr_tw, step_ptr_tn;
+  bool panel_thin = false;
+  int64_t thin_tasks = 0;                  // narrow-task tiles of one factorisation (per frequency)
+  float panel_thin_ms = 0;                 // tuner's time of the picked DMMA candidate with thin tiles
   bool panel_cst = false;                  // complex64 SIMT panel-step tiles stage C (tuned once per plan)
   std::vector<char> pick;                  // per level candidate
   std::vector<float> tune_ms;              // [candidate][level] measured times
@@ -1861,6 +1881,15 @@ static void add_panel_row_tiles(std::vector<GemmTask> &v, int bm, int bn, int f,
   if (j0 > b0 && j1 < b1) add_tiles(v, bm, bn, f, j0, j1, j1, b1, b0, j0);
   if (j0 > 0 && std::max(j1, b1) < m) add_tiles(v, bm, bn, f, j0, j1, std::max(j1, b1), m, 0, j0);
 }
+// Narrow panel-step regions: the columns add_panel_col_tiles updates at panel j0
+// (the block's columns when j0 starts a block, else the panel's), and the rows
+// [j0, j1) of add_panel_row_tiles, at most kThinMax wide / high
+constexpr int kThinMax = 8;
+static bool panel_col_narrow(int k, int j0) {
+  const int b0 = j0 / kOuter * kOuter, b1 = std::min(k, b0 + kOuter);
+  return (j0 == b0 ? b1 : std::min(k, j0 + kPanel)) - j0 <= kThinMax;
+}
+static bool panel_row_narrow(int k, int j0) { return std::min(k, j0 + kPanel) - j0 <= kThinMax; }
 
 Plan *build_plan(Handle &h, int small_m, bool tensor_schur) {
   Symbolic &S = h.sym;
@@ -1997,6 +2026,40 @@ Plan *build_plan(Handle &h, int small_m, bool tensor_schur) {
         P->step_ptr_d.push_back((int64_t)P->tasks.size());
       }
     }
+    // the same slots split into wide tasks (DMMA tiles) and narrow ones (thin tiles)
+    P->step_ptr_tw.assign(1, (int64_t)P->tasks.size());
+    for (int l = 0; l < S.nlevel; ++l)
+      for (int st = 0; st < P->nsteps[l]; ++st) {
+        const int j0 = st * kPanel;
+        for (int q = P->large_ptr[l]; q < P->large_ptr[l + 1]; ++q) {
+          const int f = P->fronts_large[q];
+          if (j0 < S.k[f] && !panel_col_narrow(S.k[f], j0)) add_panel_col_tiles(P->tasks, 128, 32, f, S.k[f], S.m[f], j0);
+        }
+        P->step_ptr_tw.push_back((int64_t)P->tasks.size());
+        for (int q = P->large_ptr[l]; q < P->large_ptr[l + 1]; ++q) {
+          const int f = P->fronts_large[q];
+          if (j0 < S.k[f] && !panel_row_narrow(S.k[f], j0)) add_panel_row_tiles(P->tasks, 32, 128, f, S.k[f], S.m[f], j0);
+        }
+        P->step_ptr_tw.push_back((int64_t)P->tasks.size());
+      }
+    P->step_ptr_tn.assign(1, (int64_t)P->tasks.size());
+    for (int l = 0; l < S.nlevel; ++l)
+      for (int st = 0; st < P->nsteps[l]; ++st) {
+        const int j0 = st * kPanel;
+        for (int q = P->large_ptr[l]; q < P->large_ptr[l + 1]; ++q) {
+          const int f = P->fronts_large[q];
+          if (j0 < S.k[f] && panel_col_narrow(S.k[f], j0))
+            add_panel_col_tiles(P->tasks, tile_bm(kThinCol), tile_bn(kThinCol), f, S.k[f], S.m[f], j0);
+        }
+        P->step_ptr_tn.push_back((int64_t)P->tasks.size());
+        for (int q = P->large_ptr[l]; q < P->large_ptr[l + 1]; ++q) {
+          const int f = P->fronts_large[q];
+          if (j0 < S.k[f] && panel_row_narrow(S.k[f], j0))
+            add_panel_row_tiles(P->tasks, tile_bm(kThinRow), tile_bn(kThinRow), f, S.k[f], S.m[f], j0);
+        }
+        P->step_ptr_tn.push_back((int64_t)P->tasks.size());
+      }
+    P->thin_tasks = P->step_ptr_tn.back() - P->step_ptr_tn.front();
     P->tuned = false;
   }
   return P;
@@ -2300,12 +2363,26 @@ struct Sweeper {
 
   // panel-step GEMM of (level, step) slot q: which 0 = panel columns (skinny),
   // 1 = U rows (short); SIMT tiles, or DMMA tiles when the tuner chose them
-  void panel_gemm(const FrontArgs<T> &b, int64_t q, int which, int nb) {
+  int panel_gemm(const FrontArgs<T> &b, int64_t q, int which, int nb) {
     const GemmTask *tasks = P.d_tasks.template as<GemmTask>();
     if constexpr (sizeof(T) == 8) {
       if (P.panel_dmma) {
-        const int64_t t0 = P.step_ptr_d[q + which], t1 = P.step_ptr_d[q + which + 1];
-        if (t1 == t0) return;
+        const bool thin = P.panel_thin;
+        int nl = 0;
+        if (thin) {   // the narrow tasks of the slot in thin SIMT tiles
+          const int64_t n0 = P.step_ptr_tn[q + which], n1 = P.step_ptr_tn[q + which + 1];
+          if (n1 > n0) {
+            ++nl;
+            const dim3 g((unsigned)(n1 - n0), nb);
+            if (which == 0)
+              front_gemm_kernel<T, kThinCol><<<g, 256, 0, h.stream>>>(b, tasks + n0);
+            else
+              front_gemm_kernel<T, kThinRow><<<g, 256, 0, h.stream>>>(b, tasks + n0);
+          }
+        }
+        const std::vector<int64_t> &sp = thin ? P.step_ptr_tw : P.step_ptr_d;
+        const int64_t t0 = sp[q + which], t1 = sp[q + which + 1];
+        if (t1 == t0) return nl;
         const dim3 grid((unsigned)(t1 - t0), nb);
         if (P.panel_dmma == 3) {
           if (which == 0)
@@ -2323,11 +2400,11 @@ struct Sweeper {
           else
             front_dmma_kernel<1, 4><<<grid, 128, 0, h.stream>>>(b, tasks + t0);
         }
-        return;
+        return nl + 1;
       }
     }
     const int64_t t0 = P.step_ptr[q + which], t1 = P.step_ptr[q + which + 1];
-    if (t1 == t0) return;
+    if (t1 == t0) return 0;
     const dim3 grid((unsigned)(t1 - t0), nb);
     if (P.panel_cst) {
       if (which == 0)
@@ -2340,6 +2417,7 @@ struct Sweeper {
       else
         front_gemm_kernel<T, kShort><<<grid, 256, 0, h.stream>>>(b, tasks + t0);
     }
+    return 1;
   }
 
   // FP64 Schur update of level l with candidate tile c (0 SIMT 128x64, 1 DMMA
@@ -2430,6 +2508,7 @@ struct Sweeper {
       cudaEvent_t pe[2 * NP];
       for (auto &x : pe) SS_CK(cudaEventCreate(&x));
       float pt[NP] = {0, 0, 0, 0};
+      P.panel_thin = false;
       for (int c = 0; c < NP; ++c) {
         P.panel_dmma = c;
         cudaEventRecord(pe[2 * c], h.stream);
@@ -2447,11 +2526,32 @@ struct Sweeper {
       SS_CK(cudaGetLastError());
       SS_CK(cudaStreamSynchronize(h.stream));
       for (int c = 0; c < NP; ++c) cudaEventElapsedTime(&pt[c], pe[2 * c], pe[2 * c + 1]);
-      for (auto &x : pe) cudaEventDestroy(x);
       P.panel_dmma = 0;
       for (int c = 1; c < NP; ++c)
         if (pt[c] < pt[P.panel_dmma]) P.panel_dmma = c;
       for (int c = 0; c < NP; ++c) P.panel_ms[c] = pt[c];
+      // the picked DMMA tiles once more with the narrow tasks in thin SIMT tiles;
+      // kept if faster
+      P.panel_thin = false;
+      if (P.panel_dmma > 0 && P.thin_tasks > 0) {
+        P.panel_thin = true;
+        cudaEventRecord(pe[0], h.stream);
+        for (int l = 0; l < S.nlevel; ++l) {
+          FrontArgs<T> b = a;
+          b.fronts = P.d_large.as<int>() + P.large_ptr[l];
+          for (int st = 0; st < P.nsteps[l]; ++st) {
+            const int64_t q = P.level_step0[l] + 2 * st;
+            panel_gemm(b, q, 0, nb);
+            panel_gemm(b, q, 1, nb);
+          }
+        }
+        cudaEventRecord(pe[1], h.stream);
+        SS_CK(cudaGetLastError());
+        SS_CK(cudaStreamSynchronize(h.stream));
+        cudaEventElapsedTime(&P.panel_thin_ms, pe[0], pe[1]);
+        P.panel_thin = P.panel_thin_ms < pt[P.panel_dmma];
+      }
+      for (auto &x : pe) cudaEventDestroy(x);
       } else {
       // panel-step GEMMs (complex64, SIMT tiles): once reading C after the K loop,
       // once with C staged in shared memory while it runs
@@ -2483,6 +2583,11 @@ struct Sweeper {
     } else {
       // a forced DMMA Schur tile puts the panel-step GEMMs on the same kind of tile
       P.panel_dmma = sizeof(T) != 8 ? 0 : atoi(force) == 2 ? 1 : atoi(force) == 1 ? 2 : atoi(force) == 3 ? 3 : 0;
+      P.panel_thin = false;
+    }
+    if constexpr (sizeof(T) == 8) {
+      // measurement / test override of the thin tiles (they go with the DMMA tiles)
+      if (const char *e = getenv("SS_PANEL_THIN")) P.panel_thin = atoi(e) != 0 && P.panel_dmma > 0 && P.thin_tasks > 0;
     }
     if constexpr (sizeof(T) == 4) {
       if (const char *e = getenv("SS_PANEL_CST")) P.panel_cst = atoi(e) != 0;   // measurement override
@@ -2556,8 +2661,7 @@ struct Sweeper {
         const int64_t q = P.level_step0[l] + 2 * s;
         const int64_t g0 = P.step_ptr[q], g1 = P.step_ptr[q + 1], g2 = P.step_ptr[q + 2];
         if (g1 > g0) {   // panel columns <- earlier pivots
-          panel_gemm(b, q, 0, nb);
-          ++launches;
+          launches += panel_gemm(b, q, 0, nb);
         }
         const size_t psm = (size_t)std::max(0, P.maxk_large[l] - j0) * (kPanel + 1) * sizeof(cplx<T>);
         const int prow = P.maxk_large[l] - j0;   // panel rows of the widest front
@@ -2579,8 +2683,7 @@ struct Sweeper {
         }
         front_swap_kernel<T><<<dim3(nl, nb, zc), bs, 0, h.stream>>>(b, j0);
         if (g2 > g1) {   // U row block <- earlier pivots
-          panel_gemm(b, q, 1, nb);
-          ++launches;
+          launches += panel_gemm(b, q, 1, nb);
         }
         front_u12_trsm_kernel<T><<<dim3(nl, nb, zc), bs, 0, h.stream>>>(b, j0);
         launches += 4;
@@ -3093,6 +3196,7 @@ static int sweep_impl(Handle &h, int n_f, const double *omega, double V, double 
   h.st[32] = nfail;
   h.st[20] = h.st[21] = h.st[22] = h.st[36] = 0;
   h.st[23] = P.panel_cst ? 4 : P.panel_dmma;
+  h.st[37] = P.panel_thin ? (double)P.thin_tasks : 0.0;
   h.st[24] = P.panel_ms[0];
   h.st[25] = std::min(std::min(P.panel_ms[1], P.panel_ms[2]), P.panel_ms[3]);
   h.st[26] = (double)P.fronts_small.size();

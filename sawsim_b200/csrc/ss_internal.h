@@ -159,7 +159,7 @@ struct Handle {
     int auto_probe_m = 12;               // Krylov steps of SS_PREC_AUTO's probe
   } opt;
   // stats
-  static constexpr int kStats = 37;
+  static constexpr int kStats = 38;
   double st[kStats] = {0};
 };
 

@@ -300,7 +300,7 @@ class FrequencySolver:
                  'schur_candidate2', 'panel_gemm_dmma', 'panel_tune_simt_ms', 'panel_tune_dmma_ms', 'small_fronts',
                  'schur_tune_ms', 'auto_probe_ms', 'fp64_resolved', 'krylov_steps_primal', 'krylov_steps_adjoint',
                  'mixed_not_converged', 'fp64_resolve_ms', 'element_kernel_ms', 'scatter_kernel_ms',
-                 'schur_candidate3']
+                 'schur_candidate3', 'panel_thin_tiles']
 
     def stats(self) -> dict:
         n = len(self.STAT_KEYS)

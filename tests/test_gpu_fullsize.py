@@ -109,3 +109,33 @@ def test_hex_full_backward_error(built_lib):
             assert backward_error(A, disp[o.active], rhs) < 1e-12, fi
     finally:
         g.close()
+
+
+def test_me1_full_thin_panel_tiles(me1_full, monkeypatch):
+    """The benchmarked cell's tail panels (its 36-pivot leaves factor a 32-wide
+    panel, then 4 pivots whose panel-step GEMMs are 4 columns wide / 4 rows high)
+    with those GEMMs in thin SIMT 128x8 / 8x128 tiles beside the DMMA tiles: a
+    backward error below 1e-12 in the oracle's system, and the charges of the
+    DMMA-only panel GEMMs within 1e-8 (the same pivots, other rounding)."""
+    case, o, _ = me1_full
+    f = case.freqs[[0, len(case.freqs) // 2, -1]]
+    monkeypatch.setenv('SS_SCHUR_TILE', '3')    # tuner off: C-staged DMMA Schur and panel tiles
+    out = {}
+    for thin in ('0', '1'):
+        monkeypatch.setenv('SS_PANEL_THIN', thin)
+        e = cases.engine_for(case)
+        try:
+            Q, st, _ = e.charges(2 * np.pi * f, 1.0, 'fp64')
+            s = e.stats()
+            if thin == '1':
+                w = 2 * np.pi * f[1]
+                A, rhs = o.system(w)
+                disp, _, _ = e.solve(w)
+        finally:
+            e.close()
+        assert (st == 0).all()
+        assert s['panel_gemm_dmma'] == 3
+        out[thin] = (Q, s['panel_thin_tiles'])
+    assert out['0'][1] == 0 and out['1'][1] > 0
+    assert backward_error(A, disp[o.active], rhs) < 1e-12
+    assert np.max(np.abs(out['1'][0] - out['0'][0]) / np.abs(out['0'][0])) < 1e-8
