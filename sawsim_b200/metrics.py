@@ -16,8 +16,14 @@ Restates the fr/fa part of the reference's figure-of-merit module
 * ``_rounded`` :174-185 -- GHz and MHz rounded to 0.1 kHz, other floats to 6
   significant digits.
 
-Q extraction and the mode list of the reference are not restated: the sweep
-backend needs only fr, fa and k2eff to state its accuracy against FP64.
+* ``peak_quality`` :38-64 and ``peak_quality_extrapolated`` :67-81 -- Q of a
+  peak of |Y|^2 (fr) or |Z|^2 (fa) from its 3 dB width, with the linear
+  interpolation bias removed by Richardson extrapolation; the Q windows of a
+  lossy locate (``sawsim_b200.locate.quality``) use them.
+
+The coarse per-sweep q_r / q_a estimates and the mode list of ``resonances``
+are not restated: the sweep backend states fr, fa and k2eff against FP64, and a
+lossy locate takes Q from its resolved windows, as the reference's does.
 """
 from __future__ import annotations
 
@@ -119,3 +125,54 @@ def compare(reference: dict, candidate: dict) -> dict:
     a, b = reference.get('k2eff'), candidate.get('k2eff')
     d['k2eff_diff_pct_points'] = _round('', (b - a) * 100) if a is not None and b is not None else None
     return d
+
+
+def peak_quality(f, power):
+    """Q of the highest peak of ``power`` (|Y|^2 for fr, |Z|^2 = 1/|Y|^2 for fa),
+    or None when the peak is a window edge or a half-power crossing lies outside
+    the window (metrics.py:38-64).
+
+    The peak is the vertex of the parabola through the top sample and its two
+    neighbours (shift clipped to half a step); the half-power frequencies are
+    linear interpolations of ``power`` between the samples that straddle half the
+    vertex value, nearest the peak on each side; Q = f0 / (fh - fl)."""
+    f = np.asarray(f, dtype=float)
+    p = np.asarray(power, dtype=float)
+    n = p.size
+    i = int(np.argmax(p))
+    if i == 0 or i == n - 1:
+        return None
+    pl, pc, pr = p[i - 1], p[i], p[i + 1]
+    curv = pl - 2 * pc + pr
+    s = 0.5 * (pl - pr) / curv if curv < 0 else 0.0
+    s = min(max(s, -0.5), 0.5)
+    step = f[i + 1] - f[i]
+    f0 = f[i] + s * step
+    half = (pc - 0.25 * (pl - pr) * s) / 2
+    a = next((j for j in range(i, 0, -1) if p[j - 1] <= half < p[j]), None)
+    b = next((j for j in range(i, n - 1) if p[j + 1] <= half < p[j]), None)
+    if a is None or b is None:
+        return None
+    fl = f[a - 1] + (half - p[a - 1]) / (p[a] - p[a - 1]) * (f[a] - f[a - 1])
+    fh = f[b] + (p[b] - half) / (p[b] - p[b + 1]) * (f[b + 1] - f[b])
+    return dict(f0_hz=float(f0), fl_hz=float(fl), fh_hz=float(fh), q=float(f0 / (fh - fl)),
+                samples_in_linewidth=int(b - a + 1), step_hz=float(step))
+
+
+def peak_quality_extrapolated(f, power):
+    """``peak_quality`` with the half-power interpolation bias removed
+    (metrics.py:67-81): the bias falls as 1/n^2 in the samples per linewidth, so
+    with Q_n from every sample and Q_n/2 the mean over the two every-other-sample
+    subsets, Q = Q_n + (Q_n - Q_n/2) / 3.  Adds ``q_linear`` (Q_n) and ``q_half``
+    (Q_n/2, None when neither subset resolves the peak)."""
+    full = peak_quality(f, power)
+    if full is None:
+        return None
+    f = np.asarray(f)
+    power = np.asarray(power)
+    sub = [peak_quality(f[k::2], power[k::2]) for k in (0, 1)]
+    qs = [r['q'] for r in sub if r]
+    if not qs:
+        return dict(full, q_linear=full['q'], q_half=None)
+    q_half = float(np.mean(qs))
+    return dict(full, q=full['q'] + (full['q'] - q_half) / 3, q_linear=full['q'], q_half=q_half)
