@@ -25,6 +25,7 @@ from __future__ import annotations
 import os
 import sys
 from contextlib import contextmanager
+from pathlib import Path
 
 import numpy as np
 
@@ -127,13 +128,34 @@ _PATCHES = [('sawsim.saw2d.sweep', 'FrequencySolver', FrequencySolver),
             ('sawsim.hex_solver', 'FrequencySolver3D', FrequencySolver3D)]
 
 
+def _metadata_writer(write):
+    """The pipelines' ``atomic_json`` (solver.py:28-32) with ``metadata.json``
+    naming this backend.  The reference writes ``backend`` as 'PARDISO' or 'SciPy
+    SuperLU' from whether pypardiso imports (solver.py:146, hex_solver.py:74) and
+    ``frequency_workers`` from its fork-pool size (solver.py:146), neither of which
+    says what solved a sweep that ran here; every other file passes unchanged."""
+    if getattr(write, 'sawsim_b200', False):
+        return write
+
+    def atomic_json(path, data):
+        if Path(path).name == 'metadata.json' and isinstance(data, dict) and 'backend' in data:
+            data = dict(data, backend=f'B200 (sawsim_b200, {_precision(None)})')
+            if 'frequency_workers' in data:
+                data['frequency_workers'] = 1
+        return write(path, data)
+
+    atomic_json.sawsim_b200 = True
+    return atomic_json
+
+
 def install(modules=None):
     """Point the reference's already imported modules at this backend.
 
     ``modules`` maps module names to module objects (default ``sys.modules``);
-    the names of ``_PATCHES`` that a loaded module defines are replaced.  Returns
-    the list of ``module.attribute`` names replaced, so that a caller can check
-    that the pipeline it runs was reached."""
+    the names of ``_PATCHES`` that a loaded module defines are replaced, and the
+    pipelines' ``atomic_json`` is wrapped so that their ``metadata.json`` names
+    this backend.  Returns the list of ``module.attribute`` names replaced, so
+    that a caller can check that the pipeline it runs was reached."""
     mods = sys.modules if modules is None else modules
     done = []
     for mod, attr, new in _PATCHES:
@@ -141,6 +163,10 @@ def install(modules=None):
         if m is not None and hasattr(m, attr):
             setattr(m, attr, new)
             done.append(f'{mod}.{attr}')
+    m = mods.get('sawsim.solver')
+    if m is not None and hasattr(m, 'atomic_json'):
+        m.atomic_json = _metadata_writer(m.atomic_json)
+        done.append('sawsim.solver.atomic_json')
     return done
 
 

@@ -1,6 +1,7 @@
 """The backend switch on CPU: which reference names ``install`` replaces, the
-environment selection, and ``charge_stream``'s point-by-point path for engines
-that are not this backend's (the reference's own, here a stand-in)."""
+environment selection, the metadata the pipelines write through the wrapped
+``atomic_json``, and ``charge_stream``'s point-by-point path for engines that are
+not this backend's (the reference's own, here a stand-in)."""
 import types
 
 import numpy as np
@@ -66,3 +67,22 @@ def test_charge_stream_point_by_point_for_other_engines():
         with backend.charge_stream(_PointEngine(is_hex), f, 2.0, is_hex=is_hex) as res:
             q = [next(res) for _ in f]
         assert np.allclose(q, 2 * np.pi * f * 2.0)
+
+
+def test_install_names_the_backend_in_the_metadata(monkeypatch):
+    monkeypatch.delenv('SAWSIM_B200_PRECISION', raising=False)
+    written = []
+    m = types.ModuleType('sawsim.solver')
+    m.atomic_json = lambda path, data: written.append((str(path), data))
+    mods = {'sawsim.solver': m}
+    assert backend.install(mods) == ['sawsim.solver.atomic_json']
+    first = m.atomic_json
+    backend.install(mods)                      # a second install does not wrap twice
+    assert m.atomic_json is first
+    meta = dict(backend='SciPy SuperLU', frequency_workers=8, nodes=12)
+    m.atomic_json('out/metadata.json', meta)
+    m.atomic_json('out/curve.json', dict(backend='left alone'))
+    assert written[0] == ('out/metadata.json', dict(backend='B200 (sawsim_b200, fp64)', frequency_workers=1,
+                                                    nodes=12))
+    assert meta['backend'] == 'SciPy SuperLU'  # the caller's dict is not modified
+    assert written[1] == ('out/curve.json', dict(backend='left alone'))
