@@ -123,6 +123,7 @@ def add_quality(result, eng, band_limits_ghz, **kw) -> dict:
             result[f'f{key}_ghz'] = round(q['f_ghz'], 7)
     if result.get('fr_ghz') and result.get('fa_ghz'):
         result['k2eff'] = round(math.pi ** 2 / 4 * (result['fa_ghz'] - result['fr_ghz']) / result['fa_ghz'], 6)
+    result['notes'] = [n for n in result.get('notes', []) if not n.startswith('Q not resolved')]
     result['quality'] = dict(method='Q = f_peak / 3 dB width of |Y|^2 (fr) and |Z|^2 (fa); final window +/-1.5 '
                                     'linewidths, interpolation bias removed by Richardson extrapolation; fr/fa '
                                     'are the refined peaks', resonance=qr, antiresonance=qa)

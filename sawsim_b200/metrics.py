@@ -1,7 +1,7 @@
 """Resonance / antiresonance extraction from a swept admittance curve (host side).
 
-Restates the fr/fa part of the reference's figure-of-merit module
-(``src/sawsim/metrics.py``), which judges the sweep's fr/fa criterion:
+Restates the reference's figure-of-merit module (``src/sawsim/metrics.py``),
+which judges the sweep's fr/fa criterion:
 
 * ``resonances`` :98-171 -- |Y|/f removes the static-capacitance slope; every
   local maximum of |Y|/f (``_local_extrema`` :33-35) is paired with the lowest
@@ -14,16 +14,17 @@ Restates the fr/fa part of the reference's figure-of-merit module
   fa on |Y|/f);
 * ``compare`` :188-199 -- fr/fa deviation in MHz and ppm, k2eff in %-points;
 * ``_rounded`` :174-185 -- GHz and MHz rounded to 0.1 kHz, other floats to 6
-  significant digits.
-
+  significant digits;
 * ``peak_quality`` :38-64 and ``peak_quality_extrapolated`` :67-81 -- Q of a
   peak of |Y|^2 (fr) or |Z|^2 (fa) from its 3 dB width, with the linear
   interpolation bias removed by Richardson extrapolation; the Q windows of a
-  lossy locate (``sawsim_b200.locate.quality``) use them.
+  lossy locate (``sawsim_b200.locate.quality``) use them;
+* ``_half_power_q`` :84-95 -- the coarse q_r / q_a of one sweep: the 3 dB width
+  of |Y| (|Z| for fa) between the neighbouring extrema, only when it spans at
+  least ``MIN_SAMPLES_IN_LINEWIDTH`` samples; and the mode list of
+  ``resonances`` :160-170 (every pair, strongest first, then by frequency).
 
-The coarse per-sweep q_r / q_a estimates and the mode list of ``resonances``
-are not restated: the sweep backend states fr, fa and k2eff against FP64, and a
-lossy locate takes Q from its resolved windows, as the reference's does.
+Warnings are the reference's codes (the text before its colon).
 """
 from __future__ import annotations
 
@@ -32,6 +33,9 @@ import math
 import numpy as np
 
 K2_FORMULA = 'k2eff = pi^2/4 * (fa - fr) / fa'
+MIN_SAMPLES_IN_LINEWIDTH = 8      # a 3 dB width over fewer samples is a sampling artefact
+Q_NOTE = ('Q not resolved at this frequency step (3 dB width spans < %d samples); q_r/q_a are null - locate '
+          'with beta_dk/eta_eps > 0 resolves Q' % MIN_SAMPLES_IN_LINEWIDTH)
 
 
 def _vertex(f, g, i):
@@ -57,22 +61,45 @@ def _minima(y):
 
 
 def _round(key, v):
+    """GHz and MHz to 0.1 kHz, other floats to 6 significant digits, through nested
+    dicts and lists (a list's items take the list's key)."""
     if isinstance(v, float):
         if key.endswith('_ghz'):
             return round(v, 7)
         if key.endswith('_mhz'):
             return round(v, 4)
         return float('%.6g' % v)
+    if isinstance(v, dict):
+        return {k: _round(k, x) for k, x in v.items()}
+    if isinstance(v, list):
+        return [_round(key, x) for x in v]
     return v
 
 
-def resonances(frequency_hz, admittance) -> dict:
-    """fr / fa (GHz), k2eff and warnings of a sampled admittance (complex Y or |Y|)."""
+def _half_power_q(f, mag, i, lo, hi):
+    """Q = f[i] / 3 dB width of the peak of ``mag`` at sample i, the half-power
+    samples searched outwards within [lo, hi]; None unless both exist and the
+    width spans at least MIN_SAMPLES_IN_LINEWIDTH samples."""
+    p = mag ** 2
+    half = p[i] / 2
+    a = next((j for j in range(i - 1, lo - 1, -1) if p[j] <= half), None)
+    b = next((j for j in range(i + 1, hi + 1) if p[j] <= half), None)
+    if a is None or b is None or b - a < MIN_SAMPLES_IN_LINEWIDTH:
+        return None
+    fl = np.interp(half, [p[a], p[a + 1]], [f[a], f[a + 1]])
+    fh = np.interp(half, [p[b], p[b - 1]], [f[b], f[b - 1]])
+    return float(f[i] / (fh - fl)) if fh > fl else None
+
+
+def resonances(frequency_hz, admittance, max_modes: int = 5) -> dict:
+    """fr / fa (GHz), k2eff, the coarse q_r / q_a, the in-band modes (at most
+    ``max_modes``), warnings and notes of a sampled admittance (complex Y or |Y|)."""
     f = np.asarray(frequency_hz, dtype=float)
     mag = np.abs(np.asarray(admittance))
     n = f.size
-    out = dict(fr_ghz=None, fa_ghz=None, k2eff=None, k2_formula=K2_FORMULA, frequency_step_mhz=None,
-               uncertainty_mhz=None, points_between_fr_fa=None, warnings=[])
+    out = dict(fr_ghz=None, fa_ghz=None, k2eff=None, k2_formula=K2_FORMULA, q_r=None, q_a=None,
+               frequency_step_mhz=None, uncertainty_mhz=None, points_between_fr_fa=None, modes=[], warnings=[],
+               notes=[])
     if n < 5 or not np.all(np.isfinite(mag)):
         out['warnings'].append('curve too short or contains non-finite values')
         return out
@@ -90,16 +117,20 @@ def resonances(frequency_hz, admittance) -> dict:
             continue
         if a != n - 1 and f[a] - f[p] > 0.15 * f[p]:
             continue
-        pairs.append(((g[p] - g[a]) / g[p], int(p), a))
+        pairs.append(((g[p] - g[a]) / g[p], int(p), a, stop))
     if not pairs:
         if int(np.argmax(g)) in (0, n - 1):
             out['warnings'].append('peak_at_band_edge')
         else:
             out['warnings'].append('no_resonance_found')
-        return {k: _round(k, v) for k, v in out.items()}
-    _, r, a = max(pairs, key=lambda t: (min(t[0], 0.5), g[t[1]]))
+        return _round('', out)
+    rank = lambda t: (min(t[0], 0.5), g[t[1]])      # noqa: E731
+    score, r, a, stop = max(pairs, key=rank)
     fr = _vertex(f, inv, r)
     out['fr_ghz'] = fr * 1e-9
+    minima = _minima(g)
+    before = minima[minima < r]
+    out['q_r'] = _half_power_q(f, mag, r, int(before[-1]) if before.size else 0, a)
     if a == n - 1:
         out['warnings'].append('antiresonance_not_found')
     else:
@@ -107,11 +138,21 @@ def resonances(frequency_hz, admittance) -> dict:
         out['fa_ghz'] = fa * 1e-9
         out['k2eff'] = math.pi ** 2 / 4 * (fa - fr) / fa
         out['points_between_fr_fa'] = int(a - r - 1)
+        out['q_a'] = _half_power_q(f, 1.0 / np.maximum(mag, np.finfo(float).tiny), a, r, stop)
         if a - r < 6:
             out['warnings'].append('coarse_sampling')
     if max(g[0], g[-1]) > 3 * g[r]:
         out['warnings'].append('stronger_response_at_band_edge')
-    return {k: _round(k, v) for k, v in out.items()}
+    if out['q_r'] is None:
+        out['notes'].append(Q_NOTE)
+    for st, p, q, _ in sorted(pairs, key=rank, reverse=True)[:max_modes]:
+        out['modes'].append(dict(fr_ghz=_vertex(f, inv, p) * 1e-9, fa_ghz=_vertex(f, g, q) * 1e-9 if q != n - 1 else None,
+                                 peak_abs_y=float(mag[p]), strength=float(st), is_main=bool(p == r)))
+    out['modes'].sort(key=lambda m: m['fr_ghz'])
+    strong = [m for m in out['modes'] if m['strength'] > 0.5 * min(score, 0.5) and m['peak_abs_y'] > 0.1 * mag[r]]
+    if len(strong) > 1:
+        out['warnings'].append('multiple_modes')
+    return _round('', out)
 
 
 def compare(reference: dict, candidate: dict) -> dict:

@@ -1,7 +1,7 @@
 """fr/fa extraction (sawsim_b200.metrics) against the reference's own extractor
-(src/sawsim/metrics.py:98-171) on its stored template curves and synthetic
-resonators (tests/golden/metrics_curves.npz, made by make_metrics_golden.py).
-CPU only."""
+(src/sawsim/metrics.py:84-171) on its stored template curves and synthetic
+lossless and lossy resonators (tests/golden/metrics_curves.npz, made by
+make_metrics_golden.py).  CPU only."""
 import json
 import math
 
@@ -13,19 +13,15 @@ from sawsim_b200.metrics import compare, resonances
 
 _G = np.load(GOLDEN / 'metrics_curves.npz')
 _META = json.loads(str(_G['meta']))
-# the warning codes this restatement keeps (Q and mode-list warnings are not restated)
-_KEPT = {'peak_at_band_edge', 'no_resonance_found', 'antiresonance_not_found', 'coarse_sampling',
-         'stronger_response_at_band_edge'}
 
 
 @pytest.mark.parametrize('i', range(len(_META)), ids=[m['name'] for m in _META])
 def test_matches_reference_extractor(i):
-    ref = _META[i]
-    r = resonances(_G[f'f{i}'], _G[f'y{i}'])
-    assert r['fr_ghz'] == ref['fr_ghz']
-    assert r['fa_ghz'] == ref['fa_ghz']
-    assert r['k2eff'] == ref['k2eff']
-    assert set(r['warnings']) == {w for w in ref['warnings'] if w in _KEPT}
+    """The whole result: fr / fa / k2eff, the coarse q_r / q_a, the mode list,
+    warning codes and notes."""
+    ref = dict(_META[i])
+    ref.pop('name')
+    assert resonances(_G[f'f{i}'], _G[f'y{i}']) == ref
 
 
 def test_subgrid_lossless_pair():
