@@ -289,6 +289,33 @@ int ss_measure_gemm_ceiling(ss_handle *h, int kernel, int m, int k, int n_fronts
                             double *tflops);
 
 /*
+ * Host-only analysis of a mesh system: the global pattern, the Bloch fold and
+ * condensation, the nested-dissection ordering and the multifrontal front tree
+ * that ss_analyze builds, computed on the host with no CUDA device and no handle
+ * (no counterpart in the reference, whose SuperLU / PARDISO calls analyse inside
+ * every per-frequency solve, src/sawsim/saw2d/sweep.py:346-353).  It shows the
+ * fronts, fill, flops and front memory of a cell before it runs on a GPU.
+ *
+ * Inputs as for ss_set_mesh (without materials) and ss_set_bc.  Outputs:
+ * sizes[4] = {active DOFs n, fronts F, total front rows R, tree levels};
+ * stats[6] = {factorisation flops per point, nnz(L+U), widest front, most
+ * pivots of a front, complex front elements per point (m x padded ld, summed),
+ * condensed nonzeros}.  Arrays that are not NULL are filled: active[n] (global
+ * DOF of each active DOF, ascending), order[n] (elimination position of each
+ * active DOF), k[F], m[F] (pivots, rows), parent[F] (-1 at a root), level[F],
+ * rows_ptr[F+1] and rows[R] (each front's rows in elimination positions: its
+ * pivots, then its update rows ascending).  Call once with NULL arrays for the
+ * sizes, then with arrays of those sizes.  Errors: SS_EINVAL for bad inputs or
+ * an analysis that fails (there is no handle, so no error text).
+ */
+int ss_analyze_host(int element_kind, int64_t n_nodes, const double *pos_m, int64_t n_elem,
+                    const int64_t *conn, int64_t gdof, int64_t n_fix, const int64_t *fix, int64_t n_zheng,
+                    const int64_t *zheng, int64_t n_fu, const int64_t *fu, int64_t n_groups,
+                    const int64_t *group_ptr, const int64_t *group_dofs, int64_t two_stage, int64_t *sizes,
+                    double *stats, int64_t *active, int64_t *order, int32_t *k, int32_t *m, int32_t *parent,
+                    int32_t *level, int64_t *rows_ptr, int64_t *rows);
+
+/*
  * Q9 assembly that allocates nothing (no counterpart in the reference).  It is
  * for callers of this library that may not allocate device memory: a host
  * framework that hands out all device memory from its own pool (a caching

@@ -51,6 +51,9 @@ SIGNATURES = [
     ('ss_stats', C.c_int, [_P, _DP, C.c_int]),
     ('ss_set_option', C.c_int, [_P, C.c_char_p, C.c_double]),
     ('ss_measure_gemm_ceiling', C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _DP]),
+    ('ss_analyze_host', C.c_int, [C.c_int, C.c_int64, _DP, C.c_int64, _I64P, C.c_int64, C.c_int64, _I64P, C.c_int64,
+                                  _I64P, C.c_int64, _I64P, C.c_int64, _I64P, _I64P, C.c_int64, _I64P, _DP, _I64P,
+                                  _I64P, _I32P, _I32P, _I32P, _I32P, _I64P, _I64P]),
     ('ss_assemble_q9_noalloc', C.c_int, [C.c_int, C.c_int64, _P, C.c_int64, _P, _P, _P, _P, _P, _P, C.c_int, _P, _P,
                                          _P, _P, _P, _P, C.c_double, _P, _P, _P, C.c_int64, _P, _P, _P]),
 ]

@@ -1,0 +1,82 @@
+"""Host-only analysis of a cell (``ss_analyze_host``): the condensation, the
+nested-dissection ordering and the front tree that a GPU engine would use, with
+no CUDA device.  ``analyze_q9`` / ``analyze_hex27`` take the inputs of the
+engine constructors (mesh and boundary sets; no materials) and return the
+sizes, the work and memory per frequency point, and the front tree."""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+from .engine import _bc_arrays
+
+
+@dataclass
+class Analysis:
+    n_active: int
+    flops_per_point: float          # factorisation flops of one frequency point
+    nnz_lu: float
+    max_front: int
+    max_pivots: int
+    front_bytes_per_point: dict     # complex128 / complex64 fronts of one point
+    condensed_nnz: int
+    levels: int
+    active: np.ndarray              # global DOF of each active DOF, ascending
+    order: np.ndarray               # elimination position of each active DOF
+    k: np.ndarray                   # pivots per front (fronts in postorder)
+    m: np.ndarray                   # rows per front
+    parent: np.ndarray              # parent front, -1 at a root
+    level: np.ndarray               # tree level (leaves 0)
+    rows_ptr: np.ndarray
+    rows: np.ndarray                # front rows in elimination positions (pivots first)
+
+
+def _run(kind, pos, conn, gdof, bc, two_stage):
+    lib = L.load()
+    pos, conn = L.f64(pos), L.i64(conn)
+    fix, zheng, fu, gptr, gd = _bc_arrays(bc)
+    args = [kind, pos.shape[0], L.ptr(pos, C.c_double), conn.shape[0], L.ptr(conn, C.c_int64), int(gdof),
+            fix.size, L.ptr(fix, C.c_int64), zheng.size, L.ptr(zheng, C.c_int64), fu.size, L.ptr(fu, C.c_int64),
+            gptr.size - 1, L.ptr(gptr, C.c_int64), L.ptr(gd, C.c_int64), int(two_stage)]
+    sizes = np.zeros(4, dtype=np.int64)
+    stats = np.zeros(6)
+    rc = lib.ss_analyze_host(*args, L.ptr(sizes, C.c_int64), L.ptr(stats, C.c_double),
+                             *([None] * 8))
+    if rc != L.SS_OK:
+        raise L.SawsimError(rc, 'host analysis failed')
+    n, nf, nr, _ = (int(x) for x in sizes)
+    active, order = np.zeros(n, np.int64), np.zeros(n, np.int64)
+    k, m, parent, level = (np.zeros(nf, np.int32) for _ in range(4))
+    rows_ptr, rows = np.zeros(nf + 1, np.int64), np.zeros(nr, np.int64)
+    rc = lib.ss_analyze_host(*args, L.ptr(sizes, C.c_int64), L.ptr(stats, C.c_double),
+                             L.ptr(active, C.c_int64), L.ptr(order, C.c_int64), L.ptr(k, C.c_int32),
+                             L.ptr(m, C.c_int32), L.ptr(parent, C.c_int32), L.ptr(level, C.c_int32),
+                             L.ptr(rows_ptr, C.c_int64), L.ptr(rows, C.c_int64))
+    if rc != L.SS_OK:
+        raise L.SawsimError(rc, 'host analysis failed')
+    return Analysis(n_active=n, flops_per_point=float(stats[0]), nnz_lu=float(stats[1]), max_front=int(stats[2]),
+                    max_pivots=int(stats[3]),
+                    front_bytes_per_point=dict(complex128=16 * stats[4], complex64=8 * stats[4]),
+                    condensed_nnz=int(stats[5]), levels=int(sizes[3]), active=active, order=order, k=k, m=m,
+                    parent=parent, level=level, rows_ptr=rows_ptr, rows=rows)
+
+
+def analyze_q9(pos_m, quads, bc, mode_extension=1) -> Analysis:
+    """Analysis of a Q9 cell: ``pos_m`` (N, 2) node coordinates, ``quads`` (ne, 9)
+    0-based connectivity, ``bc`` the ``(fix, zheng, fu, merge_groups)`` tuple of
+    ``sweep.bc_periodic`` (as ``FrequencySolver.from_q9`` takes them)."""
+    pos = np.asarray(pos_m)[:, :2]
+    nc = 4 if mode_extension else 3
+    kind = L.SS_Q9_ME1 if mode_extension else L.SS_Q9_ME0
+    return _run(kind, pos, quads, nc * pos.shape[0], bc, 0)
+
+
+def analyze_hex27(pos_m, hexas, bc) -> Analysis:
+    """Analysis of a Hex27 slab with ``bc = (fix, zheng, fu, groups, two_stage)``
+    (as ``FrequencySolver.from_hex27`` takes them)."""
+    fix, zheng, fu, groups, two_stage = bc
+    pos = np.asarray(pos_m)
+    return _run(L.SS_HEX27, pos, hexas, 4 * pos.shape[0], (fix, zheng, fu, groups), two_stage)
