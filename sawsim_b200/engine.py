@@ -351,8 +351,18 @@ class FrequencySolver:
         return Q.view(np.complex128), st, it
 
     def sweep(self, fre, V: float = 1.0, precision: str = 'fp64'):
-        """Charges at frequencies ``fre`` (Hz), all points in batched GPU factorisations."""
-        Q, st, _ = self.charges(2 * np.pi * np.asarray(fre, dtype=float), V, precision)
+        """Charges at frequencies ``fre`` (Hz), all points in batched GPU factorisations.
+        Raises ``SawsimError`` when a point fails (a singular or non-finite solve, or
+        an unconverged refinement), as the reference's solve raises on a singular
+        matrix and its pipeline on a non-finite charge (solver.py:121-122);
+        ``charges`` returns the per-point statuses instead."""
+        fre = np.asarray(fre, dtype=float)
+        Q, st, _ = self.charges(2 * np.pi * fre, V, precision)
+        bad = np.flatnonzero(st)
+        if bad.size:
+            code = int(st[bad[0]])
+            raise L.SawsimError(code, f'{bad.size} of {st.size} points failed, the first at '
+                                      f'{fre.ravel()[bad[0]] * 1e-9:.9f} GHz')
         return Q
 
     def solve(self, omega: float, V: float = 1.0):
