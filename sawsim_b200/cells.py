@@ -22,6 +22,7 @@ The unit cell is two pitches wide with one + and one - electrode
 """
 from __future__ import annotations
 
+import math
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -218,6 +219,168 @@ def sp_quad_layer_cell() -> Q9Cell:
     p = 1.085
     return q9_cell(p, 8, [Band(TAG_PIEZO, 0.6, 3), Band(22, 0.5, 2), Band(23, 1.0, 4), Band(24, 7.83, 29),
                           Band(25, 2.17, 8)], Band(TAG_ELECTRODE, 0.17, 1))
+
+
+def _stack_bands(pitch_um, electrode_um, substrate_um, backings, coatings, mesh_um, pml_pitches):
+    """Element bands of the generic stack, bottom first: (tag, y_bottom, y_top, rows),
+    with 'E' for the electrode band, following src/sawsim/sp_meshes/stack.py:27-68:
+    mesh_um near the surface (depth <= 2p), max(h, min(4h, p/2)) deeper, a band
+    that crosses depth 2p split there; the PML (2p, at least 8 rows, deep
+    spacing) below the last backing; above y = 0 the electrode band, then the
+    coatings (the first measured from the piezo surface)."""
+    p, h, d = float(pitch_um), float(mesh_um), float(electrode_um)
+    h_deep = max(h, min(4 * h, p / 2))
+    near = 2 * p
+    nb, nc = len(backings), len(coatings)
+    depth = [(TAG_PIEZO, 0.0, float(substrate_um))]
+    z = float(substrate_um)
+    for i, t in enumerate(backings):
+        depth.append((22 + i, z, z + t))
+        z += t
+    split = []
+    for tag, top, bot in depth:
+        split += [(tag, top, near), (tag, near, bot)] if top < near < bot - 1e-12 else [(tag, top, bot)]
+
+    def nrows(span, step):
+        return max(1, math.ceil(span / step - 1e-9))
+
+    below = [(tag, -bot, -top, nrows(bot - top, h if bot <= near + 1e-12 else h_deep)) for tag, top, bot in split]
+    pml_h = pml_pitches * p
+    tag_pml = 22 + nb + nc
+    below.append((tag_pml, -(z + pml_h), -z, max(8, nrows(pml_h, h_deep))))
+    below.sort(key=lambda b: b[1])
+    above = [('E', 0.0, d, nrows(d, h))]
+    if nc:
+        top = float(coatings[0])
+        if not top > d:
+            raise ValueError('the first coating is measured from the piezo surface and must exceed the electrode')
+        above.append((22 + nb, d, top, nrows(top - d, h)))
+        for j, t in enumerate(coatings[1:], start=1):
+            above.append((22 + nb + j, top, top + t, nrows(t, h)))
+            top += t
+    return below, above, dict(h_near=h, h_deep=h_deep, pml_thickness_um=pml_h, tag_pml=tag_pml,
+                              tag_backing=[22 + i for i in range(nb)], tag_coating=[22 + nb + j for j in range(nc)])
+
+
+def sp_stack_cell(pitch_um: float = 1.085, metal_ratio: float = 0.5, electrode_um: float = 0.17,
+                  substrate_um: float = 8.0, backings=(), coatings=(), mesh_um: float = 0.5,
+                  pml_pitches: float = 2.0) -> Q9Cell:
+    """The reference's generic ``sp_stack`` template (``src/sawsim/sp_meshes/stack.py``),
+    rebuilt without Gmsh: a two-pitch cell with one + and one - electrode, from the
+    bottom: PML | backings (last .. first) | piezo substrate | electrodes, embedded
+    in the first coating when there is one | further coatings.
+
+    Across, 9 cuts at the electrode edges and centres make 8 strips of
+    ceil(width / mesh_um) uniform columns each, the same on every level; down,
+    every band has the rows of ``_stack_bands``, uniform inside the band.  Without
+    coatings the electrode band holds only the four electrode strips (free
+    surface between them).  ``backings`` and ``coatings`` are thicknesses in um
+    (0-6 and 0-3 of them); tags 16 piezo, 15 electrode, 22.. backings, then
+    coatings, then the PML; lines 17 / 18 (the electrodes' contact, flanks and
+    top), 19 left, 20 right, 21 bottom.  Material order (the reference's
+    ``build_mesh`` for sp_stack): 0 piezo, 1 electrode, then backings and
+    coatings; the PML takes the last backing's material, or the piezo's.
+    """
+    p = float(pitch_um)
+    w = 2 * p
+    below, above, meta = _stack_bands(pitch_um, electrode_um, substrate_um, list(backings), list(coatings),
+                                      mesh_um, pml_pitches)
+    mr = float(metal_ratio)
+    cuts = [0.0, p * (1 - mr) / 2, p / 2, p * (1 + mr) / 2, p, p * (3 - mr) / 2, 1.5 * p, p * (3 + mr) / 2, w]
+    cols = [max(1, math.ceil((cuts[i + 1] - cuts[i]) / mesh_um - 1e-9)) for i in range(8)]
+    # element edges and the strip / band of every element column / row
+    xe, strip_of = [], []
+    for i in range(8):
+        xe += [cuts[i] + (cuts[i + 1] - cuts[i]) * j / cols[i] for j in range(cols[i])]
+        strip_of += [i] * cols[i]
+    xe.append(w)
+    bands = below + above
+    ye, band_of = [], []
+    for bi, (_, y0, y1, nr) in enumerate(bands):
+        ye += [y0 + (y1 - y0) * r / nr for r in range(nr)]
+        band_of += [bi] * nr
+    ye.append(bands[-1][2])
+    ncol, nrow = len(xe) - 1, len(ye) - 1
+    e_band = len(below)                                     # the band between y = 0 and y = d
+    teeth = {1: TAG_ZHENG, 2: TAG_ZHENG, 5: TAG_FU, 6: TAG_FU}
+    coated = bool(meta['tag_coating'])
+
+    def elem_tag(r, c):
+        bi = band_of[r]
+        if bi != e_band:
+            return bands[bi][0]
+        if strip_of[c] in teeth:
+            return TAG_ELECTRODE
+        return meta['tag_coating'][0] if coated else None  # free surface between bare electrodes
+
+    tags = np.array([[elem_tag(r, c) or 0 for c in range(ncol)] for r in range(nrow)])
+    # candidate node grid (element edges and mid-points), then only the used nodes
+    xn = np.empty(2 * ncol + 1)
+    xn[0::2] = xe
+    xn[1::2] = 0.5 * (np.array(xe[:-1]) + np.array(xe[1:]))
+    yn = np.empty(2 * nrow + 1)
+    yn[0::2] = ye
+    yn[1::2] = 0.5 * (np.array(ye[:-1]) + np.array(ye[1:]))
+    grid = np.arange(yn.size * xn.size).reshape(yn.size, xn.size)
+
+    def q9(r, c):
+        j, i = 2 * r, 2 * c
+        g = grid
+        return [g[j, i], g[j, i + 2], g[j + 2, i + 2], g[j + 2, i],
+                g[j, i + 1], g[j + 1, i + 2], g[j + 2, i + 1], g[j + 1, i], g[j + 1, i + 1]]
+
+    quads, qtags = [], []
+    for r in range(nrow):
+        for c in range(ncol):
+            if tags[r, c]:
+                quads.append(q9(r, c))
+                qtags.append(tags[r, c])
+    lines = []
+
+    def edge(n0, nm, n1, tag):
+        lines.append([n0, n1, nm, tag])
+
+    for r in range(nrow):
+        for c in range(ncol):
+            if not tags[r, c]:
+                continue
+            j, i = 2 * r, 2 * c
+            if r == 0:
+                edge(grid[j, i], grid[j, i + 1], grid[j, i + 2], TAG_BOTTOM)
+            if c == 0:
+                edge(grid[j, i], grid[j + 1, i], grid[j + 2, i], TAG_LEFT)
+            if c == ncol - 1:
+                edge(grid[j, i + 2], grid[j + 1, i + 2], grid[j + 2, i + 2], TAG_RIGHT)
+            s = strip_of[c]
+            if band_of[r] == e_band and s in teeth:
+                lt = teeth[s]
+                if r == 0 or band_of[r - 1] != e_band:            # contact with the piezo surface
+                    edge(grid[j, i], grid[j, i + 1], grid[j, i + 2], lt)
+                if r == nrow - 1 or band_of[r + 1] != e_band:     # electrode top
+                    edge(grid[j + 2, i], grid[j + 2, i + 1], grid[j + 2, i + 2], lt)
+                if s in (1, 5) and (c == 0 or strip_of[c - 1] != s):
+                    edge(grid[j, i], grid[j + 1, i], grid[j + 2, i], lt)            # outer flank
+                if s in (2, 6) and (c == ncol - 1 or strip_of[c + 1] != s):
+                    edge(grid[j, i + 2], grid[j + 1, i + 2], grid[j + 2, i + 2], lt)  # outer flank
+    used = np.unique(np.array(quads).ravel())
+    renum = np.full(grid.size, -1, dtype=np.int64)
+    renum[used] = np.arange(used.size)
+    X, Y = np.meshgrid(xn, yn)
+    P = np.column_stack([X.ravel()[used], Y.ravel()[used], np.zeros(used.size)])
+    POS = _clean13(P)
+    Q = renum[np.array(quads)]
+    QUADS9 = np.column_stack([Q.astype(float) + 1, np.array(qtags, dtype=float)])
+    Ln = np.array(lines, dtype=np.int64)
+    LINES3 = np.column_stack([renum[Ln[:, :3]].astype(float) + 1, Ln[:, 3].astype(float)])
+    tb, tc = meta['tag_backing'], meta['tag_coating']
+    tag_map = {TAG_PIEZO: 0, TAG_ELECTRODE: 1, meta['tag_pml']: (1 + len(tb)) if tb else 0}
+    tag_map.update({t: i + 2 for i, t in enumerate(tb + tc)})
+    bottom = float(POS[:, 1].min())
+    return Q9Cell(POS=POS, QUADS9=QUADS9, LINES3=LINES3, tag_map=tag_map, pml_tag=meta['tag_pml'],
+                  pml_top_um=bottom + meta['pml_thickness_um'], pml_bottom_um=bottom, period_um=w,
+                  info=dict(rows=[b[3] for b in bands], cols=cols, levels=[b[1] for b in bands] + [bands[-1][2]],
+                            cuts=cuts, h_near=meta['h_near'], h_deep=meta['h_deep'],
+                            tag_backing=tb, tag_coating=tc, pml_thickness_um=meta['pml_thickness_um']))
 
 
 def me0_cell(columns: int = 16, rows: int = 64, pitch_um: float = 1.085) -> Q9Cell:
