@@ -13,6 +13,9 @@ stand-in for the gmsh module):
   ratio), what the reference's ``sp_meshes/stack.py:GM`` lays out: the band
   levels and strip cuts (its geometry points), rows and columns per band and
   strip, the physical tag of every (band, strip) surface, its tag lists;
+* the layered templates' configurations (sp_double_layer, sp_triple_layer,
+  sp_quad_layer: their tests/data records), resolved materials and the fr / fa
+  of their independent FEM and published curves;
 * the single-layer configuration of the reference's own cross-template test
   (tests/test_stack_materials.py:54-63, ``sp_stack`` with no layers against the
   ``sp_single_layer`` data): the resolved materials (records of its material
@@ -205,10 +208,40 @@ def single_layer():
                                                sweeps=r['sweeps']))
 
 
+def layered_templates():
+    """The layered templates' configurations (their tests/data records), resolved
+    materials and the fr / fa of their independent FEM and published curves."""
+    from sawsim.material_library import get_record
+    from sawsim.material_runtime import from_record
+    from sawsim.metrics import resonances
+    from sawsim.saw2d.materials import oula_transfer
+    out = []
+    for name in ('sp_double_layer', 'sp_triple_layer', 'sp_quad_layer'):
+        meta = json.loads((REF / f'tests/data/{name}.json').read_text())
+        data = np.load(REF / f'tests/data/{name}.npz')
+        cfg = {k: v for k, v in meta['config'].items() if k != 'material_snapshots'}
+        sub = from_record(get_record(cfg['substrate_material']))
+        el = from_record(get_record(cfg['electrode_material']))
+        lays = [from_record(get_record(layer['material_id'])) for layer in cfg['layers']]
+        C, e, eps = oula_transfer([cfg['euler_phi_deg'], cfg['euler_theta_deg'], cfg['euler_psi_deg']], sub.C,
+                                  sub.e, sub.eps)
+        rho = [sub.rho, el.rho] + [m.rho for m in lays]
+        Cs = [C, el.C] + [m.C for m in lays]
+        es = [e, el.e] + [m.e for m in lays]
+        epss = [eps, el.eps] + [m.eps for m in lays]
+        fem = resonances(data['frequency_hz'], data['reference_magnitude'])
+        pub = resonances(data['frequency_hz'], data['sawsim_magnitude'])
+        out.append(dict(name=name, config=cfg, rho=rho, C=[np.asarray(x).tolist() for x in Cs],
+                        e=[np.asarray(x).tolist() for x in es], eps=[np.asarray(x).tolist() for x in epss],
+                        independent_fem=dict(fr_ghz=fem['fr_ghz'], fa_ghz=fem['fa_ghz']),
+                        published=dict(fr_ghz=pub['fr_ghz'], fa_ghz=pub['fa_ghz'])))
+    return out
+
+
 def main():
     layouts = [dict(args, layout=gm_layout(**args)) for args in LAYOUTS]
     sys.modules.pop('gmsh', None)
-    out = dict(layouts=layouts, single_layer=single_layer())
+    out = dict(layouts=layouts, single_layer=single_layer(), layered=layered_templates())
     (HERE / 'sp_stack.json').write_text(json.dumps(out))
     s = out['single_layer']
     print(len(layouts), 'layouts; single layer: independent FEM', s['independent_fem'], 'reference on the rebuilt mesh',

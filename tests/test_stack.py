@@ -98,3 +98,20 @@ def test_single_layer_stack_matches_the_independent_fem():
     assert abs(r['fr_ghz'] - fem['fr_ghz']) < 1e-3 and abs(r['fa_ghz'] - fem['fa_ghz']) < 1e-3
     assert abs(r['fr_ghz'] - ref['fr_ghz']) <= 1e-6 and abs(r['fa_ghz'] - ref['fa_ghz']) <= 1e-6
     assert r['band_ghz'] == ref['band_ghz'] and r['sweeps'] == ref['sweeps']
+
+
+@pytest.mark.parametrize('t', _G['layered'], ids=[t['name'] for t in _G['layered']])
+def test_stack_reproduces_the_layered_templates(t):
+    """The same cross-template bar on the layered templates: sp_stack with their
+    backings at their configurations, located by the oracle, within 1 MHz of their
+    independent FEM fr / fa (sp_triple_layer is meshed unstructured by Gmsh and
+    has no rebuild of its own)."""
+    cfg = t['config']
+    mats = [Material(t['rho'][i], np.array(t['C'][i]), np.array(t['e'][i]), np.array(t['eps'][i]))
+            for i in range(len(t['rho']))]
+    cell = cells.sp_stack_cell(cfg['pitch_um'], cfg['metal_ratio'], cfg['electrode_um'], cfg['substrate_um'],
+                               [layer['thickness_um'] for layer in cfg['layers']], [], cfg['mesh_um'])
+    r = locate(_OracleRun(cell, mats, cfg['pitch_um']), cfg['start_ghz'], cfg['stop_ghz'], 41,
+               tuple(_G['single_layer']['band_limits_ghz']), zoom_points=101, precision='fp64')
+    fem = t['independent_fem']
+    assert r['ok'] and abs(r['fr_ghz'] - fem['fr_ghz']) < 1e-3 and abs(r['fa_ghz'] - fem['fa_ghz']) < 1e-3
