@@ -567,6 +567,51 @@ def hex_slab_cell(pitch_um: float, nx: int, ny: int, bands, electrode: Band, ape
                    aperture_um=float(aperture_um), info=dict(nx=nx, ny=ny, nz=nz, electrode_cols=cols))
 
 
+# Element layers of the Hex27 templates (src/sawsim/sp_hex_meshes/{single,double,triple,quad}.py):
+# every band gets max(1, ceil(coef * thickness / base * ref / mesh_um)) layers; rows per
+# template (piezo, backings..., PML), then the reference size ``ref`` those coefficients assume
+_HEX_TEMPLATE_LAYERS = {
+    'single': ([(30, 6.51)], (10, 2.17), 0.217),
+    'double': ([(3, 0.6), (30, 6.51)], (10, 2.17), 0.217),
+    'triple': ([(3, 0.6), (3, 0.5), (30, 6.51)], (11, 2.17), 0.217),
+    'quad': ([(3, 0.6), (3, 0.5), (5, 1.0), (30, 6.0)], (10, 2.0), 0.2),
+}
+
+
+def sp_2p5d_template_cell(kind: str, pitch_um: float = 1.085, electrode_um: float = 0.17,
+                          substrate_um: float = 0.6, layers_um=(6.51,), metal_ratio: float = 0.5,
+                          mesh_um: float = 0.217, aperture_um: float = 0.217, nx: int = 16) -> HexCell:
+    """The reference's 2.5D Hex27 templates (``sp_2p5d_{kind}_layer``, kind single /
+    double / triple / quad; ``src/sawsim/sp_hex_meshes/*.py``) rebuilt without Gmsh.
+
+    Down (z): the piezo substrate, the backing layers and a 2p PML, each with the
+    element layers of the template's own rule (``_HEX_TEMPLATE_LAYERS``); the
+    electrodes stand ``electrode_um`` high with their layers of the same rule.
+    Across the aperture (y): one element, as the templates' transfinite y edges
+    give.  Along x the templates leave the division to Gmsh's mesh size
+    (``mesh_um``); ``nx`` uniform columns stand in for it: at the templates'
+    defaults (strips of 1.25 and 2.5 x mesh_um) nx = 16 reproduces the reference's
+    published curves within its own regression tolerance.  Tags: 7 piezo, 8
+    electrode, 9.. backings, the PML after them with the last backing's material
+    (the piezo's for the single layer).
+    """
+    rows, pml_rule, ref = _HEX_TEMPLATE_LAYERS[kind]
+    hs = [float(substrate_um)] + [float(t) for t in layers_um]
+    if len(hs) != len(rows):
+        raise ValueError(f'sp_2p5d_{kind}_layer takes {len(rows) - 1} backing layers')
+
+    def layers(coef, h, base):
+        return max(1, math.ceil(coef * h / base * ref / mesh_um - 1e-12))
+
+    p = float(pitch_um)
+    bands = [Band(HEX_TAG_PIEZO, hs[0], layers(*rows[0][:1], hs[0], rows[0][1]))]
+    for i, h in enumerate(hs[1:]):
+        bands.append(Band(HEX_TAG_LAYER + i, h, layers(rows[i + 1][0], h, rows[i + 1][1])))
+    bands.append(Band(HEX_TAG_LAYER + len(hs) - 1, 2 * p, layers(pml_rule[0], 2 * p, pml_rule[1])))
+    electrode = Band(HEX_TAG_ELECTRODE, float(electrode_um), max(1, math.ceil(electrode_um / 0.17 * ref / mesh_um - 1e-12)))
+    return hex_slab_cell(p, nx, 1, bands, electrode, aperture_um, metal_ratio=metal_ratio)
+
+
 def hex_double_layer_slab(nx: int = 8, ny: int = 4, nz: int = 48, pitch_um: float = 1.085) -> HexCell:
     """Double-layer Hex27 slab: 3m film 0.6p / SiO2 1.4p / SiO2 PML 2p (z), aperture
     0.5p, Al electrodes 0.08p (one layer) on top.  ``nz`` element layers split
