@@ -316,6 +316,22 @@ int ss_analyze_host(int element_kind, int64_t n_nodes, const double *pos_m, int6
                     int32_t *level, int64_t *rows_ptr, int64_t *rows);
 
 /*
+ * The same host-only analysis from an assembled pattern, as ss_set_csr takes it
+ * (the reference engine's FrequencySolver(K, M, ...), sweep.py:283-314): the
+ * union pattern of K and M (gdof rows, columns strictly ascending), and
+ * optionally the node of every DOF and the node coordinates (dim 2 or 3), which
+ * give the geometric ordering of the mesh path; without them the ordering is the
+ * graph nested dissection of ss_analyze.  Boundary sets and outputs as for
+ * ss_analyze_host.
+ */
+int ss_analyze_host_csr(int64_t gdof, const int64_t *indptr, const int64_t *indices, int64_t n_nodes, int dim,
+                        const int64_t *dof_node, const double *node_xyz, int64_t n_fix, const int64_t *fix,
+                        int64_t n_zheng, const int64_t *zheng, int64_t n_fu, const int64_t *fu, int64_t n_groups,
+                        const int64_t *group_ptr, const int64_t *group_dofs, int64_t two_stage, int64_t *sizes,
+                        double *stats, int64_t *active, int64_t *order, int32_t *k, int32_t *m, int32_t *parent,
+                        int32_t *level, int64_t *rows_ptr, int64_t *rows);
+
+/*
  * Q9 assembly that allocates nothing (no counterpart in the reference).  It is
  * for callers of this library that may not allocate device memory: a host
  * framework that hands out all device memory from its own pool (a caching

@@ -54,6 +54,9 @@ SIGNATURES = [
     ('ss_analyze_host', C.c_int, [C.c_int, C.c_int64, _DP, C.c_int64, _I64P, C.c_int64, C.c_int64, _I64P, C.c_int64,
                                   _I64P, C.c_int64, _I64P, C.c_int64, _I64P, _I64P, C.c_int64, _I64P, _DP, _I64P,
                                   _I64P, _I32P, _I32P, _I32P, _I32P, _I64P, _I64P]),
+    ('ss_analyze_host_csr', C.c_int, [C.c_int64, _I64P, _I64P, C.c_int64, C.c_int, _I64P, _DP, C.c_int64, _I64P,
+                                      C.c_int64, _I64P, C.c_int64, _I64P, C.c_int64, _I64P, _I64P, C.c_int64, _I64P,
+                                      _DP, _I64P, _I64P, _I32P, _I32P, _I32P, _I32P, _I64P, _I64P]),
     ('ss_assemble_q9_noalloc', C.c_int, [C.c_int, C.c_int64, _P, C.c_int64, _P, _P, _P, _P, _P, _P, C.c_int, _P, _P,
                                          _P, _P, _P, _P, C.c_double, _P, _P, _P, C.c_int64, _P, _P, _P]),
 ]

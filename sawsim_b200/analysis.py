@@ -34,27 +34,32 @@ class Analysis:
     rows: np.ndarray                # front rows in elimination positions (pivots first)
 
 
-def _run(kind, pos, conn, gdof, bc, two_stage):
-    lib = L.load()
-    pos, conn = L.f64(pos), L.i64(conn)
+def _bc_args(bc, two_stage):
     fix, zheng, fu, gptr, gd = _bc_arrays(bc)
-    args = [kind, pos.shape[0], L.ptr(pos, C.c_double), conn.shape[0], L.ptr(conn, C.c_int64), int(gdof),
-            fix.size, L.ptr(fix, C.c_int64), zheng.size, L.ptr(zheng, C.c_int64), fu.size, L.ptr(fu, C.c_int64),
-            gptr.size - 1, L.ptr(gptr, C.c_int64), L.ptr(gd, C.c_int64), int(two_stage)]
+    return [fix.size, L.ptr(fix, C.c_int64), zheng.size, L.ptr(zheng, C.c_int64), fu.size, L.ptr(fu, C.c_int64),
+            gptr.size - 1, L.ptr(gptr, C.c_int64), L.ptr(gd, C.c_int64), int(two_stage)], (fix, zheng, fu, gptr, gd)
+
+
+def _run(kind, pos, conn, gdof, bc, two_stage):
+    pos, conn = L.f64(pos), L.i64(conn)
+    bca, keep = _bc_args(bc, two_stage)
+    args = [kind, pos.shape[0], L.ptr(pos, C.c_double), conn.shape[0], L.ptr(conn, C.c_int64), int(gdof)] + bca
+    return _call(L.load().ss_analyze_host, args)
+
+
+def _call(fn, args):
     sizes = np.zeros(4, dtype=np.int64)
     stats = np.zeros(6)
-    rc = lib.ss_analyze_host(*args, L.ptr(sizes, C.c_int64), L.ptr(stats, C.c_double),
-                             *([None] * 8))
+    rc = fn(*args, L.ptr(sizes, C.c_int64), L.ptr(stats, C.c_double), *([None] * 8))
     if rc != L.SS_OK:
         raise L.SawsimError(rc, 'host analysis failed')
     n, nf, nr, _ = (int(x) for x in sizes)
     active, order = np.zeros(n, np.int64), np.zeros(n, np.int64)
     k, m, parent, level = (np.zeros(nf, np.int32) for _ in range(4))
     rows_ptr, rows = np.zeros(nf + 1, np.int64), np.zeros(nr, np.int64)
-    rc = lib.ss_analyze_host(*args, L.ptr(sizes, C.c_int64), L.ptr(stats, C.c_double),
-                             L.ptr(active, C.c_int64), L.ptr(order, C.c_int64), L.ptr(k, C.c_int32),
-                             L.ptr(m, C.c_int32), L.ptr(parent, C.c_int32), L.ptr(level, C.c_int32),
-                             L.ptr(rows_ptr, C.c_int64), L.ptr(rows, C.c_int64))
+    rc = fn(*args, L.ptr(sizes, C.c_int64), L.ptr(stats, C.c_double), L.ptr(active, C.c_int64),
+            L.ptr(order, C.c_int64), L.ptr(k, C.c_int32), L.ptr(m, C.c_int32), L.ptr(parent, C.c_int32),
+            L.ptr(level, C.c_int32), L.ptr(rows_ptr, C.c_int64), L.ptr(rows, C.c_int64))
     if rc != L.SS_OK:
         raise L.SawsimError(rc, 'host analysis failed')
     return Analysis(n_active=n, flops_per_point=float(stats[0]), nnz_lu=float(stats[1]), max_front=int(stats[2]),
@@ -80,3 +85,28 @@ def analyze_hex27(pos_m, hexas, bc) -> Analysis:
     fix, zheng, fu, groups, two_stage = bc
     pos = np.asarray(pos_m)
     return _run(L.SS_HEX27, pos, hexas, 4 * pos.shape[0], (fix, zheng, fu, groups), two_stage)
+
+
+def analyze_csr(pattern, bc, two_stage=0, dof_node=None, node_xyz=None) -> Analysis:
+    """Analysis from an assembled pattern (``ss_analyze_host_csr``): ``pattern`` a
+    scipy sparse matrix whose structure is the union of K's and M's, ``bc`` the
+    ``(fix, zheng, fu, groups)`` of the reference engine's constructor
+    (``FrequencySolver.from_matrices`` takes the same); ``dof_node`` and
+    ``node_xyz`` (nodes x 2 or 3) give the geometric ordering of the mesh path,
+    else the graph nested dissection."""
+    A = pattern.tocsr()
+    A.sort_indices()
+    A.sum_duplicates()
+    indptr, indices = L.i64(A.indptr), L.i64(A.indices)
+    gdof = A.shape[0]
+    if node_xyz is not None:
+        xyz = L.f64(node_xyz)
+        n_nodes, dim = xyz.shape
+        xp = L.ptr(xyz, C.c_double)
+    else:
+        n_nodes, dim, xp = (int(np.max(dof_node)) + 1 if dof_node is not None else 0), 0, None
+    dn = L.i64(dof_node) if dof_node is not None else None
+    bca, keep = _bc_args(bc, two_stage)
+    args = [gdof, L.ptr(indptr, C.c_int64), L.ptr(indices, C.c_int64), n_nodes, dim,
+            None if dn is None else L.ptr(dn, C.c_int64), xp] + bca
+    return _call(L.load().ss_analyze_host_csr, args)

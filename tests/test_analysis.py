@@ -21,7 +21,7 @@ import scipy.sparse as sp
 
 from oracle import hex27 as oh, q9 as oq9, solver as osol
 from sawsim_b200 import _lib as L, cases
-from sawsim_b200.analysis import analyze_hex27, analyze_q9
+from sawsim_b200.analysis import analyze_csr, analyze_hex27, analyze_q9
 
 
 def _node_graph(conn, N):
@@ -166,3 +166,29 @@ def test_benchmarked_cell_analysis():
     assert a.n_active == 262664 and np.array_equal(a.active, np.setdiff1d(np.arange(4 * c.mesh.N), presc))
     _check_tree(a)
     assert a.front_bytes_per_point['complex128'] < 5e9     # 37 points per chunk in 180 GB
+
+
+def test_matrix_input_with_node_map_equals_the_mesh_path():
+    """From the assembled pattern with the node of every DOF and the node
+    coordinates, the analysis is the mesh path's, front for front."""
+    c, bc, T, active, S = _q9('me1_64x256', 8, 16)
+    a = analyze_q9(c.mesh.pos_m, c.mesh.quads, bc)
+    b = analyze_csr(S, bc, dof_node=np.arange(S.shape[0]) % c.mesh.N, node_xyz=c.mesh.pos_m[:, :2])
+    for key in ('active', 'order', 'k', 'm', 'parent', 'level', 'rows_ptr', 'rows'):
+        assert np.array_equal(getattr(a, key), getattr(b, key)), key
+
+
+@pytest.mark.parametrize('cell', ['q9', 'hex27'])
+def test_graph_nested_dissection_fill_is_exact(cell):
+    """Without geometry (a Gmsh-meshed template's assembled matrices): the graph
+    nested dissection's front tree is valid and its fill exact."""
+    if cell == 'q9':
+        c, bc, T, active, S = _q9('me1_64x256', 8, 16)
+        a = analyze_csr(S, bc)
+    else:
+        c, T, active, S = _hex(8, 1, 6)
+        fix, zheng, fu, groups, two_stage = c.bc
+        a = analyze_csr(S, (fix, zheng, fu, groups), two_stage=two_stage)
+    assert np.array_equal(a.active, active)
+    _check_tree(a)
+    _check_fill(a, T, active, S)
