@@ -110,3 +110,65 @@ def analyze_csr(pattern, bc, two_stage=0, dof_node=None, node_xyz=None) -> Analy
     args = [gdof, L.ptr(indptr, C.c_int64), L.ptr(indices, C.c_int64), n_nodes, dim,
             None if dn is None else L.ptr(dn, C.c_int64), xp] + bca
     return _call(L.load().ss_analyze_host_csr, args)
+
+
+def level_work(a: Analysis, itemsize: int = 16) -> list:
+    """Work and traffic of one frequency point's factorisation, level by level
+    (leaves first): fronts, pivots, the Schur-update flops (8 k (m-k)^2 per front,
+    complex multiply-adds x 8) and bytes (the update block read and written once,
+    the two panels read once), the rest of the factorisation's flops (the panel
+    LU, L21 and U12: 8 (k^3/3 + k^2 (m-k) + k (m-k)^2) minus the Schur part), the
+    bytes the front assembly moves at the least (each front written once, m x m,
+    each child's update block read once) and the factors' bytes (L+U entries, read
+    once by each triangular solve)."""
+    k = a.k.astype(float)
+    u = (a.m - a.k).astype(float)
+    schur = 8.0 * k * u * u
+    total = 8.0 * (k ** 3 / 3 + k * k * u + k * u * u)
+    front_bytes = itemsize * a.m.astype(float) ** 2
+    cb_bytes = itemsize * u * u                     # read by the parent's assembly
+    lu_bytes = itemsize * (k * k + 2 * k * u)
+    schur_bytes = itemsize * (2 * u * u + 2 * k * u)   # F22 read and written, F21 and F12 read
+    out = []
+    for lev in range(a.levels):
+        sel = a.level == lev
+        kids = np.isin(a.parent, np.flatnonzero(sel))
+        out.append(dict(level=lev, fronts=int(sel.sum()), pivots=int(a.k[sel].sum()),
+                        max_front=int(a.m[sel].max()), schur_flops=float(schur[sel].sum()),
+                        schur_bytes=float(schur_bytes[sel].sum()),
+                        other_flops=float((total - schur)[sel].sum()),
+                        assembly_bytes=float(front_bytes[sel].sum() + cb_bytes[kids].sum()),
+                        lu_bytes=float(lu_bytes[sel].sum())))
+    return out
+
+
+def _main(argv=None):
+    """Per-level work of a cell's factorisation as a markdown table:
+    ``python -m sawsim_b200.analysis --case me1_64x256 --points 37``."""
+    import argparse
+    from . import cases
+    p = argparse.ArgumentParser(description=_main.__doc__)
+    p.add_argument('--case', default='me1_64x256')
+    p.add_argument('--points', type=int, default=1, help='points per factorisation (the chunk)')
+    p.add_argument('--itemsize', type=int, default=16, help='16 complex128, 8 complex64')
+    args = p.parse_args(argv)
+    if args.case.startswith('hex'):
+        c = cases.make_hex_case(args.case)
+        a = analyze_hex27(c.pos_m, c.hexas, c.bc)
+    else:
+        c = cases.make_case(args.case)
+        a = analyze_q9(c.mesh.pos_m, c.mesh.quads, c.bc, c.mode_extension)
+    n = args.points
+    print(f'{args.case}: {a.n_active} active DOFs, {a.k.size} fronts, {a.levels} levels; '
+          f'{a.flops_per_point / 1e9:.1f} GFLOP and {a.nnz_lu / 1e6:.2f} M L+U entries per point; x {n} points')
+    print()
+    print('| level | fronts | pivots | widest front | Schur GFLOP | Schur GB | other GFLOP | assembly GB | L+U GB |')
+    print('|---:|---:|---:|---:|---:|---:|---:|---:|---:|')
+    for r in level_work(a, args.itemsize):
+        print(f"| {r['level']} | {r['fronts']} | {r['pivots']} | {r['max_front']} | {n * r['schur_flops'] / 1e9:.1f} | "
+              f"{n * r['schur_bytes'] / 1e9:.2f} | {n * r['other_flops'] / 1e9:.1f} | "
+              f"{n * r['assembly_bytes'] / 1e9:.2f} | {n * r['lu_bytes'] / 1e9:.2f} |")
+
+
+if __name__ == '__main__':
+    _main()

@@ -21,7 +21,7 @@ import scipy.sparse as sp
 
 from oracle import hex27 as oh, q9 as oq9, solver as osol
 from sawsim_b200 import _lib as L, cases
-from sawsim_b200.analysis import analyze_csr, analyze_hex27, analyze_q9
+from sawsim_b200.analysis import analyze_csr, analyze_hex27, analyze_q9, level_work
 
 
 def _node_graph(conn, N):
@@ -192,3 +192,13 @@ def test_graph_nested_dissection_fill_is_exact(cell):
     assert np.array_equal(a.active, active)
     _check_tree(a)
     _check_fill(a, T, active, S)
+
+
+def test_level_work_adds_up():
+    c, bc, T, active, S = _q9('me1_64x256', 8, 16)
+    a = analyze_q9(c.mesh.pos_m, c.mesh.quads, bc)
+    w = level_work(a)
+    assert len(w) == a.levels and sum(r['fronts'] for r in w) == a.k.size
+    assert sum(r['schur_flops'] + r['other_flops'] for r in w) == pytest.approx(a.flops_per_point, rel=1e-12)
+    assert sum(r['lu_bytes'] for r in w) == pytest.approx(16 * a.nnz_lu, rel=1e-12)
+    assert sum(r['pivots'] for r in w) == a.n_active
