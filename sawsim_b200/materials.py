@@ -135,6 +135,15 @@ def project_xy_plane_strain(mat: Material) -> Material:
     return Material(mat.rho, mat.C[np.ix_(s, s)], mat.e[np.ix_(el, s)], mat.eps[np.ix_(el, el)])
 
 
+def project_xz_plane_strain(mat: Material) -> Material:
+    """The TC-SAW projection (materials.py:303-308): the source frame's xz plane
+    becomes the mesh's xy plane (strain rows xx, zz, xz; fields x, z), after the
+    source-frame rotation; the result is lifted like an xy projection."""
+    s = [0, 2, 4]
+    el = [0, 2]
+    return Material(mat.rho, mat.C[np.ix_(s, s)], mat.e[np.ix_(el, s)], mat.eps[np.ix_(el, el)])
+
+
 def lift_plane_strain(mat: Material) -> Material:
     """Zero-filled 6x6/3x6/3x3 tensors from projected 3x3/2x3/2x2 ones (piezo_fem.py:389-401)."""
     if mat.C.shape != (3, 3) or mat.e.shape != (2, 3) or mat.eps.shape != (2, 2):

@@ -15,7 +15,8 @@ It records, with the reference's functions only:
   poly-Si and cubic Si constants of the synthetic cells;
 * ``rotation_matrix`` and ``oula_transfer`` (src/sawsim/saw2d/materials.py:28-71,
   :250-265) of each seeded crystal at its own seeded Euler triple and at four
-  fixed triples, and ``project_xy_plane_strain`` (:281-290) of the results;
+  fixed triples, and ``project_xy_plane_strain`` (:281-290) and
+  ``project_xz_plane_strain`` (:303-308) of the results;
 * central differences (step 1e-4 degrees) of ``oula_transfer`` in the second
   Euler angle at the seeded triples, the reference value of the d/dtheta
   tangent that the adjoint gradient seeds.
@@ -38,7 +39,7 @@ sys.path.insert(0, str(REF / 'src'))
 
 from sawsim.crystal import EPS0, tensors                                     # noqa: E402
 from sawsim.material_library import get_record                                # noqa: E402
-from sawsim.saw2d.materials import (Material, oula_transfer, project_xy_plane_strain,  # noqa: E402
+from sawsim.saw2d.materials import (Material, oula_transfer, project_xy_plane_strain, project_xz_plane_strain,  # noqa: E402
                                     rotation_matrix)
 
 from sawsim_b200 import materials as mt                                       # noqa: E402
@@ -68,14 +69,17 @@ def main():
         out[f's{seed}_C'], out[f's{seed}_e'], out[f's{seed}_eps'] = C, e, eps
         triples = np.vstack([euler[None, :], FIXED])
         out[f's{seed}_triples'] = triples
-        rot = []
+        rot, xz = [], []
         for t in triples:
             a = rotation_matrix(t)
             Cr, er, epsr = oula_transfer(t, C, e, eps)
             p = project_xy_plane_strain(Material(4700.0, Cr, er, epsr))
             rot.append(np.concatenate([a.ravel(), Cr.ravel(), er.ravel(), epsr.ravel(), p.C.ravel(), p.e.ravel(),
                                        p.eps.ravel()]))
+            q = project_xz_plane_strain(Material(4700.0, Cr, er, epsr))
+            xz.append(np.concatenate([q.C.ravel(), q.e.ravel(), q.eps.ravel()]))
         out[f's{seed}_rot'] = np.array(rot)
+        out[f's{seed}_xz'] = np.array(xz)
         tp, tm = euler.copy(), euler.copy()
         tp[1] += H
         tm[1] -= H

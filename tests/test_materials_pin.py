@@ -2,8 +2,9 @@
 
 The fixture ``golden/materials.npz`` was written by ``golden/make_materials_golden.py``
 with the reference's ``crystal.tensors`` (src/sawsim/crystal.py:30-78),
-``oula_transfer`` / ``rotation_matrix`` / ``project_xy_plane_strain``
-(src/sawsim/saw2d/materials.py:28-71, :250-265, :281-290) and central
+``oula_transfer`` / ``rotation_matrix`` / ``project_xy_plane_strain`` /
+``project_xz_plane_strain``
+(src/sawsim/saw2d/materials.py:28-71, :250-265, :281-290, :303-308) and central
 differences of ``oula_transfer`` in the second Euler angle.  These tests check
 ``sawsim_b200.materials`` (which feeds both the GPU path and the oracle) and the
 d/dtheta tangent of ``sawsim_b200.params`` against them.
@@ -74,6 +75,16 @@ def test_rotation_and_projection_match_oula_transfer(seed):
         ours = np.concatenate([a.ravel(), r.C.ravel(), r.e.ravel(), r.eps.ravel(), p.C.ravel(), p.e.ravel(),
                                p.eps.ravel()])
         np.testing.assert_array_equal(ours, ref, err_msg=str(t))
+
+
+@pytest.mark.parametrize('seed', range(4))
+def test_tc_projection_matches_reference(seed):
+    """The TC-SAW xz-plane projection of the rotated tensors: equal to the
+    reference's project_xz_plane_strain bit for bit."""
+    m = _crystal(G[f's{seed}_consts'])
+    for t, ref in zip(G[f's{seed}_triples'], G[f's{seed}_xz']):
+        q = mt.project_xz_plane_strain(mt.rotate(m, t))
+        np.testing.assert_array_equal(np.concatenate([q.C.ravel(), q.e.ravel(), q.eps.ravel()]), ref, err_msg=str(t))
 
 
 @pytest.mark.parametrize('seed', range(4))
