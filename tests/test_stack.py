@@ -115,3 +115,22 @@ def test_stack_reproduces_the_layered_templates(t):
                tuple(_G['single_layer']['band_limits_ghz']), zoom_points=101, precision='fp64')
     fem = t['independent_fem']
     assert r['ok'] and abs(r['fr_ghz'] - fem['fr_ghz']) < 1e-3 and abs(r['fa_ghz'] - fem['fa_ghz']) < 1e-3
+
+
+@pytest.mark.parametrize('case', _G['layouts'][:2], ids=['no_layers', 'layers_and_coatings'])
+def test_stack_through_the_product_host_path(case):
+    """The rebuilt stack through the product's own host path (mesh, Bloch sets,
+    host analysis): the active DOFs are the oracle's (its bc_periodic and fold) and
+    the front tree is complete, so the GPU engine takes the cell like any Q9 cell."""
+    from sawsim_b200 import cases
+    from sawsim_b200.analysis import analyze_q9
+    c = cells.sp_stack_cell(case['pitch'], case['mr'], case['d'], case['h_piezo'], case['backings'],
+                            case['coatings'], case['mesh_um'])
+    mesh = cases.mesh_from_msh(c.msh())
+    a = analyze_q9(mesh.pos_m, mesh.quads, cases.bc_periodic(mesh, c.LINES3, 3))
+    m = oq9.build_model(c.msh())
+    fix, zheng, fu, groups = osol.bc_periodic(m, c.LINES3, ndisp=3)
+    _, slaves, _ = osol.merge_transform(4 * m.N, groups)
+    presc = np.unique(np.concatenate([np.asarray(fix, int), slaves, np.asarray(zheng, int), np.asarray(fu, int)]))
+    assert np.array_equal(a.active, np.setdiff1d(np.arange(4 * m.N), presc))
+    assert int(a.k.sum()) == a.n_active
