@@ -89,12 +89,13 @@ def analyze_hex27(pos_m, hexas, bc) -> Analysis:
 
 def analyze_csr(pattern, bc, two_stage=0, dof_node=None, node_xyz=None) -> Analysis:
     """Analysis from an assembled pattern (``ss_analyze_host_csr``): ``pattern`` a
-    scipy sparse matrix whose structure is the union of K's and M's, ``bc`` the
+    scipy sparse matrix whose structure is the union of K's and M's (for example
+    ``abs(K) + abs(M)``, which no cancellation can thin out), ``bc`` the
     ``(fix, zheng, fu, groups)`` of the reference engine's constructor
     (``FrequencySolver.from_matrices`` takes the same); ``dof_node`` and
     ``node_xyz`` (nodes x 2 or 3) give the geometric ordering of the mesh path,
     else the graph nested dissection."""
-    A = pattern.tocsr()
+    A = pattern.tocsr(copy=True)
     A.sort_indices()
     A.sum_duplicates()
     indptr, indices = L.i64(A.indptr), L.i64(A.indices)
