@@ -42,3 +42,24 @@ def test_hex_template_reproduces_published_curves(t):
     pub, fem = np.array(t['published']), np.array(t['independent_fem'])
     assert np.max(np.abs(Y - pub) / pub) < 5e-4
     assert np.max(np.abs(Y - fem) / fem) < t['reference_rtol']
+
+
+@pytest.mark.parametrize('t', _G, ids=[t['kind'] for t in _G])
+def test_hex_template_through_the_product_host_path(t):
+    """The rebuilt templates through the product's own host path (the Bloch / front-back
+    sets of cases.bc_periodic_3d, the host analysis): the oracle's active DOFs and a
+    complete front tree, so the GPU engine takes them like the slab cells."""
+    from sawsim_b200 import cases
+    from sawsim_b200.analysis import analyze_hex27
+    cfg = t['config']
+    cell = cells.sp_2p5d_template_cell(t['kind'], cfg['pitch_um'], cfg['electrode_um'], cfg['substrate_um'],
+                                       [layer['thickness_um'] for layer in cfg['layers']], cfg['metal_ratio'],
+                                       cfg['mesh_um'], cfg['aperture_um'])
+    pos_m = cell.POS * 1e-6
+    N = cell.POS.shape[0]
+    a = analyze_hex27(pos_m, cell.HEXAS27, cases.bc_periodic_3d(cell.sets, pos_m, N))
+    mach, elec = oh.boundary_idx_vect_3ds(cell.sets, pos_m, 3 * N)
+    presc = np.unique(np.concatenate([mach['fix'], mach['period_B'], mach['period_R'], elec['period_R'],
+                                      elec['period_B'], elec['zheng'], elec['fu']]))
+    assert np.array_equal(a.active, np.setdiff1d(np.arange(4 * N), presc))
+    assert int(a.k.sum()) == a.n_active
