@@ -50,8 +50,11 @@ def _freqs(config):
     return np.linspace(config['start_ghz'] * 1e9, config['stop_ghz'] * 1e9, int(config['points']))
 
 
-def case_for(config: dict, materials: list):
-    """``(case, loss)`` of a configuration: a ``cases.Case`` (Q9) or ``cases.HexCase``."""
+def case_for(config, materials: list):
+    """``(case, loss)`` of a configuration (a dict of the reference's configuration
+    fields, or its ``SimulationConfig``): a ``cases.Case`` (Q9) or ``cases.HexCase``."""
+    if not isinstance(config, dict):
+        config = config.model_dump()
     model_id = config['model_id']
     loss = Loss(float(config.get('beta_dk') or 0.0), float(config.get('eta_eps') or 0.0))
     layers = [_thickness(x) for x in config.get('layers', [])]

@@ -82,3 +82,17 @@ def test_unsupported_requests_are_refused():
         templates.case_for(DOUBLE, mats[:2])
     with pytest.raises(ValueError, match='no Gmsh-free rebuild'):
         templates.case_for(dict(DOUBLE, model_id='sp_tcsaw'), mats)
+
+
+def test_config_objects_are_accepted():
+    """A configuration object with ``model_dump`` (the reference's SimulationConfig)
+    gives the same case as its dict."""
+    _, mats = _double_materials()
+
+    class Config:
+        def model_dump(self):
+            return dict(DOUBLE)
+
+    a, _ = templates.case_for(Config(), mats)
+    b, _ = templates.case_for(DOUBLE, mats)
+    assert np.array_equal(a.mat_idx, b.mat_idx) and np.array_equal(a.freqs, b.freqs)
